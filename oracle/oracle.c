@@ -1,0 +1,720 @@
+/*
+ * CPU oracle for the CasPhy tree-building hot path -- TEST INFRASTRUCTURE.
+ *
+ * Only tests/, __graft_entry__.smoke() and bench.py (cpu_baseline and
+ * --impl reference legs) load this file's shared object; the product
+ * library never does.  Each function restates one reference executable's
+ * semantics (host loop + device kernel) in plain C, citing the reference
+ * lines it follows.  Paths are relative to the CasPhy source tree.
+ *
+ * Arithmetic is reproduced exactly:
+ *  - joinEdgeIndel accumulates binary16 (`half`) weights one site at a time in
+ *    ascending site order (cu/joinEdgeIndel.cu:73-79); here each add is done
+ *    in double (exact for two binary16 operands) and rounded once to
+ *    binary16, round-to-nearest-even, which is what the device `add.f16`
+ *    does.  Weights are converted from the float64 file with one RNE
+ *    rounding (cu/joinEdgeIndel.cu:296-298).
+ *  - joinEdgeBitReverse / radiusNeighbor accumulate binary32 weights over
+ *    the query's set bits in ascending bit order
+ *    (cu/joinEdgeBitReverse.cu:61-69, cu/radiusNeighbor.cu:33-41).
+ *  - argmax ties: larger value wins, then the smaller node index; the
+ *    reduction starts from (-1, 0) (cu/joinEdgeIndel.cu:110-121).
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef uint32_t u32;
+typedef uint16_t u16;
+typedef uint64_t u64;
+
+/* ------------------------------------------------------------------ */
+/* binary16                                                             */
+/* ------------------------------------------------------------------ */
+
+uint16_t oracle_f64_to_f16(double x) {
+    u64 u;
+    memcpy(&u, &x, 8);
+    u16 sign = (u16)((u >> 48) & 0x8000u);
+    u64 ax = u & 0x7FFFFFFFFFFFFFFFull;
+    if (ax >= 0x7FF0000000000000ull) {
+        if (ax > 0x7FF0000000000000ull) return (u16)(sign | 0x7E00u); /* NaN */
+        return (u16)(sign | 0x7C00u);                                   /* inf */
+    }
+    double a;
+    memcpy(&a, &ax, 8);
+    if (a >= 65520.0) return (u16)(sign | 0x7C00u);
+    if (a < 6.103515625e-05) { /* below 2^-14: subnormal grid of 2^-24 */
+        double r = nearbyint(a * 16777216.0);
+        return (u16)(sign | (u16)r);
+    }
+    int e;
+    (void)frexp(a, &e);                 /* a = f * 2^e, f in [0.5,1) */
+    double r = nearbyint(ldexp(a, 11 - e)); /* in [1024, 2048] */
+    int E = e - 1;
+    if (r >= 2048.0) { r = 1024.0; E += 1; }
+    if (E > 15) return (u16)(sign | 0x7C00u);
+    return (u16)(sign | (u16)(((E + 15) << 10) | ((int)r - 1024)));
+}
+
+double oracle_f16_to_f64(uint16_t h) {
+    int s = h >> 15, e = (h >> 10) & 31, m = h & 1023;
+    double v;
+    if (e == 0) v = ldexp((double)m, -24);
+    else if (e == 31) v = m ? NAN : INFINITY;
+    else v = ldexp((double)(m + 1024), e - 25);
+    return s ? -v : v;
+}
+
+uint16_t oracle_f16_add(uint16_t a, uint16_t b) {
+    return oracle_f64_to_f16(oracle_f16_to_f64(a) + oracle_f16_to_f64(b));
+}
+
+#define H_NEG_ONE ((u16)0xBC00u)
+
+static int nthreads_or_default(int n) { return n > 0 ? n : 1; }
+
+/* ------------------------------------------------------------------ */
+/* Shared greedy-join bookkeeping (cu/joinEdgeIndel.cu:321-468,          */
+/* cu/joinEdgeBitReverse.cu:356-505).  Values are compared as doubles.  */
+/* ------------------------------------------------------------------ */
+
+typedef struct {
+    u32 ntip, nnode, nedge;
+    u32 *node2cache; /* nnode, ntip = invalid */
+    u32 *cache2node; /* ntip, nnode = dead */
+    u32 *valid;      /* ascending cache indices */
+    u32 nvalid;
+    u32 *localMaxIdx;
+    u32 *rawEdge;    /* nedge*2, join order */
+} JoinBook;
+
+static int book_init(JoinBook *b, u32 ntip) {
+    b->ntip = ntip;
+    b->nnode = 2 * ntip - 1;
+    b->nedge = 2 * ntip - 2;
+    b->node2cache = (u32 *)malloc(sizeof(u32) * b->nnode);
+    b->cache2node = (u32 *)malloc(sizeof(u32) * ntip);
+    b->valid = (u32 *)malloc(sizeof(u32) * ntip);
+    b->localMaxIdx = (u32 *)calloc(ntip, sizeof(u32));
+    b->rawEdge = (u32 *)malloc(sizeof(u32) * (b->nedge ? b->nedge : 1) * 2);
+    if (!b->node2cache || !b->cache2node || !b->valid || !b->localMaxIdx || !b->rawEdge)
+        return ORACLE_ENOMEM;
+    for (u32 i = 0; i < b->nnode; i++) b->node2cache[i] = i < ntip ? i : ntip;
+    for (u32 i = 0; i < ntip; i++) { b->cache2node[i] = i; b->valid[i] = i; }
+    b->nvalid = ntip;
+    return ORACLE_OK;
+}
+
+static void book_free(JoinBook *b) {
+    free(b->node2cache); free(b->cache2node); free(b->valid);
+    free(b->localMaxIdx); free(b->rawEdge);
+}
+
+/* Removal keeps ascending order (cu/joinEdgeIndel.cu:430-437). */
+static void book_remove_valid(JoinBook *b, u32 c) {
+    u32 p = 0;
+    while (p < b->nvalid && b->valid[p] < c) p++;
+    if (p < b->nvalid && b->valid[p] == c) {
+        memmove(b->valid + p, b->valid + p + 1, sizeof(u32) * (b->nvalid - p - 1));
+        b->nvalid--;
+    }
+}
+
+/* (v, i) beats (bv, bi)?  cu/joinEdgeIndel.cu:117 */
+static inline int better(double v, u32 i, double bv, u32 bi) {
+    return v > bv || (v == bv && i < bi);
+}
+
+/*
+ * Pre-order relabel and output (cu/joinEdgeIndel.cu:488-558).  The
+ * reference looks up, for the node on top of the stack, the first not yet
+ * consumed edge (lowest index) whose parent is that node; internal node v's
+ * edges sit at 2(v-ntip) and 2(v-ntip)+1, so a per-node cursor is the same
+ * walk.  rawState(r) is the child state recorded for raw edge r; the root
+ * state is rawState(nedge).
+ */
+static int dfs_output(const JoinBook *b, const u32 *rawState, u32 rowlen,
+                      u32 *edge_out, u32 *state_out) {
+    const u32 ntip = b->ntip, nnode = b->nnode, nedge = b->nedge;
+    u32 *relabel = (u32 *)malloc(sizeof(u32) * nnode);
+    u32 *stack = (u32 *)malloc(sizeof(u32) * (nedge + 1));
+    unsigned char *cursor = (unsigned char *)calloc(nnode, 1);
+    if (!relabel || !stack || !cursor) { free(relabel); free(stack); free(cursor); return ORACLE_ENOMEM; }
+    for (u32 i = 0; i < nnode; i++) relabel[i] = i < ntip ? i : nnode;
+    memcpy(state_out, rawState + (size_t)nedge * rowlen, sizeof(u32) * rowlen);
+    u32 nstate = 1, nout = 0, count = ntip;
+    long sp = 0;
+    stack[0] = nedge; /* root node id */
+    while (sp >= 0) {
+        u32 v = stack[sp];
+        if (v < ntip || cursor[v] >= 2) { sp--; continue; }
+        u32 ei = 2 * (v - ntip) + cursor[v];
+        cursor[v]++;
+        u32 p = b->rawEdge[2 * ei], c = b->rawEdge[2 * ei + 1];
+        stack[++sp] = c;
+        if (relabel[p] == nnode) relabel[p] = count++;
+        u32 lp = relabel[p], lc;
+        if (relabel[c] == nnode) {
+            memcpy(state_out + (size_t)nstate * rowlen, rawState + (size_t)ei * rowlen, sizeof(u32) * rowlen);
+            nstate++;
+            relabel[c] = count++;
+        }
+        lc = relabel[c];
+        edge_out[2 * nout] = lp;
+        edge_out[2 * nout + 1] = lc;
+        nout++;
+    }
+    free(relabel); free(stack); free(cursor);
+    return nout == nedge ? ORACLE_OK : ORACLE_EINTERNAL;
+}
+
+/* ------------------------------------------------------------------ */
+/* joinEdgeIndel  (cu/joinEdgeIndel.cu:67-85, 87-99, 244-558)           */
+/* ------------------------------------------------------------------ */
+
+typedef struct {
+    u32 ncol;
+    const u32 *cache; /* ntip x ncol */
+    const u16 *w16;   /* nState x ncol */
+} IndelCtx;
+
+/* calculateSharedKernel (cu/joinEdgeIndel.cu:67-85) for one pair. */
+static u16 indel_score(const IndelCtx *k, u32 q, u32 c) {
+    const u32 *a = k->cache + (size_t)q * k->ncol, *r = k->cache + (size_t)c * k->ncol;
+    u16 acc = 0;
+    for (u32 i = 0; i < k->ncol; i++) {
+        u32 t = a[i];
+        if (t == r[i] && t > 1) acc = oracle_f16_add(acc, k->w16[(size_t)(t - 2) * k->ncol + i]);
+    }
+    return acc;
+}
+
+/* updateAncestralKernel (cu/joinEdgeIndel.cu:87-99). */
+static void indel_merge(u32 *a, const u32 *b, u32 n) {
+    for (u32 i = 0; i < n; i++) {
+        u32 x = a[i], y = b[i];
+        if (x == 0) a[i] = y;
+        else if (y >= 1 && x != y) a[i] = 1;
+    }
+}
+
+int oracle_join_indel(uint32_t ntip, uint32_t ncol, const uint32_t *codes,
+                      uint32_t nState, const double *w, const uint32_t *tipSize,
+                      uint32_t minSize, float minRatio, uint32_t *edge_out,
+                      uint32_t *state_out, uint64_t *stats, int nthreads) {
+    if (ntip == 0 || ncol == 0) return ORACLE_EINVAL;
+    nthreads = nthreads_or_default(nthreads);
+    for (size_t i = 0; i < (size_t)ntip * ncol; i++)
+        if (codes[i] > 1 && codes[i] - 2 >= nState) return ORACLE_ERANGE;
+    const size_t nw = (size_t)nState * ncol;
+    u16 *w16 = (u16 *)malloc(sizeof(u16) * (nw ? nw : 1));
+    u32 *cache = (u32 *)malloc(sizeof(u32) * (size_t)ntip * ncol);
+    u16 *localMax = (u16 *)malloc(sizeof(u16) * ntip);
+    u16 *shared = (u16 *)malloc(sizeof(u16) * ntip);
+    u32 nnode = 2 * ntip - 1;
+    u32 *rawState = (u32 *)malloc(sizeof(u32) * (size_t)nnode * ncol);
+    u32 *nodeSize = (u32 *)malloc(sizeof(u32) * (size_t)ntip * 2);
+    JoinBook b;
+    int st = book_init(&b, ntip);
+    if (st || !w16 || !cache || !localMax || !shared || !rawState || !nodeSize) { st = ORACLE_ENOMEM; goto done; }
+    for (size_t i = 0; i < nw; i++) w16[i] = oracle_f64_to_f16(w[i]);
+    memcpy(cache, codes, sizeof(u32) * (size_t)ntip * ncol);
+    memcpy(nodeSize, tipSize, sizeof(u32) * ntip);
+    IndelCtx k = {ncol, cache, w16};
+    u64 nStale = 0, nPairs = 0, nJoin = 0;
+
+    /* initial upper-triangle local maxima (cu/joinEdgeIndel.cu:355-369) */
+    for (u32 i = 0; i + 1 < ntip; i++) {
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+        for (long j = (long)i + 1; j < (long)ntip; j++) shared[j] = indel_score(&k, i, (u32)j);
+        double bv = -1.0;
+        u32 bi = 0;
+        for (u32 j = i + 1; j < ntip; j++) {
+            double v = oracle_f16_to_f64(shared[j]);
+            if (better(v, j, bv, bi)) { bv = v; bi = j; }
+        }
+        localMax[i] = oracle_f64_to_f16(bv);
+        b.localMaxIdx[i] = bi;
+        nPairs += ntip - i - 1;
+    }
+    localMax[ntip - 1] = H_NEG_ONE;
+
+    u32 nodeCount = ntip;
+    while (nodeCount < b.nnode) {
+        u32 j1, j2, c1, c2;
+        for (;;) {
+            double bv = -1.0;
+            u32 bi = 0;
+            for (u32 c = 0; c < ntip; c++) {
+                double v = oracle_f16_to_f64(localMax[c]);
+                if (better(v, b.cache2node[c], bv, bi)) { bv = v; bi = b.cache2node[c]; }
+            }
+            j1 = bi;
+            if (j1 >= b.nnode) { st = ORACLE_EINTERNAL; goto done; }
+            c1 = b.node2cache[j1];
+            if (c1 >= ntip) { st = ORACLE_EINTERNAL; goto done; }
+            j2 = b.localMaxIdx[c1];
+            c2 = j2 < b.nnode ? b.node2cache[j2] : ntip;
+            if (c2 < ntip) break;
+            /* stale partner: rescore c1 against every valid row (:387-399) */
+            nStale++;
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+            for (long p = 0; p < (long)b.nvalid; p++) {
+                u32 c = b.valid[p];
+                shared[c] = c == c1 ? H_NEG_ONE : indel_score(&k, c1, c);
+            }
+            nPairs += b.nvalid - 1;
+            bv = -1.0;
+            bi = 0;
+            for (u32 p = 0; p < b.nvalid; p++) {
+                u32 c = b.valid[p];
+                double v = oracle_f16_to_f64(shared[c]);
+                if (better(v, b.cache2node[c], bv, bi)) { bv = v; bi = b.cache2node[c]; }
+            }
+            localMax[c1] = oracle_f64_to_f16(bv);
+            b.localMaxIdx[c1] = bi;
+        }
+        const u32 r = nodeCount - ntip;
+        memcpy(rawState + (size_t)(2 * r) * ncol, cache + (size_t)c1 * ncol, sizeof(u32) * ncol);
+        memcpy(rawState + (size_t)(2 * r + 1) * ncol, cache + (size_t)c2 * ncol, sizeof(u32) * ncol);
+        u32 s1 = nodeSize[j1], s2 = nodeSize[j2];
+        if (s1 < minSize && (float)s1 * minRatio < (float)s2) {
+            memcpy(cache + (size_t)c1 * ncol, cache + (size_t)c2 * ncol, sizeof(u32) * ncol);
+        } else if (s2 < minSize && (float)s2 * minRatio < (float)s1) {
+            ;
+        } else {
+            indel_merge(cache + (size_t)c1 * ncol, cache + (size_t)c2 * ncol, ncol);
+        }
+        nodeSize[nodeCount] = s1 + s2;
+        b.rawEdge[4 * r] = nodeCount; b.rawEdge[4 * r + 1] = j1;
+        b.rawEdge[4 * r + 2] = nodeCount; b.rawEdge[4 * r + 3] = j2;
+        b.node2cache[j1] = ntip; b.node2cache[j2] = ntip; b.node2cache[nodeCount] = c1;
+        b.cache2node[c1] = nodeCount; b.cache2node[c2] = b.nnode;
+        book_remove_valid(&b, c2);
+        /* new node against every valid row, strict improvement (:439-463) */
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+        for (long p = 0; p < (long)b.nvalid; p++) {
+            u32 c = b.valid[p];
+            if (c != c1) shared[c] = indel_score(&k, c1, c);
+        }
+        nPairs += b.nvalid - 1;
+        for (u32 p = 0; p < b.nvalid; p++) {
+            u32 c = b.valid[p];
+            if (c == c1) continue;
+            if (oracle_f16_to_f64(shared[c]) > oracle_f16_to_f64(localMax[c])) {
+                localMax[c] = shared[c];
+                b.localMaxIdx[c] = nodeCount;
+            }
+        }
+        localMax[c1] = H_NEG_ONE;
+        localMax[c2] = H_NEG_ONE;
+        nodeCount++;
+        nJoin++;
+    }
+    memcpy(rawState + (size_t)(b.nnode - 1) * ncol, cache + (size_t)b.node2cache[nodeCount - 1] * ncol,
+           sizeof(u32) * ncol);
+    st = dfs_output(&b, rawState, ncol, edge_out, state_out);
+    if (stats) { stats[0] = nStale; stats[1] = nPairs; stats[2] = nJoin; }
+done:
+    book_free(&b);
+    free(w16); free(cache); free(localMax); free(shared); free(rawState); free(nodeSize);
+    return st;
+}
+
+/* ------------------------------------------------------------------ */
+/* joinEdgeBitReverse (cu/joinEdgeBitReverse.cu:53-121, 285-597)       */
+/* ------------------------------------------------------------------ */
+
+typedef struct {
+    u32 nbin;
+    const u32 *seq;
+    const float *wf;
+} BitCtx;
+
+/* calculateSharedKernel: float sum over the query's set bits in ascending
+ * order where the candidate bit is set (cu/joinEdgeBitReverse.cu:61-69,
+ * bit list built by calculateSharedPacked :235-244). */
+static float bit_score(const BitCtx *k, u32 q, u32 c) {
+    const u32 *a = k->seq + (size_t)q * k->nbin, *r = k->seq + (size_t)c * k->nbin;
+    float acc = 0.0f;
+    for (u32 j = 0; j < k->nbin; j++) {
+        u32 v = a[j] & r[j];
+        while (v) {
+            int bit = __builtin_ctz(v);
+            acc += k->wf[j * 32 + bit];
+            v &= v - 1;
+        }
+    }
+    return acc;
+}
+
+int oracle_join_bit(uint32_t ntip, uint32_t nbin, const uint32_t *words,
+                    const double *w, int ancestralType, uint32_t *edge_out,
+                    uint32_t *state_out, uint64_t *stats, int nthreads) {
+    if (ntip == 0 || nbin == 0) return ORACLE_EINVAL;
+    nthreads = nthreads_or_default(nthreads);
+    const u32 nsite = nbin * 32;
+    float *wf = (float *)malloc(sizeof(float) * nsite);
+    u32 *seq = (u32 *)malloc(sizeof(u32) * (size_t)ntip * nbin);
+    u32 *bis = (u32 *)calloc((size_t)ntip * nbin, sizeof(u32));
+    float *localMax = (float *)malloc(sizeof(float) * ntip);
+    float *shared = (float *)malloc(sizeof(float) * ntip);
+    u32 nnode = 2 * ntip - 1;
+    u32 *rawState = (u32 *)malloc(sizeof(u32) * (size_t)nnode * nbin);
+    JoinBook b;
+    int st = book_init(&b, ntip);
+    if (st || !wf || !seq || !bis || !localMax || !shared || !rawState) { st = ORACLE_ENOMEM; goto done; }
+    for (u32 i = 0; i < nsite; i++) wf[i] = (float)w[i];
+    memcpy(seq, words, sizeof(u32) * (size_t)ntip * nbin);
+    BitCtx k = {nbin, seq, wf};
+    u64 nStale = 0, nPairs = 0, nJoin = 0;
+
+    for (u32 i = 0; i + 1 < ntip; i++) {
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+        for (long j = (long)i + 1; j < (long)ntip; j++) shared[j] = bit_score(&k, i, (u32)j);
+        float bv = -1.0f;
+        u32 bi = 0;
+        for (u32 j = i + 1; j < ntip; j++)
+            if (better(shared[j], j, bv, bi)) { bv = shared[j]; bi = j; }
+        localMax[i] = bv;
+        b.localMaxIdx[i] = bi;
+        nPairs += ntip - i - 1;
+    }
+    localMax[ntip - 1] = -1.0f;
+
+    u32 nodeCount = ntip;
+    while (nodeCount < b.nnode) {
+        u32 j1, j2, c1, c2;
+        for (;;) {
+            float bv = -1.0f;
+            u32 bi = 0;
+            for (u32 c = 0; c < ntip; c++)
+                if (better(localMax[c], b.cache2node[c], bv, bi)) { bv = localMax[c]; bi = b.cache2node[c]; }
+            j1 = bi;
+            if (j1 >= b.nnode) { st = ORACLE_EINTERNAL; goto done; }
+            c1 = b.node2cache[j1];
+            if (c1 >= ntip) { st = ORACLE_EINTERNAL; goto done; }
+            j2 = b.localMaxIdx[c1];
+            c2 = j2 < b.nnode ? b.node2cache[j2] : ntip;
+            if (c2 < ntip) break;
+            nStale++;
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+            for (long p = 0; p < (long)b.nvalid; p++) {
+                u32 c = b.valid[p];
+                shared[c] = c == c1 ? -1.0f : bit_score(&k, c1, c);
+            }
+            nPairs += b.nvalid - 1;
+            bv = -1.0f;
+            bi = 0;
+            for (u32 p = 0; p < b.nvalid; p++) {
+                u32 c = b.valid[p];
+                if (better(shared[c], b.cache2node[c], bv, bi)) { bv = shared[c]; bi = b.cache2node[c]; }
+            }
+            localMax[c1] = bv;
+            b.localMaxIdx[c1] = bi;
+        }
+        const u32 r = nodeCount - ntip;
+        /* nodeStateOutputKernel: seq & ~bistate (:115-121, :436-443) */
+        for (u32 j = 0; j < nbin; j++) {
+            rawState[(size_t)(2 * r) * nbin + j] = seq[(size_t)c1 * nbin + j] & ~bis[(size_t)c1 * nbin + j];
+            rawState[(size_t)(2 * r + 1) * nbin + j] = seq[(size_t)c2 * nbin + j] & ~bis[(size_t)c2 * nbin + j];
+        }
+        for (u32 j = 0; j < nbin; j++) {
+            u32 s1 = seq[(size_t)c1 * nbin + j], s2 = seq[(size_t)c2 * nbin + j];
+            u32 b1 = bis[(size_t)c1 * nbin + j], b2 = bis[(size_t)c2 * nbin + j];
+            if (ancestralType == 0) { /* updateAncestralKernel (:77-95) */
+                u32 diff = s1 ^ s2;
+                u32 conflict = diff & (b1 | b2);
+                seq[(size_t)c1 * nbin + j] = (s1 | s2) & ~conflict;
+                bis[(size_t)c1 * nbin + j] = (diff & ~(b1 ^ b2)) | (b1 & b2);
+            } else { /* updateAncestralKernel2 (:97-113) */
+                seq[(size_t)c1 * nbin + j] = (s1 & s2) | (b1 & s2) | (b2 & s1);
+                bis[(size_t)c1 * nbin + j] = (s1 ^ s2) & ~(b1 | b2);
+            }
+        }
+        b.rawEdge[4 * r] = nodeCount; b.rawEdge[4 * r + 1] = j1;
+        b.rawEdge[4 * r + 2] = nodeCount; b.rawEdge[4 * r + 3] = j2;
+        b.node2cache[j1] = ntip; b.node2cache[j2] = ntip; b.node2cache[nodeCount] = c1;
+        b.cache2node[c1] = nodeCount; b.cache2node[c2] = b.nnode;
+        book_remove_valid(&b, c2);
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+        for (long p = 0; p < (long)b.nvalid; p++) {
+            u32 c = b.valid[p];
+            if (c != c1) shared[c] = bit_score(&k, c1, c);
+        }
+        nPairs += b.nvalid - 1;
+        for (u32 p = 0; p < b.nvalid; p++) {
+            u32 c = b.valid[p];
+            if (c == c1) continue;
+            if (shared[c] > localMax[c]) { localMax[c] = shared[c]; b.localMaxIdx[c] = nodeCount; }
+        }
+        localMax[c1] = -1.0f;
+        localMax[c2] = -1.0f;
+        nodeCount++;
+        nJoin++;
+    }
+    {
+        u32 c = b.node2cache[nodeCount - 1];
+        for (u32 j = 0; j < nbin; j++)
+            rawState[(size_t)(b.nnode - 1) * nbin + j] = seq[(size_t)c * nbin + j] & ~bis[(size_t)c * nbin + j];
+    }
+    st = dfs_output(&b, rawState, nbin, edge_out, state_out);
+    if (stats) { stats[0] = nStale; stats[1] = nPairs; stats[2] = nJoin; }
+done:
+    book_free(&b);
+    free(wf); free(seq); free(bis); free(localMax); free(shared); free(rawState);
+    return st;
+}
+
+/* ------------------------------------------------------------------ */
+/* nodeKeepIndel (cu/nodeKeepIndel.cu:32-48,130-152)                    */
+/* nodeKeepBit   (cu/nodeKeepBit.cu:33-51,186-211)                      */
+/* ------------------------------------------------------------------ */
+
+static int node_keep_common(int bitmode, u32 nnodeRows, u32 ncol, const u32 *nodeState,
+                            u32 nedge, const u32 *edge, u32 nRetain, const u32 *outmat,
+                            u32 cutoff, u32 *out_nodes, u32 *nout) {
+    const u32 ntip = nnodeRows + 1;
+    u32 currentNode = ntip - 1, flag = 0, n = 0;
+    for (u32 i = 0; i < nedge; i++) {
+        u32 parent = edge[2 * i], child = edge[2 * i + 1];
+        if (!(child + 1 > ntip)) continue;
+        if (flag == 1 && currentNode <= parent) continue;
+        u32 row = child - ntip;
+        if (row >= nnodeRows) return ORACLE_ERANGE;
+        const u32 *ref = nodeState + (size_t)row * ncol;
+        flag = 1;
+        for (u32 j = 0; j < nRetain && flag; j++) {
+            const u32 *o = outmat + (size_t)j * ncol;
+            u32 cnt = 0;
+            if (bitmode) {
+                for (u32 t = 0; t < ncol; t++) cnt += (u32)__builtin_popcount(ref[t] & ~o[t]);
+            } else {
+                for (u32 t = 0; t < ncol; t++)
+                    if (ref[t] > 1 && o[t] != ref[t] && o[t] >= 1) cnt++;
+            }
+            if (cnt < cutoff) flag = 0;
+        }
+        if (flag == 1) { currentNode = child; out_nodes[n++] = child; }
+    }
+    *nout = n;
+    return ORACLE_OK;
+}
+
+int oracle_node_keep_indel(uint32_t nnodeRows, uint32_t ncol, const uint32_t *nodeState,
+                           uint32_t nedge, const uint32_t *edge, uint32_t nRetain,
+                           const uint32_t *outmat, uint32_t cutoff,
+                           uint32_t *out_nodes, uint32_t *nout) {
+    return node_keep_common(0, nnodeRows, ncol, nodeState, nedge, edge, nRetain, outmat, cutoff, out_nodes, nout);
+}
+
+int oracle_node_keep_bit(uint32_t nnodeRows, uint32_t nbin, const uint32_t *nodeState,
+                         uint32_t nedge, const uint32_t *edge, uint32_t nRetain,
+                         const uint32_t *outmat, uint32_t cutoff,
+                         uint32_t *out_nodes, uint32_t *nout) {
+    return node_keep_common(1, nnodeRows, nbin, nodeState, nedge, edge, nRetain, outmat, cutoff, out_nodes, nout);
+}
+
+/* ------------------------------------------------------------------ */
+/* radiusNeighbor (cu/radiusNeighbor.cu:26-50, 162-437).  The output of  */
+/* the host mirror loop (:383-425) is, for every row i, the ascending   */
+/* list {j : score(i,j) >= radius}; the score is symmetric because both */
+/* directions add the same weights in the same ascending bit order.     */
+/* ------------------------------------------------------------------ */
+
+static float radius_bit_score(const u32 *bmat, u32 nrow, u32 ntip, const float *wf, u32 q, u32 c) {
+    float acc = 0.0f;
+    for (u32 j = 0; j < nrow; j++) {
+        u32 v = bmat[(size_t)j * ntip + q] & bmat[(size_t)j * ntip + c];
+        while (v) {
+            int bit = __builtin_ctz(v);
+            acc += wf[j * 32 + bit];
+            v &= v - 1;
+        }
+    }
+    return acc;
+}
+
+/* Emit lists from a predicate evaluated per (i,j). */
+typedef int (*pair_pred)(const void *ctx, u32 i, u32 j);
+
+static int emit_lists(u32 ntip, pair_pred pred, const void *ctx, u32 *counts, u32 *idx,
+                      u64 cap, u64 *total, int nthreads) {
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 16)
+    for (long i = 0; i < (long)ntip; i++) {
+        u32 n = 0;
+        for (u32 j = 0; j < ntip; j++) n += pred(ctx, (u32)i, j) ? 1u : 0u;
+        counts[i] = n;
+    }
+    u64 tot = 0;
+    for (u32 i = 0; i < ntip; i++) tot += counts[i];
+    if (total) *total = tot;
+    if (!idx) return ORACLE_OK;
+    if (tot > cap) return ORACLE_ERANGE;
+    u64 *off = (u64 *)malloc(sizeof(u64) * (ntip ? ntip : 1));
+    if (!off) return ORACLE_ENOMEM;
+    u64 acc = 0;
+    for (u32 i = 0; i < ntip; i++) { off[i] = acc; acc += counts[i]; }
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 16)
+    for (long i = 0; i < (long)ntip; i++) {
+        u64 o = off[i];
+        for (u32 j = 0; j < ntip; j++)
+            if (pred(ctx, (u32)i, j)) idx[o++] = j;
+    }
+    free(off);
+    return ORACLE_OK;
+}
+
+typedef struct { const u32 *bmat; u32 nrow, ntip; const float *wf; float radius; } RbCtx;
+static int rb_pred(const void *p, u32 i, u32 j) {
+    const RbCtx *c = (const RbCtx *)p;
+    return radius_bit_score(c->bmat, c->nrow, c->ntip, c->wf, i, j) >= c->radius;
+}
+
+int oracle_radius_bit(uint32_t nrow, uint32_t ntip, const uint32_t *bmat,
+                      const double *w, int32_t radius, uint32_t *counts,
+                      uint32_t *idx, uint64_t idx_cap, uint64_t *total, int nthreads) {
+    if (ntip == 0 || nrow == 0) return ORACLE_EINVAL;
+    nthreads = nthreads_or_default(nthreads);
+    float *wf = (float *)malloc(sizeof(float) * nrow * 32);
+    if (!wf) return ORACLE_ENOMEM;
+    for (u32 i = 0; i < nrow * 32; i++) wf[i] = (float)w[i];
+    RbCtx c = {bmat, nrow, ntip, wf, (float)radius};
+    int st = emit_lists(ntip, rb_pred, &c, counts, idx, idx_cap, total, nthreads);
+    free(wf);
+    return st;
+}
+
+/* radiusNeighborDNA (cu/radiusNeighborDNA.cu:27-87): low nibble of each
+ * fasta2bin byte, count of positions whose nibbles intersect. */
+static u32 dna_count(const u32 *raw, u32 nbinRaw, u32 q, u32 c) {
+    const u32 *a = raw + (size_t)q * nbinRaw, *b = raw + (size_t)c * nbinRaw;
+    u32 n = 0;
+    for (u32 t = 0; t < nbinRaw; t++) {
+        u32 v = a[t] & b[t] & 0x0F0F0F0Fu;
+        n += ((v & 0xFFu) != 0) + ((v & 0xFF00u) != 0) + ((v & 0xFF0000u) != 0) + ((v & 0xFF000000u) != 0);
+    }
+    return n;
+}
+
+typedef struct { const u32 *raw; u32 nbinRaw; u32 radius; } RdCtx;
+static int rd_pred(const void *p, u32 i, u32 j) {
+    const RdCtx *c = (const RdCtx *)p;
+    return dna_count(c->raw, c->nbinRaw, i, j) >= c->radius;
+}
+
+int oracle_radius_dna(uint32_t ntip, uint32_t nbinRaw, const uint32_t *raw,
+                      uint32_t radius, uint32_t *counts, uint32_t *idx,
+                      uint64_t idx_cap, uint64_t *total, int nthreads) {
+    if (ntip == 0 || nbinRaw == 0) return ORACLE_EINVAL;
+    RdCtx c = {raw, nbinRaw, radius};
+    return emit_lists(ntip, rd_pred, &c, counts, idx, idx_cap, total, nthreads_or_default(nthreads));
+}
+
+/* tryRadius (cu/tryRadius.cu:26-50,122-158).  Threads past ntip in the last
+ * 128-thread block score 0 and join the ballot, so a radius <= 0 adds
+ * ceil(ntip/128)*128 - ntip to every count. */
+int oracle_try_radius_bit(uint32_t nrow, uint32_t ntip, const uint32_t *bmat,
+                          const double *w, int32_t radius, uint32_t nrep,
+                          const uint32_t *qidx, uint32_t *counts, int nthreads) {
+    if (ntip == 0 || nrow == 0) return ORACLE_EINVAL;
+    nthreads = nthreads_or_default(nthreads);
+    float *wf = (float *)malloc(sizeof(float) * nrow * 32);
+    if (!wf) return ORACLE_ENOMEM;
+    for (u32 i = 0; i < nrow * 32; i++) wf[i] = (float)w[i];
+    const float r = (float)radius;
+    const u32 pad = ((ntip + 127u) / 128u) * 128u - ntip;
+    int bad = 0;
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
+    for (long t = 0; t < (long)nrep; t++) {
+        u32 q = qidx[t];
+        if (q >= ntip) { bad = 1; continue; }
+        u32 n = 0;
+        for (u32 j = 0; j < ntip; j++) n += radius_bit_score(bmat, nrow, ntip, wf, q, j) >= r;
+        if (0.0f >= r) n += pad;
+        counts[t] = n;
+    }
+    free(wf);
+    return bad ? ORACLE_ERANGE : ORACLE_OK;
+}
+
+/* tryRadiusDNA (cu/tryRadiusDNA.cu:45-74,139-148). */
+int oracle_try_radius_dna(uint32_t ntip, uint32_t nbinRaw, const uint32_t *raw,
+                          uint32_t radius, uint32_t nrep, const uint32_t *qidx,
+                          uint32_t *counts, int nthreads) {
+    if (ntip == 0 || nbinRaw == 0) return ORACLE_EINVAL;
+    int bad = 0;
+#pragma omp parallel for num_threads(nthreads_or_default(nthreads)) schedule(dynamic, 1)
+    for (long t = 0; t < (long)nrep; t++) {
+        u32 q = qidx[t];
+        if (q >= ntip) { bad = 1; continue; }
+        u32 n = 0;
+        for (u32 j = 0; j < ntip; j++) n += dna_count(raw, nbinRaw, q, j) >= radius;
+        counts[t] = n;
+    }
+    return bad ? ORACLE_ERANGE : ORACLE_OK;
+}
+
+/* ------------------------------------------------------------------ */
+/* TransferDisStream (cu/TransferDisStream.cu:22-128,193-339).           */
+/* The kernel reduces 8x8 tiles: for each x and each aligned group of 8  */
+/* y rows it keeps A = min popc(x^y) and B = min popc(x^~y) separately    */
+/* (absent rows contribute 32*ncol to both), then atomicMin(min(A,       */
+/* B - (32*ncol - ntip))) with u32 wrap-around; symmetric for ymin over  */
+/* groups of 8 x rows.  xmin/ymin start at 32*ncol.                      */
+/* ------------------------------------------------------------------ */
+
+static inline u32 xor_pop(const u32 *a, const u32 *b, u32 ncol) {
+    u32 d = 0;
+    for (u32 t = 0; t < ncol; t++) d += (u32)__builtin_popcount(a[t] ^ b[t]);
+    return d;
+}
+
+static void tdis_side(u32 nA, u32 nB, u32 ncol, u32 ntip, const u32 *A, const u32 *B,
+                      u32 *outmin, int nthreads) {
+    const u32 full = 32u * ncol, pad = 32u * ncol - ntip;
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 8)
+    for (long a = 0; a < (long)nA; a++) {
+        u32 best = full;
+        for (u32 g = 0; g < nB; g += 8) {
+            u32 mA = full, mB = full;
+            for (u32 k = g; k < g + 8 && k < nB; k++) {
+                u32 d = xor_pop(A + (size_t)a * ncol, B + (size_t)k * ncol, ncol);
+                u32 comp = full - d;
+                if (d < mA) mA = d;
+                if (comp < mB) mB = comp;
+            }
+            u32 t2 = mB - pad;
+            u32 v = mA > t2 ? t2 : mA;
+            if (v < best) best = v;
+        }
+        outmin[a] = best;
+    }
+}
+
+static void row_size(u32 n, u32 ncol, u32 ntip, const u32 *m, u32 *size) {
+    for (u32 i = 0; i < n; i++) {
+        u32 c = 0;
+        for (u32 t = 0; t < ncol; t++) c += (u32)__builtin_popcount(m[(size_t)i * ncol + t]);
+        if (c > ntip - c) c = ntip - c;
+        size[i] = c;
+    }
+}
+
+int oracle_transfer_dis(uint32_t nrow_y, uint32_t nrow_x, uint32_t ncol, uint32_t ntip,
+                        const uint32_t *y, const uint32_t *x, uint32_t *ymin,
+                        uint32_t *ysize, uint32_t *xmin, uint32_t *xsize, int nthreads) {
+    if (ncol == 0) return ORACLE_EINVAL;
+    nthreads = nthreads_or_default(nthreads);
+    tdis_side(nrow_x, nrow_y, ncol, ntip, x, y, xmin, nthreads);
+    tdis_side(nrow_y, nrow_x, ncol, ntip, y, x, ymin, nthreads);
+    row_size(nrow_y, ncol, ntip, y, ysize);
+    row_size(nrow_x, ncol, ntip, x, xsize);
+    return ORACLE_OK;
+}

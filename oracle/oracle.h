@@ -1,0 +1,91 @@
+/*
+ * CPU oracle for the CasPhy tree-building hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Nothing in the shipped library or the drop-in
+ * executables links this code.  It is loaded by tests/, by
+ * __graft_entry__.smoke() as the checker, and by bench.py's cpu_baseline /
+ * --impl reference leg as the timed CPU restatement ("port") of the
+ * reference algorithm.
+ *
+ * Every function restates the HOST + KERNEL semantics of one reference
+ * executable (file:line cited at each definition in oracle.c), including its
+ * arithmetic type (binary16 sums for the indel join, binary32 sums for the
+ * bit join and bit radius search) and its tie-breaking rules, so outputs are
+ * byte-identical to what the reference writes on the same inputs.
+ *
+ * Status codes: 0 ok, otherwise one of the CASPHY_E* values in
+ * include/casphy.h (mirrored here so the oracle builds standalone).
+ */
+#ifndef CASPHY_ORACLE_H
+#define CASPHY_ORACLE_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ORACLE_OK 0
+#define ORACLE_EINVAL 1
+#define ORACLE_ERANGE 2
+#define ORACLE_ENOMEM 3
+#define ORACLE_EINTERNAL 9
+
+/* binary16 helpers (exposed for unit tests) */
+uint16_t oracle_f64_to_f16(double x);
+double oracle_f16_to_f64(uint16_t h);
+uint16_t oracle_f16_add(uint16_t a, uint16_t b);
+
+/* joinEdgeIndel.  codes: ntip x ncol row-major (0 missing, 1 unedited, >=2
+ * allele).  w: nState x ncol doubles (index (code-2)*ncol + site).
+ * Outputs: edge_out 2*(2*ntip-2) u32 (pre-order relabelled), state_out
+ * max(ntip-1,1) x ncol u32 (root first).  stats (nullable): [0] stale
+ * recomputes, [1] pair-scores evaluated, [2] joins. */
+int oracle_join_indel(uint32_t ntip, uint32_t ncol, const uint32_t *codes,
+                      uint32_t nState, const double *w, const uint32_t *tipSize,
+                      uint32_t minSize, float minRatio, uint32_t *edge_out,
+                      uint32_t *state_out, uint64_t *stats, int nthreads);
+
+/* joinEdgeBitReverse.  words: ntip x nbin row-major bit rows.  w: nbin*32
+ * doubles.  ancestralType 0 or 1 (any non-zero value selects rule 1). */
+int oracle_join_bit(uint32_t ntip, uint32_t nbin, const uint32_t *words,
+                    const double *w, int ancestralType, uint32_t *edge_out,
+                    uint32_t *state_out, uint64_t *stats, int nthreads);
+
+/* nodeKeepIndel / nodeKeepBit.  Writes retained node ids (in the order the
+ * reference prints them) to out_nodes, count to *nout. */
+int oracle_node_keep_indel(uint32_t nnodeRows, uint32_t ncol, const uint32_t *nodeState,
+                           uint32_t nedge, const uint32_t *edge, uint32_t nRetain,
+                           const uint32_t *outmat, uint32_t cutoff,
+                           uint32_t *out_nodes, uint32_t *nout);
+int oracle_node_keep_bit(uint32_t nnodeRows, uint32_t nbin, const uint32_t *nodeState,
+                         uint32_t nedge, const uint32_t *edge, uint32_t nRetain,
+                         const uint32_t *outmat, uint32_t cutoff,
+                         uint32_t *out_nodes, uint32_t *nout);
+
+/* radiusNeighbor.  bmat: word-plane-major (nrow words x ntip).  counts[ntip];
+ * idx (nullable) receives the concatenated ascending lists. */
+int oracle_radius_bit(uint32_t nrow, uint32_t ntip, const uint32_t *bmat,
+                      const double *w, int32_t radius, uint32_t *counts,
+                      uint32_t *idx, uint64_t idx_cap, uint64_t *total,
+                      int nthreads);
+/* radiusNeighborDNA.  raw: ntip x nbinRaw fasta2bin words (4 codes/word). */
+int oracle_radius_dna(uint32_t ntip, uint32_t nbinRaw, const uint32_t *raw,
+                      uint32_t radius, uint32_t *counts, uint32_t *idx,
+                      uint64_t idx_cap, uint64_t *total, int nthreads);
+/* tryRadius / tryRadiusDNA with given query indices. */
+int oracle_try_radius_bit(uint32_t nrow, uint32_t ntip, const uint32_t *bmat,
+                          const double *w, int32_t radius, uint32_t nrep,
+                          const uint32_t *qidx, uint32_t *counts, int nthreads);
+int oracle_try_radius_dna(uint32_t ntip, uint32_t nbinRaw, const uint32_t *raw,
+                          uint32_t radius, uint32_t nrep, const uint32_t *qidx,
+                          uint32_t *counts, int nthreads);
+
+/* TransferDisStream. */
+int oracle_transfer_dis(uint32_t nrow_y, uint32_t nrow_x, uint32_t ncol, uint32_t ntip,
+                        const uint32_t *y, const uint32_t *x, uint32_t *ymin,
+                        uint32_t *ysize, uint32_t *xmin, uint32_t *xsize,
+                        int nthreads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,161 @@
+"""ctypes binding of the CPU oracle (oracle.c) -- TEST INFRASTRUCTURE.
+
+Imported only by tests/, __graft_entry__.smoke() (as the checker) and
+bench.py's CPU legs.  Builds liboracle.so with `make -C oracle` when it is
+missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+_u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_u64p = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            subprocess.run(["make", "-C", _HERE, "liboracle.so"], check=True,
+                           stdout=subprocess.DEVNULL)
+        L = C.CDLL(path)
+        u32, i32, f32, i = C.c_uint32, C.c_int32, C.c_float, C.c_int
+        L.oracle_f64_to_f16.argtypes = [C.c_double]
+        L.oracle_f64_to_f16.restype = C.c_uint16
+        L.oracle_f16_to_f64.argtypes = [C.c_uint16]
+        L.oracle_f16_to_f64.restype = C.c_double
+        L.oracle_f16_add.argtypes = [C.c_uint16, C.c_uint16]
+        L.oracle_f16_add.restype = C.c_uint16
+        L.oracle_join_indel.argtypes = [u32, u32, _u32p, u32, _f64p, _u32p, u32, f32,
+                                        _u32p, _u32p, _u64p, i]
+        L.oracle_join_bit.argtypes = [u32, u32, _u32p, _f64p, i, _u32p, _u32p, _u64p, i]
+        for name in ("oracle_node_keep_indel", "oracle_node_keep_bit"):
+            getattr(L, name).argtypes = [u32, u32, _u32p, u32, _u32p, u32, _u32p, u32,
+                                         _u32p, C.POINTER(u32)]
+        L.oracle_radius_bit.argtypes = [u32, u32, _u32p, _f64p, i32, _u32p, C.c_void_p,
+                                        C.c_uint64, C.POINTER(C.c_uint64), i]
+        L.oracle_radius_dna.argtypes = [u32, u32, _u32p, u32, _u32p, C.c_void_p,
+                                        C.c_uint64, C.POINTER(C.c_uint64), i]
+        L.oracle_try_radius_bit.argtypes = [u32, u32, _u32p, _f64p, i32, u32, _u32p, _u32p, i]
+        L.oracle_try_radius_dna.argtypes = [u32, u32, _u32p, u32, u32, _u32p, _u32p, i]
+        L.oracle_transfer_dis.argtypes = [u32, u32, u32, u32, _u32p, _u32p, _u32p, _u32p,
+                                          _u32p, _u32p, i]
+        _LIB = L
+    return _LIB
+
+
+def _chk(st, what):
+    if st != 0:
+        raise RuntimeError(f"oracle {what} failed with status {st}")
+
+
+def _u32(a):
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+def join_indel(codes, nstate, w, tip_size=None, min_size=0, min_ratio=2.0, nthreads=0):
+    codes = _u32(codes)
+    ntip, ncol = codes.shape
+    w = np.ascontiguousarray(w, dtype=np.float64).reshape(-1)
+    ts = _u32(np.ones(ntip) if tip_size is None else tip_size)
+    nedge = 2 * ntip - 2
+    edge = np.zeros(max(nedge, 1) * 2, dtype=np.uint32)
+    state = np.zeros(max(ntip - 1, 1) * ncol, dtype=np.uint32)
+    stats = np.zeros(3, dtype=np.uint64)
+    _chk(lib().oracle_join_indel(ntip, ncol, codes, nstate, w, ts, min_size, min_ratio,
+                                 edge, state, stats, nthreads or os.cpu_count()), "join_indel")
+    return edge[: 2 * nedge].reshape(nedge, 2), state.reshape(-1, ncol), stats
+
+
+def join_bit(words, w=None, ancestral_type=1, nthreads=0):
+    words = _u32(words)
+    ntip, nbin = words.shape
+    w = np.ones(nbin * 32) if w is None else w
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    nedge = 2 * ntip - 2
+    edge = np.zeros(max(nedge, 1) * 2, dtype=np.uint32)
+    state = np.zeros(max(ntip - 1, 1) * nbin, dtype=np.uint32)
+    stats = np.zeros(3, dtype=np.uint64)
+    _chk(lib().oracle_join_bit(ntip, nbin, words, w, ancestral_type, edge, state, stats,
+                               nthreads or os.cpu_count()), "join_bit")
+    return edge[: 2 * nedge].reshape(nedge, 2), state.reshape(-1, nbin), stats
+
+
+def node_keep(node_state, edge, outmat, cutoff, bit=False):
+    node_state, edge, outmat = _u32(node_state), _u32(edge), _u32(outmat)
+    nnode, ncol = node_state.shape
+    out = np.zeros(max(edge.shape[0], 1), dtype=np.uint32)
+    n = C.c_uint32(0)
+    f = lib().oracle_node_keep_bit if bit else lib().oracle_node_keep_indel
+    _chk(f(nnode, ncol, node_state, edge.shape[0], edge.reshape(-1), outmat.shape[0],
+           outmat.reshape(-1) if outmat.size else np.zeros(1, np.uint32), cutoff, out,
+           C.byref(n)), "node_keep")
+    return out[: n.value].copy()
+
+
+def radius_bit(bmat, w, radius, nthreads=0):
+    """bmat: (nrow words, ntip) word-plane-major.  Returns (counts, idx)."""
+    bmat = _u32(bmat)
+    nrow, ntip = bmat.shape
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    counts = np.zeros(ntip, dtype=np.uint32)
+    tot = C.c_uint64(0)
+    L = lib()
+    nt = nthreads or os.cpu_count()
+    _chk(L.oracle_radius_bit(nrow, ntip, bmat, w, radius, counts, None, 0, C.byref(tot), nt), "radius")
+    idx = np.zeros(max(tot.value, 1), dtype=np.uint32)
+    _chk(L.oracle_radius_bit(nrow, ntip, bmat, w, radius, counts, idx.ctypes.data_as(C.c_void_p),
+                             tot.value, C.byref(tot), nt), "radius")
+    return counts, idx[: tot.value]
+
+
+def radius_dna(raw, radius, nthreads=0):
+    raw = _u32(raw)
+    ntip, nb = raw.shape
+    counts = np.zeros(ntip, dtype=np.uint32)
+    tot = C.c_uint64(0)
+    L = lib()
+    nt = nthreads or os.cpu_count()
+    _chk(L.oracle_radius_dna(ntip, nb, raw, radius, counts, None, 0, C.byref(tot), nt), "radius_dna")
+    idx = np.zeros(max(tot.value, 1), dtype=np.uint32)
+    _chk(L.oracle_radius_dna(ntip, nb, raw, radius, counts, idx.ctypes.data_as(C.c_void_p),
+                             tot.value, C.byref(tot), nt), "radius_dna")
+    return counts, idx[: tot.value]
+
+
+def try_radius_bit(bmat, w, radius, qidx, nthreads=0):
+    bmat, qidx = _u32(bmat), _u32(qidx)
+    nrow, ntip = bmat.shape
+    counts = np.zeros(len(qidx), dtype=np.uint32)
+    _chk(lib().oracle_try_radius_bit(nrow, ntip, bmat, np.ascontiguousarray(w, dtype=np.float64),
+                                     radius, len(qidx), qidx, counts, nthreads or os.cpu_count()),
+         "try_radius")
+    return counts
+
+
+def try_radius_dna(raw, radius, qidx, nthreads=0):
+    raw, qidx = _u32(raw), _u32(qidx)
+    counts = np.zeros(len(qidx), dtype=np.uint32)
+    _chk(lib().oracle_try_radius_dna(raw.shape[0], raw.shape[1], raw, radius, len(qidx), qidx,
+                                     counts, nthreads or os.cpu_count()), "try_radius_dna")
+    return counts
+
+
+def transfer_dis(y, x, ntip, nthreads=0):
+    y, x = _u32(y), _u32(x)
+    ny, ncol = y.shape
+    nx = x.shape[0]
+    ymin, ysize = np.zeros(ny, np.uint32), np.zeros(ny, np.uint32)
+    xmin, xsize = np.zeros(nx, np.uint32), np.zeros(nx, np.uint32)
+    _chk(lib().oracle_transfer_dis(ny, nx, ncol, ntip, y, x, ymin, ysize, xmin, xsize,
+                                   nthreads or os.cpu_count()), "transfer_dis")
+    return ymin, ysize, xmin, xsize
