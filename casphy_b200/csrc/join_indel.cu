@@ -1,0 +1,1033 @@
+// Greedy shared-mutation join of indel-coded cells on B200.
+//
+// Replaces cu/joinEdgeIndel.cu.  Same tree, same bytes; different machine
+// mapping:
+//
+//  * Scores.  score(q, c) = sum over sites i with q_i == c_i and q_i > 1 of
+//    w[(q_i-2)*ncol + i], accumulated in binary16 in ascending site order
+//    (cu/joinEdgeIndel.cu:73-79).  When every binary16 weight is a
+//    non-negative integer and the largest reachable sum is <= 2048, all
+//    partial sums are exact, so an integer count (in packed 16-bit lanes)
+//    gives identical values; otherwise the kernels add binary16 in site order
+//    per candidate, as the reference does.
+//  * Layout.  Cell codes live twice in HBM as u16: row-major by node (for
+//    merges and output) and column-major by slot (site-major), so a query
+//    reads only the columns of its own edited sites, 16 bytes (8 candidates)
+//    per thread per site, fully coalesced.
+//  * Initial local maxima (cu/joinEdgeIndel.cu:355-369) are one persistent
+//    launch over (candidate chunk, query) tiles in chunk-major order: a 4096-
+//    candidate chunk stays in L2 while every earlier query streams it, and the
+//    per-query best is merged with a 64-bit atomicMax on (score, ~node) keys.
+//  * The join loop (cu/joinEdgeIndel.cu:376-468) is one cooperative launch,
+//    one CTA per SM, each owning a contiguous slot range.  Per join every CTA
+//    redundantly derives the global best from the per-CTA records of the
+//    previous phase, merges the two children, builds the query site list in
+//    shared memory, scores its own slots and updates their local maxima; a
+//    grid barrier (bounded wait) ends the phase.  A stale partner costs a
+//    scoring phase plus an update phase, exactly like the reference's
+//    recompute-and-retry.  Dead slots are squeezed out of the column matrix
+//    whenever fewer than 3/4 of the slots are alive.
+//  * Pre-order relabelling (cu/joinEdgeIndel.cu:488-558) walks the 2(N-1)
+//    raw edges on the host in O(N) and gathers the state rows on device.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "runtime.h"
+
+namespace casphy {
+namespace indel {
+
+constexpr int kThreads = 512;
+constexpr int kG = 8;                       // candidates per thread (one uint4 of u16)
+constexpr int kCap = kThreads * kG;         // candidates per pass
+constexpr u32 kDead = 0xFFFFFFFFu;
+constexpr u32 kNone = 0xFFFFFFFFu;
+constexpr u32 kMaxCol = 16384;
+
+struct BlockRec {
+    u64 key;
+    u32 slot;
+    u32 partner;
+};
+
+__device__ __forceinline__ u32 half_bits_of_int(u32 s) { return __half_as_ushort(__uint2half_rn(s)); }
+
+// Accumulate 8 candidates (cb .. cb+7 of column-major `col`, stride Sp) over
+// the query entries e = e0, e0+step, ... < nE.  INT: packed 16-bit lane
+// counts (acc[w] lanes = candidates 2w, 2w+1).  HALF: binary16 sums in order.
+template <bool INTP>
+struct Acc8;
+
+template <>
+struct Acc8<true> {
+    u32 a[4];
+    __device__ __forceinline__ void zero() { a[0] = a[1] = a[2] = a[3] = 0u; }
+    __device__ __forceinline__ void add(const uint4 v, u32 qc, u32 w) {
+        const u32 qq = qc * 0x00010001u;
+        const u32 x[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            // lanes hold codes < 0x8000: a lane of t is zero iff it matches
+            const u32 t = x[i] ^ qq;
+            const u32 u = t + 0x7FFF7FFFu;
+            const u32 m = (~u >> 15) & 0x00010001u;
+            a[i] += m * w;
+        }
+    }
+    __device__ __forceinline__ void store(u16* dst) const {
+        *reinterpret_cast<uint4*>(dst) = make_uint4(a[0], a[1], a[2], a[3]);
+    }
+};
+
+template <>
+struct Acc8<false> {
+    __half a[8];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int i = 0; i < 8; i++) a[i] = __ushort_as_half(0);
+    }
+    __device__ __forceinline__ void add(const uint4 v, u32 qc, u32 wbits) {
+        const u32 x[4] = {v.x, v.y, v.z, v.w};
+        const __half w = __ushort_as_half((u16)wbits);
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            if ((x[i] & 0xFFFFu) == qc) a[2 * i] = __hadd(a[2 * i], w);
+            if ((x[i] >> 16) == qc) a[2 * i + 1] = __hadd(a[2 * i + 1], w);
+        }
+    }
+    __device__ __forceinline__ void store(u16* dst) const {
+        u32 p[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+            p[i] = (u32)__half_as_ushort(a[2 * i]) | ((u32)__half_as_ushort(a[2 * i + 1]) << 16);
+        *reinterpret_cast<uint4*>(dst) = make_uint4(p[0], p[1], p[2], p[3]);
+    }
+};
+
+template <bool INTP>
+__device__ __forceinline__ void accumulate(Acc8<INTP>& acc, const u16* __restrict__ col, u32 Sp, u32 cb,
+                                           const u32* eSC, const u16* eW, int e0, int nE, int step) {
+    int e = e0;
+    // four independent loads in flight per iteration
+    for (; e + 3 * step < nE; e += 4 * step) {
+        u32 s0 = eSC[e], s1 = eSC[e + step], s2 = eSC[e + 2 * step], s3 = eSC[e + 3 * step];
+        u32 w0 = eW[e], w1 = eW[e + step], w2 = eW[e + 2 * step], w3 = eW[e + 3 * step];
+        uint4 v0 = ld_cg_v4(col + (size_t)(s0 & 0xFFFFu) * Sp + cb);
+        uint4 v1 = ld_cg_v4(col + (size_t)(s1 & 0xFFFFu) * Sp + cb);
+        uint4 v2 = ld_cg_v4(col + (size_t)(s2 & 0xFFFFu) * Sp + cb);
+        uint4 v3 = ld_cg_v4(col + (size_t)(s3 & 0xFFFFu) * Sp + cb);
+        acc.add(v0, s0 >> 16, w0);
+        acc.add(v1, s1 >> 16, w1);
+        acc.add(v2, s2 >> 16, w2);
+        acc.add(v3, s3 >> 16, w3);
+    }
+    for (; e < nE; e += step) {
+        u32 s0 = eSC[e];
+        uint4 v0 = ld_cg_v4(col + (size_t)(s0 & 0xFFFFu) * Sp + cb);
+        acc.add(v0, s0 >> 16, eW[e]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// preparation kernels
+
+struct PrepArgs {
+    u32 ntip, ncol, ncolP, nState, Sp;
+    const u32* codes;   // ntip x ncol
+    const u16* Wsel;    // nState x ncol (int weights or binary16 bits)
+    u32 maxCode;        // codes must be <= maxCode
+    u16* nodeRow;       // nnode x ncolP
+    u32* eSC;           // ntip x ncol
+    u16* eW;            // ntip x ncol
+    u32* eLen;          // ntip
+    int* err;
+};
+
+// One warp per tip: narrow codes to u16, validate, and build the tip's
+// ascending list of edited sites with their weights.
+__global__ void k_prep_rows(PrepArgs a) {
+    const u32 warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const u32 lane = threadIdx.x & 31;
+    if (warp >= a.ntip) return;
+    const u32* src = a.codes + (size_t)warp * a.ncol;
+    u16* row = a.nodeRow + (size_t)warp * a.ncolP;
+    u32* es = a.eSC + (size_t)warp * a.ncol;
+    u16* ew = a.eW + (size_t)warp * a.ncol;
+    u32 n = 0;
+    for (u32 s0 = 0; s0 < a.ncolP; s0 += 32) {
+        const u32 s = s0 + lane;
+        u32 c = s < a.ncol ? src[s] : 0u;
+        if (c > a.maxCode || (c > 1 && c - 2 >= a.nState)) {
+            atomicCAS(a.err, 0, CASPHY_ERANGE);
+            c = 0;
+        }
+        if (s < a.ncolP) row[s] = (u16)c;
+        const bool ed = c > 1;
+        const u32 bal = __ballot_sync(0xFFFFFFFFu, ed);
+        if (ed) {
+            const u32 pos = n + __popc(bal & ((1u << lane) - 1u));
+            es[pos] = s | (c << 16);
+            ew[pos] = a.Wsel[(size_t)(c - 2) * a.ncol + s];
+        }
+        n += __popc(bal);
+    }
+    if (lane == 0) a.eLen[warp] = n;
+}
+
+// colT[s][i] = nodeRow[i][s] for tips; padding slots [ntip, Sp) get code 0.
+__global__ void k_transpose(const u16* __restrict__ nodeRow, u32 ntip, u32 ncol, u32 ncolP, u32 Sp,
+                            u16* __restrict__ colT) {
+    __shared__ u16 tile[32][33];
+    const u32 i0 = blockIdx.x * 32, s0 = blockIdx.y * 32;
+    for (u32 r = threadIdx.y; r < 32; r += blockDim.y) {
+        const u32 i = i0 + r, s = s0 + threadIdx.x;
+        tile[r][threadIdx.x] = (i < ntip && s < ncol) ? nodeRow[(size_t)i * ncolP + s] : (u16)0;
+    }
+    __syncthreads();
+    for (u32 r = threadIdx.y; r < 32; r += blockDim.y) {
+        const u32 s = s0 + r, i = i0 + threadIdx.x;
+        if (s < ncol && i < Sp) colT[(size_t)s * Sp + i] = tile[threadIdx.x][r];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// initial upper-triangle local maxima
+
+struct InitArgs {
+    u32 ntip, ncol, Sp;
+    const u16* colT;
+    const u32* eSC;
+    const u16* eW;
+    const u32* eLen;
+    const u64* chunkStart;   // nChunks+1 prefix of tiles per chunk
+    u32 nChunks;
+    u64 nTiles;
+    unsigned long long* tileCounter;
+    unsigned long long* initKey;   // ntip
+};
+
+template <bool INTP>
+__global__ void __launch_bounds__(kThreads) k_init_scan(InitArgs a) {
+    __shared__ unsigned long long s_tile[2];
+    __shared__ u64 red[32];
+    if (threadIdx.x == 0) s_tile[0] = atomicAdd(a.tileCounter, 1ull);
+    __syncthreads();
+    int cur = 0;
+    for (;;) {
+        const u64 t = s_tile[cur];
+        if (t >= a.nTiles) break;
+        if (threadIdx.x == 0) s_tile[cur ^ 1] = atomicAdd(a.tileCounter, 1ull);
+        u32 k = 0;
+        while (k + 1 < a.nChunks && a.chunkStart[k + 1] <= t) k++;
+        const u32 q = (u32)(t - a.chunkStart[k]);
+        const u32 cb = k * kCap + threadIdx.x * kG;
+        u64 best = make_key(ORD_F16_NEG1, 0u);
+        if (cb < a.ntip && cb + kG > q + 1) {
+            Acc8<INTP> acc;
+            acc.zero();
+            accumulate<INTP>(acc, a.colT, a.Sp, cb, a.eSC + (size_t)q * a.ncol, a.eW + (size_t)q * a.ncol, 0,
+                             (int)a.eLen[q], 1);
+            __align__(16) u16 v[8];
+            acc.store(v);
+#pragma unroll
+            for (int m = 0; m < kG; m++) {
+                const u32 j = cb + m;
+                if (j > q && j < a.ntip) {
+                    const u32 hb = INTP ? half_bits_of_int(v[m]) : v[m];
+                    const u64 key = make_key(ord_f16((u16)hb), j);
+                    best = key > best ? key : best;
+                }
+            }
+        }
+        best = block_max_u64(best, red);
+        if (threadIdx.x == 0) atomicMax(a.initKey + q, (unsigned long long)best);
+        cur ^= 1;
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// persistent join loop
+
+struct JoinArgs {
+    u32 ntip, ncol, ncolP, nState, nnode, nCTA;
+    u32 minSize;
+    float minRatio;
+    const u16* Wsel;
+    u16* nodeRow;
+    u16* colT[2];
+    u32* lmOrd[2];
+    u32* lmIdx[2];
+    u32* slotNode[2];
+    u32* node2slot;
+    u32* nodeDeath;
+    u32* nodeSize;
+    u32* rawEdge;
+    BlockRec* rec;       // 2 * nCTA
+    u64* partial;        // 2 * nCTA
+    u32* counts;         // nCTA
+    GridSync* gs;
+    u64 limitNs;
+    unsigned long long* statsOut;  // [0] stale [1] pairs [2] compactions [3] phases
+    u32 Sp0;
+    u32 Rmax;            // max slots per CTA (smem for compaction ranks)
+};
+
+struct Range {
+    u32 S, Sp, R, lo, hi;
+};
+
+__device__ __forceinline__ Range make_range(u32 S, u32 nCTA, u32 b) {
+    Range r;
+    r.S = S;
+    r.Sp = (S + 7u) & ~7u;
+    u32 per = (S + nCTA - 1) / nCTA;
+    r.R = (per + 7u) & ~7u;
+    r.lo = min(b * r.R, S);
+    r.hi = min(r.lo + r.R, S);
+    return r;
+}
+
+// Block-wide argmax of (key, slot, partner) records.  Keys are unique among
+// live slots (one node per slot), so at most one thread holds the winner.
+__device__ __forceinline__ BlockRec block_best_rec(u64 best, u32 bslot, u32 bpart, u64* red, BlockRec* s_rec) {
+    if (threadIdx.x == 0) { s_rec->slot = kNone; s_rec->partner = 0; }
+    const u64 m = block_max_u64(best, red);  // starts and ends with __syncthreads
+    if (best == m && bslot != kNone) { s_rec->slot = bslot; s_rec->partner = bpart; }
+    __syncthreads();
+    BlockRec r;
+    r.key = m;
+    r.slot = s_rec->slot;
+    r.partner = s_rec->partner;
+    __syncthreads();
+    return r;
+}
+
+__device__ __forceinline__ u16* colT_of(const JoinArgs& a, u32 buf) { return buf ? a.colT[1] : a.colT[0]; }
+__device__ __forceinline__ u32* lmOrd_of(const JoinArgs& a, u32 buf) { return buf ? a.lmOrd[1] : a.lmOrd[0]; }
+__device__ __forceinline__ u32* lmIdx_of(const JoinArgs& a, u32 buf) { return buf ? a.lmIdx[1] : a.lmIdx[0]; }
+__device__ __forceinline__ u32* slotNode_of(const JoinArgs& a, u32 buf) { return buf ? a.slotNode[1] : a.slotNode[0]; }
+
+// Best (key, slot, partner) over this CTA's slots from the stored local maxima.
+__device__ BlockRec own_best(const JoinArgs& a, u32 buf, const Range& rg, u64* red, BlockRec* s_rec) {
+    u64 best = make_key(ORD_F16_NEG1, 0u);
+    u32 bslot = kNone, bpart = 0u;
+    const u32* sn = slotNode_of(a, buf);
+    const u32* lo = lmOrd_of(a, buf);
+    const u32* li = lmIdx_of(a, buf);
+    for (u32 c = rg.lo + threadIdx.x; c < rg.hi; c += kThreads) {
+        const u32 node = ld_cg_u32(sn + c);
+        if (node == kDead) continue;
+        const u64 key = make_key(ld_cg_u32(lo + c), node);
+        if (key > best) { best = key; bslot = c; bpart = ld_cg_u32(li + c); }
+    }
+    return block_best_rec(best, bslot, bpart, red, s_rec);
+}
+
+__device__ __forceinline__ void put_rec(BlockRec* dst, const BlockRec& r) {
+    if (threadIdx.x == 0) {
+        asm volatile("st.global.cg.v2.u64 [%0], {%1, %2};" ::"l"(dst), "l"(r.key),
+                     "l"(((u64)r.partner << 32) | r.slot)
+                     : "memory");
+    }
+}
+
+// Every CTA reduces the same per-CTA records, so all reach the same join.
+__device__ BlockRec global_best(const BlockRec* src, u32 nCTA, u64* red, BlockRec* s_rec) {
+    u64 best = 0;
+    u32 slot = kNone, partner = 0;
+    for (u32 i = threadIdx.x; i < nCTA; i += kThreads) {
+        const uint4 v = ld_cg_v4(src + i);
+        const u64 key = ((u64)v.y << 32) | v.x;
+        if (key > best) { best = key; slot = v.z; partner = v.w; }
+    }
+    return block_best_rec(best, slot, partner, red, s_rec);
+}
+
+// Builds the query site list from a row.  mode 0: query = row1 (global);
+// 1: copy row2; 2: keep row1; 3: ancestral merge of row1 and row2
+// (updateAncestralKernel, cu/joinEdgeIndel.cu:87-99).  The merged row is
+// also kept in shared memory (mrow) for the write-back.
+__device__ int build_query(const JoinArgs& a, const u16* row1, const u16* row2, int mode, u16* mrow, u32* eSC,
+                           u16* eW, u32* wcount) {
+    const u32 lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int base = 0;
+    for (u32 s0 = 0; s0 < a.ncolP; s0 += kThreads) {
+        const u32 s = s0 + threadIdx.x;
+        u32 c = 0;
+        if (s < a.ncol) {
+            const u32 x = ld_cg_u16(row1 + s);
+            if (mode == 0 || mode == 2) {
+                c = x;
+            } else {
+                const u32 y = ld_cg_u16(row2 + s);
+                if (mode == 1) c = y;
+                else c = (x == 0) ? y : ((y >= 1 && x != y) ? 1u : x);
+            }
+        }
+        if (s < a.ncolP && mrow) mrow[s] = (u16)c;
+        const bool ed = c > 1;
+        const u32 bal = __ballot_sync(0xFFFFFFFFu, ed);
+        if (lane == 0) wcount[wid] = __popc(bal);
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            u32 v = threadIdx.x < (kThreads / 32) ? wcount[threadIdx.x] : 0u;
+            u32 incl = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                u32 n = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                if (lane >= (u32)o) incl += n;
+            }
+            if (threadIdx.x < (kThreads / 32)) wcount[16 + threadIdx.x] = incl - v;
+            if (threadIdx.x == 31) wcount[15 + 16 + 1] = incl;
+        }
+        __syncthreads();
+        if (ed) {
+            const u32 pos = base + wcount[16 + wid] + __popc(bal & ((1u << lane) - 1u));
+            eSC[pos] = s | (c << 16);
+            eW[pos] = a.Wsel[(size_t)(c - 2) * a.ncol + s];
+        }
+        base += (int)wcount[32];
+        __syncthreads();
+    }
+    return base;
+}
+
+// Scores this CTA's live slots against the query list.  STALE: returns the
+// best (score, node) key over slots != c1.  JOIN: updates the local maxima
+// (strict improvement, cu/joinEdgeIndel.cu:453-460) and returns the CTA's
+// best record over all its live slots.
+template <bool INTP, bool JOIN>
+__device__ BlockRec scan_own(const JoinArgs& a, u32 buf, const Range& rg, int nE, const u32* eSC, const u16* eW,
+                             u16* part, u32 c1, u32 newNode, u64* red, BlockRec* s_rec) {
+    const u32 R = rg.hi - rg.lo;
+    int F = 1;
+    if (INTP) {
+        while (F < 16 && (u32)(kCap / (F * 2)) >= R) F *= 2;
+    }
+    const u32 cap = kCap / F;
+    const u32 Tg = kThreads / F;
+    const u32 g = threadIdx.x / Tg, t = threadIdx.x % Tg;
+    u64 best = make_key(ORD_F16_NEG1, 0u);
+    u32 bslot = kNone, bpart = 0;
+    for (u32 base = rg.lo; base < rg.hi; base += cap) {
+        const u32 cb = base + t * kG;
+        Acc8<INTP> acc;
+        acc.zero();
+        if (cb < rg.hi) accumulate<INTP>(acc, colT_of(a, buf), rg.Sp, cb, eSC, eW, (int)g, nE, F);
+        acc.store(part + g * cap + t * kG);
+        __syncthreads();
+        for (u32 x = threadIdx.x; x < cap; x += kThreads) {
+            const u32 c = base + x;
+            if (c >= rg.hi) break;
+            const u32 node = ld_cg_u32(slotNode_of(a, buf) + c);
+            if (node == kDead || c == c1) continue;
+            u32 hb;
+            if (INTP) {
+                u32 sum = 0;
+                for (int gg = 0; gg < F; gg++) sum += part[gg * cap + x];
+                hb = half_bits_of_int(sum);
+            } else {
+                hb = part[x];
+            }
+            const u32 o = ord_f16((u16)hb);
+            if (JOIN) {
+                u32* lop = lmOrd_of(a, buf);
+                u32* lip = lmIdx_of(a, buf);
+                u32 lo = ld_cg_u32(lop + c);
+                u32 li;
+                if (o > lo) {
+                    lo = o;
+                    li = newNode;
+                    lop[c] = o;
+                    lip[c] = newNode;
+                } else {
+                    li = ld_cg_u32(lip + c);
+                }
+                const u64 key = make_key(lo, node);
+                if (key > best) { best = key; bslot = c; bpart = li; }
+            } else {
+                const u64 key = make_key(o, node);
+                if (key > best) { best = key; bslot = c; }
+            }
+        }
+        __syncthreads();
+    }
+    return block_best_rec(best, bslot, bpart, red, s_rec);
+}
+
+template <bool INTP>
+__global__ void __launch_bounds__(kThreads, 1) k_join(JoinArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    u16* part = reinterpret_cast<u16*>(smem);                    // kCap u16
+    u32* eSC = reinterpret_cast<u32*>(part + kCap);              // ncol
+    u32* ranks = eSC + a.ncol;                                   // Rmax
+    u16* eW = reinterpret_cast<u16*>(ranks + a.Rmax);            // ncol
+    u16* mrow = eW + ((a.ncol + 7u) & ~7u);                      // ncolP
+    __shared__ u64 red[32];
+    __shared__ BlockRec s_rec;
+    __shared__ u32 wcount[40];
+    __shared__ u32 s_val[4];
+
+    const u32 b = blockIdx.x, nCTA = a.nCTA;
+    if (threadIdx.x == 0) { s_rec.slot = kNone; s_rec.partner = 0; }
+    __syncthreads();
+    u32 buf = 0;
+    Range rg = make_range(a.ntip, nCTA, b);
+    u32 k = 0, p = 0;
+    unsigned long long nStale = 0, nPairs = 0, nComp = 0;
+    const u32 nJoin = a.ntip - 1;
+    int fail = 0;
+
+    BlockRec my = own_best(a, buf, rg, red, &s_rec);
+    put_rec(a.rec + b, my);
+    if (grid_barrier(a.gs, nCTA, a.limitNs)) goto out;
+    p = 1;
+
+    while (k < nJoin) {
+        const BlockRec g = global_best(a.rec + ((p - 1) & 1) * nCTA, nCTA, red, &s_rec);
+        const u32 j1 = key_node(g.key), c1 = g.slot, j2 = g.partner;
+        if (c1 >= rg.S || j1 >= a.nnode || j2 >= a.nnode) { fail = CASPHY_EINTERNAL; break; }
+        if (threadIdx.x == 0) {
+            s_val[0] = ld_cg_u32(a.nodeDeath + j2);
+            s_val[1] = ld_cg_u32(a.node2slot + j2);
+            s_val[2] = ld_cg_u32(a.nodeSize + j1);
+            s_val[3] = ld_cg_u32(a.nodeSize + j2);
+        }
+        __syncthreads();
+        const u32 death = s_val[0], c2 = s_val[1], s1 = s_val[2], s2 = s_val[3];
+        __syncthreads();
+        const bool stale = death < k || c2 >= rg.S;
+        if (stale) {
+            // rescore j1 against every live slot (cu/joinEdgeIndel.cu:387-399)
+            const int nE = build_query(a, a.nodeRow + (size_t)j1 * a.ncolP, nullptr, 0, nullptr, eSC, eW, wcount);
+            BlockRec pr = scan_own<INTP, false>(a, buf, rg, nE, eSC, eW, part, c1, 0u, red, &s_rec);
+            if (threadIdx.x == 0) {
+                asm volatile("st.global.cg.u64 [%0], %1;" ::"l"(a.partial + (p & 1) * nCTA + b), "l"(pr.key) : "memory");
+            }
+            put_rec(a.rec + (p & 1) * nCTA + b, my);
+            nStale++;
+            nPairs += (a.ntip - k) - 1;
+            if (grid_barrier(a.gs, nCTA, a.limitNs)) goto out;
+            p++;
+            // combine the partial argmaxes and store the new local max of c1
+            u64 pb = 0;
+            for (u32 i = threadIdx.x; i < nCTA; i += kThreads) {
+                const u64 v = ld_cg_u64(a.partial + ((p - 1) & 1) * nCTA + i);
+                pb = v > pb ? v : pb;
+            }
+            pb = block_max_u64(pb, red);
+            if (c1 >= rg.lo && c1 < rg.hi) {
+                if (threadIdx.x == 0) {
+                    lmOrd_of(a, buf)[c1] = key_ord(pb);
+                    lmIdx_of(a, buf)[c1] = key_node(pb);
+                }
+                __syncthreads();
+                my = own_best(a, buf, rg, red, &s_rec);
+            }
+            put_rec(a.rec + (p & 1) * nCTA + b, my);
+            if (grid_barrier(a.gs, nCTA, a.limitNs)) goto out;
+            p++;
+            continue;
+        }
+        // join j1 and j2 into node ntip+k (cu/joinEdgeIndel.cu:402-467)
+        const u32 newNode = a.ntip + k;
+        int mode;
+        if (s1 < a.minSize && __uint2float_rn(s1) * a.minRatio < __uint2float_rn(s2)) mode = 1;
+        else if (s2 < a.minSize && __uint2float_rn(s2) * a.minRatio < __uint2float_rn(s1)) mode = 2;
+        else mode = 3;
+        const int nE = build_query(a, a.nodeRow + (size_t)j1 * a.ncolP, a.nodeRow + (size_t)j2 * a.ncolP, mode, mrow,
+                                   eSC, eW, wcount);
+        if (b == 0) {
+            u16* dst = a.nodeRow + (size_t)newNode * a.ncolP;
+            for (u32 s = threadIdx.x; s < a.ncolP; s += kThreads) dst[s] = mrow[s];
+            if (threadIdx.x == 0) {
+                a.nodeSize[newNode] = s1 + s2;
+                a.rawEdge[4 * k + 0] = newNode;
+                a.rawEdge[4 * k + 1] = j1;
+                a.rawEdge[4 * k + 2] = newNode;
+                a.rawEdge[4 * k + 3] = j2;
+                a.node2slot[newNode] = c1;
+                a.nodeDeath[j1] = k;
+                a.nodeDeath[j2] = k;
+            }
+        }
+        if (c1 >= rg.lo && c1 < rg.hi) {
+            u16* col = colT_of(a, buf);
+            for (u32 s = threadIdx.x; s < a.ncol; s += kThreads) col[(size_t)s * rg.Sp + c1] = mrow[s];
+            if (threadIdx.x == 0) {
+                slotNode_of(a, buf)[c1] = newNode;
+                lmOrd_of(a, buf)[c1] = ORD_F16_NEG1;
+            }
+        }
+        if (c2 >= rg.lo && c2 < rg.hi && threadIdx.x == 0) {
+            slotNode_of(a, buf)[c2] = kDead;
+            lmOrd_of(a, buf)[c2] = ORD_F16_NEG1;
+        }
+        __syncthreads();
+        my = scan_own<INTP, true>(a, buf, rg, nE, eSC, eW, part, c1, newNode, red, &s_rec);
+        put_rec(a.rec + (p & 1) * nCTA + b, my);
+        nPairs += (a.ntip - k - 1) - 1;
+        k++;
+        if (grid_barrier(a.gs, nCTA, a.limitNs)) goto out;
+        p++;
+
+        // squeeze dead slots out when fewer than 3/4 are alive
+        const u32 alive = a.ntip - k;
+        if (k < nJoin && rg.S >= 4096 && (u64)alive * 4 < (u64)rg.S * 3) {
+            // C1: live slots per CTA
+            const u32* sn = slotNode_of(a, buf);
+            {
+                u32 v = 0;
+                for (u32 c = rg.lo + threadIdx.x; c < rg.hi; c += kThreads) v += ld_cg_u32(sn + c) != kDead;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+                if ((threadIdx.x & 31) == 0) wcount[threadIdx.x >> 5] = v;
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    u32 tot = 0;
+                    for (int w = 0; w < kThreads / 32; w++) tot += wcount[w];
+                    a.counts[b] = tot;
+                }
+                __syncthreads();
+            }
+            if (grid_barrier(a.gs, nCTA, a.limitNs)) goto out;
+            p++;
+            // C2: new positions = exclusive prefix of the per-CTA live counts
+            if (threadIdx.x == 0) {
+                u32 off = 0, tot = 0;
+                for (u32 i = 0; i < nCTA; i++) {
+                    const u32 v = ld_cg_u32(a.counts + i);
+                    if (i < b) off += v;
+                    tot += v;
+                }
+                s_val[0] = off;
+                s_val[1] = tot;
+            }
+            __syncthreads();
+            const u32 off = s_val[0], Snew = s_val[1];
+            __syncthreads();
+            if (Snew != alive) { fail = CASPHY_EINTERNAL; break; }
+            const u32 Spn = (Snew + 7u) & ~7u;
+            const u32 nb = buf ^ 1u;
+            u32* snN = slotNode_of(a, nb);
+            u32* loN = lmOrd_of(a, nb);
+            u32* liN = lmIdx_of(a, nb);
+            {
+                const u32 R = rg.hi - rg.lo;
+                const u32 per = (R + kThreads - 1) / kThreads;
+                const u32 c0 = rg.lo + threadIdx.x * per;
+                const u32 cEnd = min(c0 + per, rg.hi);
+                u32 v = 0;
+                for (u32 c = c0; c < cEnd; c++) v += ld_cg_u32(sn + c) != kDead;
+                u32 incl = v;
+                const u32 lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    u32 n = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                    if (lane >= (u32)o) incl += n;
+                }
+                if (lane == 31) wcount[wid] = incl;
+                __syncthreads();
+                if (threadIdx.x < 32) {
+                    u32 wv = threadIdx.x < kThreads / 32 ? wcount[threadIdx.x] : 0u, wi = wv;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        u32 n = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+                        if (lane >= (u32)o) wi += n;
+                    }
+                    if (threadIdx.x < kThreads / 32) wcount[16 + threadIdx.x] = wi - wv;
+                }
+                __syncthreads();
+                u32 r = off + wcount[16 + wid] + incl - v;
+                const u32* lo = lmOrd_of(a, buf);
+                const u32* li = lmIdx_of(a, buf);
+                for (u32 c = c0; c < cEnd; c++) {
+                    const u32 node = ld_cg_u32(sn + c);
+                    if (node != kDead) {
+                        ranks[c - rg.lo] = r;
+                        snN[r] = node;
+                        loN[r] = ld_cg_u32(lo + c);
+                        liN[r] = ld_cg_u32(li + c);
+                        a.node2slot[node] = r;
+                        r++;
+                    } else {
+                        ranks[c - rg.lo] = kNone;
+                    }
+                }
+                __syncthreads();
+                const u16* src = colT_of(a, buf);
+                u16* dst = colT_of(a, nb);
+                for (u32 s = 0; s < a.ncol; s++) {
+                    for (u32 x = threadIdx.x; x < R; x += kThreads) {
+                        const u32 rr = ranks[x];
+                        if (rr != kNone) dst[(size_t)s * Spn + rr] = ld_cg_u16(src + (size_t)s * rg.Sp + rg.lo + x);
+                    }
+                }
+            }
+            if (b == 0 && threadIdx.x < Spn - Snew) {
+                snN[Snew + threadIdx.x] = kDead;
+                loN[Snew + threadIdx.x] = ORD_F16_NEG1;
+            }
+            if (grid_barrier(a.gs, nCTA, a.limitNs)) goto out;
+            p++;
+            // C3: switch to the compacted buffers
+            buf = nb;
+            rg = make_range(Snew, nCTA, b);
+            my = own_best(a, buf, rg, red, &s_rec);
+            put_rec(a.rec + (p & 1) * nCTA + b, my);
+            nComp++;
+            if (grid_barrier(a.gs, nCTA, a.limitNs)) goto out;
+            p++;
+        }
+    }
+out:
+    if (fail && threadIdx.x == 0) atomicCAS(&a.gs->err, 0, fail);
+    if (b == 0 && threadIdx.x == 0) {
+        a.statsOut[0] = nStale;
+        a.statsOut[1] = nPairs;
+        a.statsOut[2] = nComp;
+        a.statsOut[3] = p;
+        a.statsOut[4] = buf;
+    }
+}
+
+// state_out[r] = nodeRow[order[r]] widened to u32
+__global__ void k_gather(const u16* __restrict__ nodeRow, u32 ncol, u32 ncolP, const u32* __restrict__ order, u32 nrows,
+                         u32* __restrict__ out) {
+    const u32 r = blockIdx.x;
+    if (r >= nrows) return;
+    const u16* src = nodeRow + (size_t)order[r] * ncolP;
+    u32* dst = out + (size_t)r * ncol;
+    for (u32 s = threadIdx.x; s < ncol; s += blockDim.x) dst[s] = src[s];
+}
+
+__global__ void k_slot_init(u32 ntip, u32 Sp, u32 nnode, const unsigned long long* initKey, u32* lmOrd, u32* lmIdx,
+                            u32* slotNode, u32* node2slot, u32* nodeDeath, u32* nodeSize, const u32* tipSize) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < Sp) {
+        if (i < ntip) {
+            const u64 k = initKey[i];
+            lmOrd[i] = key_ord(k);
+            lmIdx[i] = key_node(k);
+            slotNode[i] = i;
+        } else {
+            lmOrd[i] = ORD_F16_NEG1;
+            lmIdx[i] = 0;
+            slotNode[i] = kDead;
+        }
+    }
+    if (i < nnode) {
+        node2slot[i] = i < ntip ? i : kNone;
+        nodeDeath[i] = kNone;
+        nodeSize[i] = i < ntip ? tipSize[i] : 0u;
+    }
+}
+
+__global__ void k_fill_u64(unsigned long long* p, u64 n, u64 v) {
+    const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+}  // namespace indel
+
+// ---------------------------------------------------------------------------
+// host side
+
+using namespace indel;
+
+// Pre-order walk of the raw join edges (cu/joinEdgeIndel.cu:488-558): node v's
+// edges are 2(v-ntip) (first child) and 2(v-ntip)+1; the root is 2ntip-2.
+// Writes the relabelled edge list and the node id of every state row.
+void preorder_relabel(u32 ntip, const u32* rawEdge, u32* edge_out, std::vector<u32>& order) {
+    const u32 nnode = 2 * ntip - 1, nedge = 2 * ntip - 2;
+    std::vector<u32> relabel(nnode);
+    for (u32 i = 0; i < nnode; i++) relabel[i] = i < ntip ? i : nnode;
+    std::vector<u32> stack;
+    std::vector<unsigned char> cursor(nnode, 0);
+    stack.reserve(nnode);
+    order.clear();
+    order.reserve(ntip);
+    order.push_back(nnode - 1);
+    stack.push_back(nnode - 1);
+    u32 count = ntip, nout = 0;
+    while (!stack.empty()) {
+        const u32 v = stack.back();
+        if (v < ntip || cursor[v] >= 2) { stack.pop_back(); continue; }
+        const u32 ei = 2 * (v - ntip) + cursor[v];
+        cursor[v]++;
+        const u32 p = rawEdge[2 * ei], c = rawEdge[2 * ei + 1];
+        stack.push_back(c);
+        if (relabel[p] == nnode) relabel[p] = count++;
+        if (relabel[c] == nnode) {
+            order.push_back(c);
+            relabel[c] = count++;
+        }
+        edge_out[2 * nout] = relabel[p];
+        edge_out[2 * nout + 1] = relabel[c];
+        nout++;
+    }
+    (void)nedge;
+}
+
+// binary16 conversion of the weight table, and the exactness test for the
+// integer path: every weight a non-negative integer and the largest reachable
+// score (sum over sites of the site's largest weight) at most 2048.
+static int convert_weights(u32 nState, u32 ncol, const double* w, std::vector<u16>& hbits, std::vector<u16>& wint,
+                           bool& intPath) {
+    const size_t n = (size_t)nState * ncol;
+    hbits.resize(n ? n : 1);
+    wint.resize(n ? n : 1);
+    intPath = true;
+    double maxSum = 0;
+    std::vector<double> colMax(ncol, 0.0);
+    for (size_t i = 0; i < n; i++) {
+        const double x = w[i];
+        if (std::isnan(x) || x < 0) {
+            casphy_set_last_error_msg("weights must be >= 0 and not NaN");
+            return CASPHY_EINVAL;
+        }
+        const __half h = __double2half(x);
+        const u16 hb = __half_as_ushort(h);
+        hbits[i] = hb;
+        const float hf = __half2float(h);
+        if (!(hf == std::floor(hf) && hf <= 2048.0f)) intPath = false;
+        wint[i] = intPath ? (u16)hf : 0;
+        colMax[i % ncol] = std::max(colMax[i % ncol], (double)hf);
+    }
+    for (u32 i = 0; i < ncol; i++) maxSum += colMax[i];
+    if (maxSum > 2048.0) intPath = false;
+    if ((u64)nState + 1 > 0x7FFFu) intPath = false;  // packed-lane compare needs codes < 0x8000
+    return CASPHY_OK;
+}
+
+static int join_indel_impl(u32 ntip, u32 ncol, const u32* d_codes, u32 nState, const double* weight,
+                           const u32* tipSize, u32 minSize, float minRatio, u32* edge_out, u32* d_state_out,
+                           u32* h_state_out, casphy_join_stats* stats, cudaStream_t st, DeviceScope& ds,
+                           const u32* h_codes) {
+    if (ntip == 0 || ncol == 0 || !weight || !tipSize || !edge_out) return CASPHY_EINVAL;
+    if (ncol > kMaxCol) {
+        casphy_set_last_error_msg("ncol exceeds 16384");
+        return CASPHY_ERANGE;
+    }
+    std::vector<u16> hbits, wint;
+    bool intPath = false;
+    int rc = convert_weights(nState, ncol, weight, hbits, wint, intPath);
+    if (rc) return rc;
+    casphy_join_stats lst{};
+    lst.int_path = intPath ? 1 : 0;
+    const u32 nnode = 2 * ntip - 1, nedge = 2 * ntip - 2;
+    const u32 ncolP = (ncol + 7u) & ~7u;
+    const u32 Sp = (ntip + 7u) & ~7u;
+    int dev = ds.dev, nSM = 0;
+    CASPHY_CUDA_TRY(cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, dev));
+
+    const u32 nCTA = (u32)nSM;
+    const u32 Rmax = (((ntip + nCTA - 1) / nCTA) + 7u) & ~7u;
+    // device layout
+    Carve cv;
+    auto layout = [&](Carve& c) {
+        struct L {
+            u32* codes; u16* Wsel; u16* nodeRow; u16* colT0; u16* colT1; u32* lm[6];
+            u32* node2slot; u32* nodeDeath; u32* nodeSize; u32* rawEdge; u32* eSC; u16* eW; u32* eLen;
+            unsigned long long* initKey; BlockRec* rec; u64* partial; u32* counts; GridSync* gs;
+            unsigned long long* tileCounter; u64* chunkStart; unsigned long long* stats; u32* order; u32* tipSize;
+            u32* stateOut; int* err;
+        } l;
+        l.codes = c.take<u32>(h_codes ? (size_t)ntip * ncol : 0);
+        l.Wsel = c.take<u16>(hbits.size());
+        l.nodeRow = c.take<u16>((size_t)nnode * ncolP);
+        l.colT0 = c.take<u16>((size_t)ncol * Sp);
+        l.colT1 = c.take<u16>((size_t)ncol * Sp);
+        for (int i = 0; i < 6; i++) l.lm[i] = c.take<u32>(Sp);
+        l.node2slot = c.take<u32>(nnode);
+        l.nodeDeath = c.take<u32>(nnode);
+        l.nodeSize = c.take<u32>(nnode);
+        l.rawEdge = c.take<u32>((size_t)2 * nedge + 2);
+        l.eSC = c.take<u32>((size_t)ntip * ncol);
+        l.eW = c.take<u16>((size_t)ntip * ncol);
+        l.eLen = c.take<u32>(ntip);
+        l.initKey = c.take<unsigned long long>(ntip);
+        l.rec = c.take<BlockRec>(2 * nCTA);
+        l.partial = c.take<u64>(2 * nCTA);
+        l.counts = c.take<u32>(nCTA);
+        l.gs = c.take<GridSync>(1);
+        l.tileCounter = c.take<unsigned long long>(1);
+        l.chunkStart = c.take<u64>(1024);
+        l.stats = c.take<unsigned long long>(8);
+        l.order = c.take<u32>(ntip);
+        l.tipSize = c.take<u32>(ntip);
+        l.stateOut = c.take<u32>(h_state_out ? (size_t)std::max(ntip - 1, 1u) * ncol : 0);
+        l.err = c.take<int>(1);
+        return l;
+    };
+    layout(cv);
+    void* base = nullptr;
+    rc = ds.reserve(cv.off + 256, &base);
+    if (rc) return rc;
+    Carve c2;
+    c2.base = static_cast<char*>(base);
+    auto L = layout(c2);
+    const u32* codes = d_codes;
+    if (h_codes) {
+        CASPHY_CUDA_TRY(cudaMemcpyAsync(L.codes, h_codes, sizeof(u32) * (size_t)ntip * ncol, cudaMemcpyHostToDevice, st));
+        codes = L.codes;
+    }
+    cudaEvent_t ev[6];
+    for (auto& e : ev) CASPHY_CUDA_TRY(cudaEventCreate(&e));
+    CASPHY_CUDA_TRY(cudaEventRecord(ev[0], st));
+    CASPHY_CUDA_TRY(cudaMemcpyAsync(L.Wsel, intPath ? wint.data() : hbits.data(), sizeof(u16) * hbits.size(),
+                                    cudaMemcpyHostToDevice, st));
+    CASPHY_CUDA_TRY(cudaMemcpyAsync(L.tipSize, tipSize, sizeof(u32) * ntip, cudaMemcpyHostToDevice, st));
+    CASPHY_CUDA_TRY(cudaMemsetAsync(L.err, 0, sizeof(int), st));
+    CASPHY_CUDA_TRY(cudaMemsetAsync(L.gs, 0, sizeof(GridSync), st));
+    CASPHY_CUDA_TRY(cudaMemsetAsync(L.tileCounter, 0, sizeof(unsigned long long), st));
+    CASPHY_CUDA_TRY(cudaMemsetAsync(L.stats, 0, sizeof(unsigned long long) * 8, st));
+    u64 launches = 0;
+
+    PrepArgs pa{ntip, ncol, ncolP, nState, Sp, codes, L.Wsel, intPath ? 0x7FFFu : 0xFFFFu,
+                L.nodeRow, L.eSC, L.eW, L.eLen, L.err};
+    k_prep_rows<<<(ntip + 7) / 8, 256, 0, st>>>(pa);
+    dim3 tg((Sp + 31) / 32, (ncol + 31) / 32);
+    k_transpose<<<tg, dim3(32, 8), 0, st>>>(L.nodeRow, ntip, ncol, ncolP, Sp, L.colT0);
+    launches += 2;
+    // tiles: chunk k holds candidates [k*kCap, (k+1)*kCap); queries i < min(end, ntip) - 1
+    const u32 nChunks = (ntip + kCap - 1) / kCap;
+    if (nChunks + 1 > 1024) {
+        casphy_set_last_error_msg("too many cells for the chunk table");
+        return CASPHY_ERANGE;
+    }
+    std::vector<u64> chunkStart(nChunks + 1, 0);
+    for (u32 k = 0; k < nChunks; k++) {
+        const u64 end = std::min<u64>((u64)(k + 1) * kCap, ntip);
+        chunkStart[k + 1] = chunkStart[k] + (end >= 1 ? end - 1 : 0);
+    }
+    const u64 nTiles = chunkStart[nChunks];
+    CASPHY_CUDA_TRY(cudaMemcpyAsync(L.chunkStart, chunkStart.data(), sizeof(u64) * (nChunks + 1),
+                                    cudaMemcpyHostToDevice, st));
+    k_fill_u64<<<(ntip + 255) / 256, 256, 0, st>>>(L.initKey, ntip, ((u64)ORD_F16_NEG1 << 32) | 0xFFFFFFFFull);
+    launches++;
+    int initBlocksPerSM = 0;
+    CASPHY_CUDA_TRY(cudaEventRecord(ev[1], st));
+    InitArgs ia{ntip, ncol, Sp, L.colT0, L.eSC, L.eW, L.eLen, L.chunkStart, nChunks, nTiles, L.tileCounter, L.initKey};
+    if (intPath) {
+        CASPHY_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&initBlocksPerSM, k_init_scan<true>, kThreads, 0));
+        k_init_scan<true><<<nSM * std::max(initBlocksPerSM, 1), kThreads, 0, st>>>(ia);
+    } else {
+        CASPHY_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&initBlocksPerSM, k_init_scan<false>, kThreads, 0));
+        k_init_scan<false><<<nSM * std::max(initBlocksPerSM, 1), kThreads, 0, st>>>(ia);
+    }
+    launches++;
+    CASPHY_CUDA_TRY(cudaEventRecord(ev[2], st));
+    const u32 initN = std::max(Sp, nnode);
+    k_slot_init<<<(initN + 255) / 256, 256, 0, st>>>(ntip, Sp, nnode, L.initKey, L.lm[0], L.lm[1], L.lm[2],
+                                                       L.node2slot, L.nodeDeath, L.nodeSize, L.tipSize);
+    launches++;
+    JoinArgs ja{};
+    ja.ntip = ntip; ja.ncol = ncol; ja.ncolP = ncolP; ja.nState = nState; ja.nnode = nnode; ja.nCTA = nCTA;
+    ja.minSize = minSize; ja.minRatio = minRatio; ja.Wsel = L.Wsel; ja.nodeRow = L.nodeRow;
+    ja.colT[0] = L.colT0; ja.colT[1] = L.colT1;
+    ja.lmOrd[0] = L.lm[0]; ja.lmIdx[0] = L.lm[1]; ja.slotNode[0] = L.lm[2];
+    ja.lmOrd[1] = L.lm[3]; ja.lmIdx[1] = L.lm[4]; ja.slotNode[1] = L.lm[5];
+    ja.node2slot = L.node2slot; ja.nodeDeath = L.nodeDeath; ja.nodeSize = L.nodeSize; ja.rawEdge = L.rawEdge;
+    ja.rec = L.rec; ja.partial = L.partial; ja.counts = L.counts; ja.gs = L.gs;
+    ja.limitNs = 20ull * 1000 * 1000 * 1000;
+    ja.statsOut = L.stats; ja.Sp0 = Sp; ja.Rmax = Rmax;
+    const size_t smemBytes = sizeof(u16) * kCap + sizeof(u32) * ncol + sizeof(u32) * Rmax +
+                             sizeof(u16) * (((ncol + 7u) & ~7u) + ncolP) + 64;
+    if (ntip >= 2) {
+        void* fn = intPath ? (void*)k_join<true> : (void*)k_join<false>;
+        CASPHY_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemBytes));
+        int perSM = 0;
+        CASPHY_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fn, kThreads, smemBytes));
+        if (perSM < 1) {
+            casphy_set_last_error_msg("join kernel does not fit on an SM");
+            return CASPHY_ERANGE;
+        }
+        void* args[] = {&ja};
+        CASPHY_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(nCTA), dim3(kThreads), args, smemBytes, st));
+        launches++;
+    }
+    CASPHY_CUDA_TRY(cudaEventRecord(ev[3], st));
+    std::vector<u32> raw((size_t)2 * nedge + 2);
+    unsigned long long hst[8] = {0};
+    int herr = 0;
+    GridSync hgs{};
+    CASPHY_CUDA_TRY(cudaMemcpyAsync(raw.data(), L.rawEdge, sizeof(u32) * 2 * nedge, cudaMemcpyDeviceToHost, st));
+    CASPHY_CUDA_TRY(cudaMemcpyAsync(hst, L.stats, sizeof(hst), cudaMemcpyDeviceToHost, st));
+    CASPHY_CUDA_TRY(cudaMemcpyAsync(&herr, L.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CASPHY_CUDA_TRY(cudaMemcpyAsync(&hgs, L.gs, sizeof(GridSync), cudaMemcpyDeviceToHost, st));
+    CASPHY_CUDA_TRY(cudaStreamSynchronize(st));
+    if (herr) {
+        casphy_set_last_error_msg("cell codes exceed nState+1 (or 65535)");
+        return herr;
+    }
+    if (hgs.err) {
+        casphy_set_last_error_msg(hgs.err == CASPHY_ETIMEOUT ? "join loop grid barrier timed out"
+                                                              : "join loop invariant violated");
+        return hgs.err;
+    }
+    std::vector<u32> order;
+    const u32 nrows = std::max(ntip - 1, 1u);
+    if (ntip >= 2) {
+        preorder_relabel(ntip, raw.data(), edge_out, order);
+        if (order.size() != nrows) return CASPHY_EINTERNAL;
+    } else {
+        order.assign(1, 0u);
+    }
+    CASPHY_CUDA_TRY(cudaMemcpyAsync(L.order, order.data(), sizeof(u32) * nrows, cudaMemcpyHostToDevice, st));
+    u32* sout = d_state_out ? d_state_out : L.stateOut;
+    if (sout) {
+        k_gather<<<nrows, 256, 0, st>>>(L.nodeRow, ncol, ncolP, L.order, nrows, sout);
+        launches++;
+        if (h_state_out)
+            CASPHY_CUDA_TRY(cudaMemcpyAsync(h_state_out, sout, sizeof(u32) * (size_t)nrows * ncol,
+                                            cudaMemcpyDeviceToHost, st));
+    }
+    CASPHY_CUDA_TRY(cudaEventRecord(ev[4], st));
+    CASPHY_CUDA_TRY(cudaEventSynchronize(ev[4]));
+    float t12 = 0, t23 = 0, t04 = 0;
+    cudaEventElapsedTime(&t12, ev[1], ev[2]);
+    cudaEventElapsedTime(&t23, ev[2], ev[3]);
+    cudaEventElapsedTime(&t04, ev[0], ev[4]);
+    for (auto& e : ev) cudaEventDestroy(e);
+    lst.joins = ntip - 1;
+    lst.stale_recomputes = hst[0];
+    lst.pair_scores = (u64)ntip * (ntip - 1) / 2 + hst[1];
+    lst.compactions = hst[2];
+    lst.kernel_launches = launches;
+    lst.init_scan_ms = t12;
+    lst.join_loop_ms = t23;
+    lst.total_ms = t04;
+    if (stats) *stats = lst;
+    return CASPHY_OK;
+}
+
+}  // namespace casphy
+
+extern "C" int casphy_join_indel(uint32_t ntip, uint32_t ncol, const uint32_t* codes, uint32_t nState,
+                                 const double* weight, const uint32_t* tipSize, uint32_t minSize, float minRatio,
+                                 uint32_t* edge_out, uint32_t* state_out, casphy_join_stats* stats) {
+    int rc = casphy::require_device();
+    if (rc) return rc;
+    if (!codes || !state_out) return CASPHY_EINVAL;
+    casphy::DeviceScope ds;
+    return casphy::join_indel_impl(ntip, ncol, nullptr, nState, weight, tipSize, minSize, minRatio, edge_out,
+                                   nullptr, state_out, stats, 0, ds, codes);
+}
+
+extern "C" int casphy_join_indel_dev(uint32_t ntip, uint32_t ncol, const uint32_t* d_codes, uint32_t nState,
+                                     const double* weight, const uint32_t* tipSize, uint32_t minSize,
+                                     float minRatio, uint32_t* edge_out, uint32_t* d_state_out,
+                                     casphy_join_stats* stats, void* stream) {
+    int rc = casphy::require_device();
+    if (rc) return rc;
+    if (!d_codes) return CASPHY_EINVAL;
+    casphy::DeviceScope ds;
+    return casphy::join_indel_impl(ntip, ncol, d_codes, nState, weight, tipSize, minSize, minRatio, edge_out,
+                                   d_state_out, nullptr, stats, (cudaStream_t)stream, ds, nullptr);
+}

@@ -1,0 +1,95 @@
+/*
+ * casphy.h -- C ABI of libcasphy.so, the B200 (sm_100a) implementation of
+ * CasPhy's tree-building hot path.
+ *
+ * Every entry point takes plain host pointers and sizes (the *_dev variants
+ * take device pointers and an optional cudaStream_t passed as void*), returns
+ * an int status (0 = CASPHY_OK) and never exits the process.  Outputs are the
+ * exact bytes the corresponding reference executable writes (minus the file
+ * headers, which the drop-in executables add).  Cited paths are relative to
+ * the CasPhy source tree.
+ */
+#ifndef CASPHY_H
+#define CASPHY_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CASPHY_ABI_VERSION 1
+
+#define CASPHY_OK 0
+#define CASPHY_EINVAL 1     /* bad argument (size, weight, code out of range) */
+#define CASPHY_ERANGE 2     /* a value exceeds a documented limit */
+#define CASPHY_ENOMEM 3     /* device or host allocation failed */
+#define CASPHY_ECUDA 4      /* CUDA runtime error (see casphy_last_error) */
+#define CASPHY_ETIMEOUT 5   /* a bounded device-side wait gave up */
+#define CASPHY_EIO 6        /* file missing / truncated (drop-in executables) */
+#define CASPHY_ENODEV 7     /* no CUDA device */
+#define CASPHY_EINTERNAL 9  /* invariant violated (bug) */
+
+int casphy_abi_version(void);
+const char *casphy_strerror(int status);
+/* Text of the last CUDA failure seen by this thread ("" if none). */
+const char *casphy_last_error(void);
+
+/* Statistics of one greedy join. */
+typedef struct {
+    uint64_t joins;              /* ntip - 1 */
+    uint64_t stale_recomputes;   /* partner-already-joined rescans */
+    uint64_t pair_scores;        /* (query, candidate) scores evaluated */
+    uint64_t compactions;        /* slot-matrix compactions */
+    uint64_t kernel_launches;    /* kernels launched by this call */
+    uint32_t int_path;           /* 1: exact integer accumulation was used */
+    uint32_t reserved;
+    double init_scan_ms;         /* device time, initial all-pairs scan */
+    double join_loop_ms;         /* device time, persistent join loop */
+    double total_ms;             /* device time of the whole call */
+} casphy_join_stats;
+
+/*
+ * Greedy shared-mutation join of indel-coded cells.
+ * Replaces the computation of `joinEdgeIndel <prefix> <wfile> <nState>
+ * <minSize> <minRatio>` (cu/joinEdgeIndel.cu:244-578).
+ *   codes     ntip x ncol u32, row-major: 0 missing, 1 unedited, >= 2 allele
+ *             (the .tbmat body; R writes mat+1L, R/CasPhy_functions.R:610)
+ *   weight    nState x ncol float64, weight of allele code c at site i is
+ *             weight[(c-2)*ncol + i] (the .w file, R/CasPhy_functions.R:609)
+ *   tipSize   ntip u32 (the .tipSize body)
+ *   edge_out  (2*ntip-2) x 2 u32: the .edge2 body (pre-order relabelled,
+ *             tips 0..ntip-1, root ntip)
+ *   state_out max(ntip-1,1) x ncol u32: the .nodeState2 body (root first)
+ * Weights must be finite and >= 0; codes must be <= nState+1 and < 65536.
+ */
+int casphy_join_indel(uint32_t ntip, uint32_t ncol, const uint32_t *codes,
+                      uint32_t nState, const double *weight, const uint32_t *tipSize,
+                      uint32_t minSize, float minRatio, uint32_t *edge_out,
+                      uint32_t *state_out, casphy_join_stats *stats);
+
+/* Same with device-resident codes / outputs (d_state_out may be NULL). */
+int casphy_join_indel_dev(uint32_t ntip, uint32_t ncol, const uint32_t *d_codes,
+                          uint32_t nState, const double *weight, const uint32_t *tipSize,
+                          uint32_t minSize, float minRatio, uint32_t *edge_out,
+                          uint32_t *d_state_out, casphy_join_stats *stats, void *stream);
+
+/*
+ * Greedy join of bit-coded cells.  Replaces `joinEdgeBitReverse <prefix>
+ * <wfile> <ancestralType>` (cu/joinEdgeBitReverse.cu:285-615).
+ *   words     ntip x nbin u32 bit rows (bit j of word k = site 32k+j)
+ *   weight    nbin*32 float64 per-site weights
+ *   ancestralType 0 (updateAncestralKernel) or non-zero (updateAncestralKernel2)
+ *   edge_out  (2*ntip-2) x 2 u32; state_out max(ntip-1,1) x nbin u32
+ */
+int casphy_join_bit(uint32_t ntip, uint32_t nbin, const uint32_t *words,
+                    const double *weight, int ancestralType, uint32_t *edge_out,
+                    uint32_t *state_out, casphy_join_stats *stats);
+int casphy_join_bit_dev(uint32_t ntip, uint32_t nbin, const uint32_t *d_words,
+                        const double *weight, int ancestralType, uint32_t *edge_out,
+                        uint32_t *d_state_out, casphy_join_stats *stats, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CASPHY_H */

@@ -77,6 +77,9 @@ uint16_t oracle_f16_add(uint16_t a, uint16_t b) {
 
 #define H_NEG_ONE ((u16)0xBC00u)
 
+/* Non-zero: always emulate the binary16 adds (tests compare both paths). */
+int oracle_force_f16 = 0;
+
 static int nthreads_or_default(int n) { return n > 0 ? n : 1; }
 
 /* ------------------------------------------------------------------ */
@@ -182,17 +185,47 @@ typedef struct {
     u32 ncol;
     const u32 *cache; /* ntip x ncol */
     const u16 *w16;   /* nState x ncol */
+    const u16 *wint;  /* integer weights when every partial sum is exact, else NULL */
 } IndelCtx;
 
-/* calculateSharedKernel (cu/joinEdgeIndel.cu:67-85) for one pair. */
+/* calculateSharedKernel (cu/joinEdgeIndel.cu:67-85) for one pair.  When all
+ * binary16 weights are integers in [0, 2048] and no score can exceed 2048,
+ * every binary16 partial sum is exact and an integer sum is the same value;
+ * the binary16 emulation is kept for every other weight table. */
 static u16 indel_score(const IndelCtx *k, u32 q, u32 c) {
     const u32 *a = k->cache + (size_t)q * k->ncol, *r = k->cache + (size_t)c * k->ncol;
+    if (k->wint) {
+        u32 s = 0;
+        for (u32 i = 0; i < k->ncol; i++) {
+            u32 t = a[i];
+            if (t == r[i] && t > 1) s += k->wint[(size_t)(t - 2) * k->ncol + i];
+        }
+        return oracle_f64_to_f16((double)s);
+    }
     u16 acc = 0;
     for (u32 i = 0; i < k->ncol; i++) {
         u32 t = a[i];
         if (t == r[i] && t > 1) acc = oracle_f16_add(acc, k->w16[(size_t)(t - 2) * k->ncol + i]);
     }
     return acc;
+}
+
+static u16 *exact_int_weights(const u16 *w16, u32 nState, u32 ncol) {
+    double total = 0;
+    for (u32 i = 0; i < ncol; i++) {
+        double mx = 0;
+        for (u32 s = 0; s < nState; s++) {
+            double v = oracle_f16_to_f64(w16[(size_t)s * ncol + i]);
+            if (!(v >= 0 && v <= 2048 && v == floor(v))) return NULL;
+            if (v > mx) mx = v;
+        }
+        total += mx;
+    }
+    if (total > 2048) return NULL;
+    u16 *wi = (u16 *)malloc(sizeof(u16) * ((size_t)nState * ncol + 1));
+    if (!wi) return NULL;
+    for (size_t j = 0; j < (size_t)nState * ncol; j++) wi[j] = (u16)oracle_f16_to_f64(w16[j]);
+    return wi;
 }
 
 /* updateAncestralKernel (cu/joinEdgeIndel.cu:87-99). */
@@ -220,13 +253,15 @@ int oracle_join_indel(uint32_t ntip, uint32_t ncol, const uint32_t *codes,
     u32 nnode = 2 * ntip - 1;
     u32 *rawState = (u32 *)malloc(sizeof(u32) * (size_t)nnode * ncol);
     u32 *nodeSize = (u32 *)malloc(sizeof(u32) * (size_t)ntip * 2);
+    u16 *wint = NULL;
     JoinBook b;
     int st = book_init(&b, ntip);
     if (st || !w16 || !cache || !localMax || !shared || !rawState || !nodeSize) { st = ORACLE_ENOMEM; goto done; }
     for (size_t i = 0; i < nw; i++) w16[i] = oracle_f64_to_f16(w[i]);
     memcpy(cache, codes, sizeof(u32) * (size_t)ntip * ncol);
     memcpy(nodeSize, tipSize, sizeof(u32) * ntip);
-    IndelCtx k = {ncol, cache, w16};
+    wint = oracle_force_f16 ? NULL : exact_int_weights(w16, nState, ncol);
+    IndelCtx k = {ncol, cache, w16, wint};
     u64 nStale = 0, nPairs = 0, nJoin = 0;
 
     /* initial upper-triangle local maxima (cu/joinEdgeIndel.cu:355-369) */
@@ -323,7 +358,7 @@ int oracle_join_indel(uint32_t ntip, uint32_t ncol, const uint32_t *codes,
     if (stats) { stats[0] = nStale; stats[1] = nPairs; stats[2] = nJoin; }
 done:
     book_free(&b);
-    free(w16); free(cache); free(localMax); free(shared); free(rawState); free(nodeSize);
+    free(w16); free(wint); free(cache); free(localMax); free(shared); free(rawState); free(nodeSize);
     return st;
 }
 

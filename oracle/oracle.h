@@ -29,6 +29,10 @@ extern "C" {
 #define ORACLE_ENOMEM 3
 #define ORACLE_EINTERNAL 9
 
+/* Non-zero forces joinEdgeIndel's binary16 emulation even when an exact
+ * integer sum would give the same values. */
+extern int oracle_force_f16;
+
 /* binary16 helpers (exposed for unit tests) */
 uint16_t oracle_f64_to_f16(double x);
 double oracle_f16_to_f64(uint16_t h);
