@@ -22,6 +22,24 @@ extern "C" int casphy_abi_version(void) { return CASPHY_ABI_VERSION; }
 
 extern "C" const char* casphy_last_error(void) { return g_last_error; }
 
+extern "C" int casphy_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+extern "C" int casphy_set_device(int device) {
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        casphy_set_last_cuda_error(e, "cudaSetDevice", __FILE__, __LINE__);
+        return CASPHY_ECUDA;
+    }
+    return CASPHY_OK;
+}
+
 extern "C" const char* casphy_strerror(int s) {
     switch (s) {
         case CASPHY_OK: return "ok";

@@ -112,22 +112,23 @@ template <bool INTP>
 __device__ __forceinline__ void accumulate(Acc8<INTP>& acc, const u16* __restrict__ col, u32 Sp, u32 cb,
                                            const u32* eSC, const u16* eW, int e0, int nE, int step) {
     int e = e0;
-    // four independent loads in flight per iteration
-    for (; e + 3 * step < nE; e += 4 * step) {
-        u32 s0 = eSC[e], s1 = eSC[e + step], s2 = eSC[e + 2 * step], s3 = eSC[e + 3 * step];
-        u32 w0 = eW[e], w1 = eW[e + step], w2 = eW[e + 2 * step], w3 = eW[e + 3 * step];
-        uint4 v0 = ld_cg_v4(col + (size_t)(s0 & 0xFFFFu) * Sp + cb);
-        uint4 v1 = ld_cg_v4(col + (size_t)(s1 & 0xFFFFu) * Sp + cb);
-        uint4 v2 = ld_cg_v4(col + (size_t)(s2 & 0xFFFFu) * Sp + cb);
-        uint4 v3 = ld_cg_v4(col + (size_t)(s3 & 0xFFFFu) * Sp + cb);
-        acc.add(v0, s0 >> 16, w0);
-        acc.add(v1, s1 >> 16, w1);
-        acc.add(v2, s2 >> 16, w2);
-        acc.add(v3, s3 >> 16, w3);
+    // eight independent 16-byte loads in flight per iteration
+    for (; e + 7 * step < nE; e += 8 * step) {
+        u32 sc[8], w[8];
+        uint4 v[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            sc[i] = eSC[e + i * step];
+            w[i] = eW[e + i * step];
+        }
+#pragma unroll
+        for (int i = 0; i < 8; i++) v[i] = ld_cg_v4(col + (size_t)(sc[i] & 0xFFFFu) * Sp + cb);
+#pragma unroll
+        for (int i = 0; i < 8; i++) acc.add(v[i], sc[i] >> 16, w[i]);
     }
     for (; e < nE; e += step) {
-        u32 s0 = eSC[e];
-        uint4 v0 = ld_cg_v4(col + (size_t)(s0 & 0xFFFFu) * Sp + cb);
+        const u32 s0 = eSC[e];
+        const uint4 v0 = ld_cg_v4(col + (size_t)(s0 & 0xFFFFu) * Sp + cb);
         acc.add(v0, s0 >> 16, eW[e]);
     }
 }
@@ -257,6 +258,7 @@ struct JoinArgs {
     u32 ntip, ncol, ncolP, nState, nnode, nCTA;
     u32 minSize;
     float minRatio;
+    int unitW;
     const u16* Wsel;
     u16* nodeRow;
     u16* colT[2];
@@ -267,13 +269,14 @@ struct JoinArgs {
     u32* nodeDeath;
     u32* nodeSize;
     u32* rawEdge;
-    BlockRec* rec;       // 2 * nCTA
-    u64* partial;        // 2 * nCTA
+    BlockRec* pub;       // 2 phases x nCTA x 2 published records (best, second)
+    u32* pubCnt;         // 2 phases x nCTA: live slots holding a real local max (capped at 3)
+    u64* partial;        // 2 phases x nCTA
     u32* counts;         // nCTA
-    GridSync* gs;
+    u32* flags;          // nCTA x 16 barrier epochs
+    int* err;
     u64 limitNs;
-    unsigned long long* statsOut;  // [0] stale [1] pairs [2] compactions [3] phases
-    u32 Sp0;
+    unsigned long long* statsOut;  // [0] stale [1] pairs [2] compactions [3] phases [4] refreshes [5] alg bytes
     u32 Rmax;            // max slots per CTA (smem for compaction ranks)
 };
 
@@ -292,12 +295,64 @@ __device__ __forceinline__ Range make_range(u32 S, u32 nCTA, u32 b) {
     return r;
 }
 
-// Block-wide argmax of (key, slot, partner) records.  Keys are unique among
-// live slots (one node per slot), so at most one thread holds the winner.
+// All-to-all flag barrier for a co-resident grid: CTA b publishes `epoch` in
+// its own flag, threads 0..nCTA-1 each wait for one CTA's flag.  Every wait
+// gives up after limit_ns and records CASPHY_ETIMEOUT.
+__device__ __forceinline__ int flag_barrier(u32* flags, u32 nCTA, u32 epoch, int* err, u64 limit_ns) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        st_release_u32(flags + blockIdx.x * 16u, epoch);
+    }
+    int fail = 0;
+    if (threadIdx.x < nCTA) {
+        const u32* f = flags + threadIdx.x * 16u;
+        if (ld_acquire_u32(f) < epoch) {
+            const u64 t0 = globaltimer_ns();
+            while (ld_acquire_u32(f) < epoch) {
+                if (*(volatile int*)err) { fail = 1; break; }
+                if (globaltimer_ns() - t0 > limit_ns) {
+                    atomicCAS(err, 0, CASPHY_ETIMEOUT);
+                    fail = 1;
+                    break;
+                }
+                __nanosleep(40);
+            }
+        }
+    }
+    return __syncthreads_or(fail);
+}
+
+__device__ __forceinline__ u16* colT_of(const JoinArgs& a, u32 buf) { return buf ? a.colT[1] : a.colT[0]; }
+__device__ __forceinline__ u32* lmOrd_of(const JoinArgs& a, u32 buf) { return buf ? a.lmOrd[1] : a.lmOrd[0]; }
+__device__ __forceinline__ u32* lmIdx_of(const JoinArgs& a, u32 buf) { return buf ? a.lmIdx[1] : a.lmIdx[0]; }
+__device__ __forceinline__ u32* slotNode_of(const JoinArgs& a, u32 buf) { return buf ? a.slotNode[1] : a.slotNode[0]; }
+
+// Per-thread top-2 of (key, slot, partner) records.
+struct Top2 {
+    u64 k0, k1;
+    u32 s0, s1, p0, p1;
+    __device__ __forceinline__ void init() {
+        k0 = k1 = 0ull;
+        s0 = s1 = kNone;
+        p0 = p1 = 0u;
+    }
+    __device__ __forceinline__ void push(u64 k, u32 s, u32 p) {
+        if (k > k0) {
+            k1 = k0; s1 = s0; p1 = p0;
+            k0 = k; s0 = s; p0 = p;
+        } else if (k > k1) {
+            k1 = k; s1 = s; p1 = p;
+        }
+    }
+};
+
+// Block-wide argmax of records (keys are unique among live slots, so at most
+// one thread holds the winner).
 __device__ __forceinline__ BlockRec block_best_rec(u64 best, u32 bslot, u32 bpart, u64* red, BlockRec* s_rec) {
     if (threadIdx.x == 0) { s_rec->slot = kNone; s_rec->partner = 0; }
     const u64 m = block_max_u64(best, red);  // starts and ends with __syncthreads
-    if (best == m && bslot != kNone) { s_rec->slot = bslot; s_rec->partner = bpart; }
+    if (best == m && bslot != kNone && m != 0ull) { s_rec->slot = bslot; s_rec->partner = bpart; }
     __syncthreads();
     BlockRec r;
     r.key = m;
@@ -307,57 +362,100 @@ __device__ __forceinline__ BlockRec block_best_rec(u64 best, u32 bslot, u32 bpar
     return r;
 }
 
-__device__ __forceinline__ u16* colT_of(const JoinArgs& a, u32 buf) { return buf ? a.colT[1] : a.colT[0]; }
-__device__ __forceinline__ u32* lmOrd_of(const JoinArgs& a, u32 buf) { return buf ? a.lmOrd[1] : a.lmOrd[0]; }
-__device__ __forceinline__ u32* lmIdx_of(const JoinArgs& a, u32 buf) { return buf ? a.lmIdx[1] : a.lmIdx[0]; }
-__device__ __forceinline__ u32* slotNode_of(const JoinArgs& a, u32 buf) { return buf ? a.slotNode[1] : a.slotNode[0]; }
+// Block top-2 from per-thread top-2 lists; returns them in out[0..1]
+// (key 0 = absent).
+__device__ __forceinline__ void block_top2(Top2 t, u64* red, BlockRec* s_rec, BlockRec* out) {
+    BlockRec r0 = block_best_rec(t.k0, t.s0, t.p0, red, s_rec);
+    if (t.k0 == r0.key && t.s0 == r0.slot && r0.key != 0ull) {
+        t.k0 = t.k1; t.s0 = t.s1; t.p0 = t.p1;
+        t.k1 = 0ull; t.s1 = kNone;
+    }
+    BlockRec r1 = block_best_rec(t.k0, t.s0, t.p0, red, s_rec);
+    out[0] = r0;
+    out[1] = r1;
+}
 
-// Best (key, slot, partner) over this CTA's slots from the stored local maxima.
-__device__ BlockRec own_best(const JoinArgs& a, u32 buf, const Range& rg, u64* red, BlockRec* s_rec) {
-    u64 best = make_key(ORD_F16_NEG1, 0u);
-    u32 bslot = kNone, bpart = 0u;
+// Publish this CTA's top-2 records and live-count for phase p.
+__device__ __forceinline__ void publish(const JoinArgs& a, u32 p, u32 b, const BlockRec* top, u32 cnt) {
+    if (threadIdx.x < 2) {
+        BlockRec* dst = a.pub + ((size_t)(p & 1) * a.nCTA + b) * 2 + threadIdx.x;
+        const BlockRec r = top[threadIdx.x];
+        asm volatile("st.global.cg.v2.u64 [%0], {%1, %2};" ::"l"(dst), "l"(r.key),
+                     "l"(((u64)r.partner << 32) | r.slot)
+                     : "memory");
+    }
+    if (threadIdx.x == 2) a.pubCnt[(p & 1) * a.nCTA + b] = cnt;
+}
+
+// Local copy of every CTA's published top-2 list.  tab[2b], tab[2b+1];
+// cnt[b] entries valid; exact[b]: the list holds every live slot of block b
+// that carries a real local maximum.
+struct Table {
+    BlockRec* tab;
+    unsigned char* cnt;
+    unsigned char* exact;
+};
+
+__device__ void load_table(const JoinArgs& a, u32 p, Table t) {
+    for (u32 i = threadIdx.x; i < a.nCTA * 2; i += kThreads) {
+        const uint4 v = ld_cg_v4(a.pub + (size_t)(p & 1) * a.nCTA * 2 + i);
+        BlockRec r;
+        r.key = ((u64)v.y << 32) | v.x;
+        r.slot = v.z;
+        r.partner = v.w;
+        t.tab[i] = r;
+    }
+    for (u32 i = threadIdx.x; i < a.nCTA; i += kThreads) {
+        const u32 n = ld_cg_u32(a.pubCnt + (p & 1) * a.nCTA + i);
+        t.cnt[i] = (unsigned char)min(n, 2u);
+        t.exact[i] = n <= 2;
+    }
+    __syncthreads();
+}
+
+// Own top-2 straight from the stored local maxima (refresh / compaction).
+__device__ void own_top2(const JoinArgs& a, u32 buf, const Range& rg, u64* red, BlockRec* s_rec, BlockRec* out,
+                         u32* cntOut, u32* wsum) {
+    Top2 t;
+    t.init();
+    u32 n = 0;
     const u32* sn = slotNode_of(a, buf);
     const u32* lo = lmOrd_of(a, buf);
     const u32* li = lmIdx_of(a, buf);
     for (u32 c = rg.lo + threadIdx.x; c < rg.hi; c += kThreads) {
         const u32 node = ld_cg_u32(sn + c);
         if (node == kDead) continue;
-        const u64 key = make_key(ld_cg_u32(lo + c), node);
-        if (key > best) { best = key; bslot = c; bpart = ld_cg_u32(li + c); }
+        const u32 o = ld_cg_u32(lo + c);
+        if (o == ORD_F16_NEG1) continue;
+        n++;
+        t.push(make_key(o, node), c, ld_cg_u32(li + c));
     }
-    return block_best_rec(best, bslot, bpart, red, s_rec);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xFFFFFFFFu, n, o);
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = n;
+    block_top2(t, red, s_rec, out);  // contains __syncthreads
+    u32 tot = 0;
+    for (int w = 0; w < kThreads / 32; w++) tot += wsum[w];
+    *cntOut = tot;
+    __syncthreads();
 }
 
-__device__ __forceinline__ void put_rec(BlockRec* dst, const BlockRec& r) {
-    if (threadIdx.x == 0) {
-        asm volatile("st.global.cg.v2.u64 [%0], {%1, %2};" ::"l"(dst), "l"(r.key),
-                     "l"(((u64)r.partner << 32) | r.slot)
-                     : "memory");
-    }
-}
-
-// Every CTA reduces the same per-CTA records, so all reach the same join.
-__device__ BlockRec global_best(const BlockRec* src, u32 nCTA, u64* red, BlockRec* s_rec) {
-    u64 best = 0;
-    u32 slot = kNone, partner = 0;
-    for (u32 i = threadIdx.x; i < nCTA; i += kThreads) {
-        const uint4 v = ld_cg_v4(src + i);
-        const u64 key = ((u64)v.y << 32) | v.x;
-        if (key > best) { best = key; slot = v.z; partner = v.w; }
-    }
-    return block_best_rec(best, slot, partner, red, s_rec);
-}
-
-// Builds the query site list from a row.  mode 0: query = row1 (global);
-// 1: copy row2; 2: keep row1; 3: ancestral merge of row1 and row2
-// (updateAncestralKernel, cu/joinEdgeIndel.cu:87-99).  The merged row is
-// also kept in shared memory (mrow) for the write-back.
+// Builds the query site list (ascending sites with code > 1) from a row.
+// mode 0: query = row1; 1: copy row2; 2: keep row1; 3: ancestral merge of
+// row1 and row2 (updateAncestralKernel, cu/joinEdgeIndel.cu:87-99).  The row
+// is also left in shared memory (mrow) for the write-back.
 __device__ int build_query(const JoinArgs& a, const u16* row1, const u16* row2, int mode, u16* mrow, u32* eSC,
                            u16* eW, u32* wcount) {
     const u32 lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    int base = 0;
-    for (u32 s0 = 0; s0 < a.ncolP; s0 += kThreads) {
-        const u32 s = s0 + threadIdx.x;
+    // each thread owns a contiguous run of `per` sites so one block scan
+    // keeps the list ascending
+    const u32 per = (a.ncolP + kThreads - 1) / kThreads;
+    const u32 s0 = threadIdx.x * per;
+    u32 cnt = 0;
+    u32 codes[4];
+    const bool small = per <= 4;
+    for (u32 i = 0; i < per; i++) {
+        const u32 s = s0 + i;
         u32 c = 0;
         if (s < a.ncol) {
             const u32 x = ld_cg_u16(row1 + s);
@@ -370,40 +468,54 @@ __device__ int build_query(const JoinArgs& a, const u16* row1, const u16* row2, 
             }
         }
         if (s < a.ncolP && mrow) mrow[s] = (u16)c;
-        const bool ed = c > 1;
-        const u32 bal = __ballot_sync(0xFFFFFFFFu, ed);
-        if (lane == 0) wcount[wid] = __popc(bal);
-        __syncthreads();
-        if (threadIdx.x < 32) {
-            u32 v = threadIdx.x < (kThreads / 32) ? wcount[threadIdx.x] : 0u;
-            u32 incl = v;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                u32 n = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-                if (lane >= (u32)o) incl += n;
-            }
-            if (threadIdx.x < (kThreads / 32)) wcount[16 + threadIdx.x] = incl - v;
-            if (threadIdx.x == 31) wcount[15 + 16 + 1] = incl;
-        }
-        __syncthreads();
-        if (ed) {
-            const u32 pos = base + wcount[16 + wid] + __popc(bal & ((1u << lane) - 1u));
-            eSC[pos] = s | (c << 16);
-            eW[pos] = a.Wsel[(size_t)(c - 2) * a.ncol + s];
-        }
-        base += (int)wcount[32];
-        __syncthreads();
+        if (small) codes[i] = c;
+        cnt += c > 1;
     }
-    return base;
+    u32 incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const u32 n = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= (u32)o) incl += n;
+    }
+    if (lane == 31) wcount[wid] = incl;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const u32 v = threadIdx.x < kThreads / 32 ? wcount[threadIdx.x] : 0u;
+        u32 wi = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const u32 n = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+            if (lane >= (u32)o) wi += n;
+        }
+        if (threadIdx.x < kThreads / 32) wcount[16 + threadIdx.x] = wi - v;
+        if (threadIdx.x == 31) wcount[32] = wi;
+    }
+    __syncthreads();
+    u32 pos = wcount[16 + wid] + incl - cnt;
+    for (u32 i = 0; i < per; i++) {
+        const u32 s = s0 + i;
+        u32 c;
+        if (small) c = codes[i];
+        else c = s < a.ncolP && mrow ? mrow[s] : (s < a.ncol ? ld_cg_u16(row1 + s) : 0u);
+        if (c > 1) {
+            eSC[pos] = s | (c << 16);
+            eW[pos] = a.unitW ? (u16)1 : a.Wsel[(size_t)(c - 2) * a.ncol + s];
+            pos++;
+        }
+    }
+    const int n = (int)wcount[32];
+    __syncthreads();
+    return n;
 }
 
-// Scores this CTA's live slots against the query list.  STALE: returns the
-// best (score, node) key over slots != c1.  JOIN: updates the local maxima
-// (strict improvement, cu/joinEdgeIndel.cu:453-460) and returns the CTA's
-// best record over all its live slots.
+// Scores this CTA's live slots against the query list.
+// STALE: returns (in top[0]) the best (score, node) over slots != c1.
+// JOIN: updates local maxima (strict improvement, cu/joinEdgeIndel.cu:453-460)
+// and returns the CTA's top-2 records; *cntOut = slots with a real maximum.
 template <bool INTP, bool JOIN>
-__device__ BlockRec scan_own(const JoinArgs& a, u32 buf, const Range& rg, int nE, const u32* eSC, const u16* eW,
-                             u16* part, u32 c1, u32 newNode, u64* red, BlockRec* s_rec) {
+__device__ void scan_own(const JoinArgs& a, u32 buf, const Range& rg, int nE, const u32* eSC, const u16* eW,
+                         u16* part, u32 c1, u32 newNode, u64* red, BlockRec* s_rec, BlockRec* top, u32* cntOut,
+                         u32* wsum) {
     const u32 R = rg.hi - rg.lo;
     int F = 1;
     if (INTP) {
@@ -412,8 +524,12 @@ __device__ BlockRec scan_own(const JoinArgs& a, u32 buf, const Range& rg, int nE
     const u32 cap = kCap / F;
     const u32 Tg = kThreads / F;
     const u32 g = threadIdx.x / Tg, t = threadIdx.x % Tg;
-    u64 best = make_key(ORD_F16_NEG1, 0u);
-    u32 bslot = kNone, bpart = 0;
+    Top2 tt;
+    tt.init();
+    u32 n = 0;
+    const u32* sn = slotNode_of(a, buf);
+    u32* lop = lmOrd_of(a, buf);
+    u32* lip = lmIdx_of(a, buf);
     for (u32 base = rg.lo; base < rg.hi; base += cap) {
         const u32 cb = base + t * kG;
         Acc8<INTP> acc;
@@ -424,7 +540,7 @@ __device__ BlockRec scan_own(const JoinArgs& a, u32 buf, const Range& rg, int nE
         for (u32 x = threadIdx.x; x < cap; x += kThreads) {
             const u32 c = base + x;
             if (c >= rg.hi) break;
-            const u32 node = ld_cg_u32(slotNode_of(a, buf) + c);
+            const u32 node = ld_cg_u32(sn + c);
             if (node == kDead || c == c1) continue;
             u32 hb;
             if (INTP) {
@@ -436,8 +552,6 @@ __device__ BlockRec scan_own(const JoinArgs& a, u32 buf, const Range& rg, int nE
             }
             const u32 o = ord_f16((u16)hb);
             if (JOIN) {
-                u32* lop = lmOrd_of(a, buf);
-                u32* lip = lmIdx_of(a, buf);
                 u32 lo = ld_cg_u32(lop + c);
                 u32 li;
                 if (o > lo) {
@@ -448,48 +562,97 @@ __device__ BlockRec scan_own(const JoinArgs& a, u32 buf, const Range& rg, int nE
                 } else {
                     li = ld_cg_u32(lip + c);
                 }
-                const u64 key = make_key(lo, node);
-                if (key > best) { best = key; bslot = c; bpart = li; }
+                if (lo != ORD_F16_NEG1) {
+                    n++;
+                    tt.push(make_key(lo, node), c, li);
+                }
             } else {
-                const u64 key = make_key(o, node);
-                if (key > best) { best = key; bslot = c; }
+                tt.push(make_key(o, node), c, 0u);
             }
         }
         __syncthreads();
     }
-    return block_best_rec(best, bslot, bpart, red, s_rec);
+    if (JOIN) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xFFFFFFFFu, n, o);
+        if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = n;
+        block_top2(tt, red, s_rec, top);
+        u32 tot = 0;
+        for (int w = 0; w < kThreads / 32; w++) tot += wsum[w];
+        *cntOut = tot;
+        __syncthreads();
+    } else {
+        top[0] = block_best_rec(tt.k0, tt.s0, 0u, red, s_rec);
+    }
+}
+
+// Decision shared by every CTA: the best published record over all blocks.
+// Returns false when a block's best is unknown (its list was used up by
+// stale updates) so the owners must republish first.
+__device__ bool table_best(const Table& t, u32 nCTA, BlockRec* s_best, u64* red) {
+    __shared__ int s_unknown;
+    if (threadIdx.x == 0) s_unknown = 0;
+    __syncthreads();
+    u64 best = 0ull;
+    u32 bi = kNone;
+    for (u32 i = threadIdx.x; i < nCTA; i += kThreads) {
+        if (t.cnt[i] == 0) {
+            if (!t.exact[i]) s_unknown = 1;
+            continue;
+        }
+        if (t.tab[2 * i].key > best) { best = t.tab[2 * i].key; bi = i; }
+    }
+    const u64 m = block_max_u64(best, red);
+    if (best == m && bi != kNone) *s_best = t.tab[2 * bi];
+    __syncthreads();
+    const bool ok = s_unknown == 0 && m != 0ull;
+    return ok;
 }
 
 template <bool INTP>
 __global__ void __launch_bounds__(kThreads, 1) k_join(JoinArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
-    u16* part = reinterpret_cast<u16*>(smem);                    // kCap u16
-    u32* eSC = reinterpret_cast<u32*>(part + kCap);              // ncol
-    u32* ranks = eSC + a.ncol;                                   // Rmax
-    u16* eW = reinterpret_cast<u16*>(ranks + a.Rmax);            // ncol
-    u16* mrow = eW + ((a.ncol + 7u) & ~7u);                      // ncolP
+    u16* part = reinterpret_cast<u16*>(smem);                          // kCap u16
+    BlockRec* tabRec = reinterpret_cast<BlockRec*>(part + kCap);       // 2*nCTA
+    u32* eSC = reinterpret_cast<u32*>(tabRec + 2 * a.nCTA);            // ncol
+    u32* ranks = eSC + a.ncol;                                         // Rmax
+    u16* eW = reinterpret_cast<u16*>(ranks + a.Rmax);                  // ncol (rounded to 8)
+    u16* mrow = eW + ((a.ncol + 7u) & ~7u);                            // ncolP
+    unsigned char* tabCnt = reinterpret_cast<unsigned char*>(mrow + a.ncolP);  // nCTA
+    unsigned char* tabExact = tabCnt + a.nCTA;                         // nCTA
     __shared__ u64 red[32];
-    __shared__ BlockRec s_rec;
+    __shared__ BlockRec s_rec, s_best;
+    __shared__ BlockRec s_top[2];
     __shared__ u32 wcount[40];
+    __shared__ u32 wsum[16];
     __shared__ u32 s_val[4];
 
+    const Table T{tabRec, tabCnt, tabExact};
     const u32 b = blockIdx.x, nCTA = a.nCTA;
-    if (threadIdx.x == 0) { s_rec.slot = kNone; s_rec.partner = 0; }
-    __syncthreads();
     u32 buf = 0;
     Range rg = make_range(a.ntip, nCTA, b);
     u32 k = 0, p = 0;
-    unsigned long long nStale = 0, nPairs = 0, nComp = 0;
+    unsigned long long nStale = 0, nPairs = 0, nComp = 0, nRefresh = 0, algBytes = 0;
     const u32 nJoin = a.ntip - 1;
     int fail = 0;
+    u32 cnt = 0;
 
-    BlockRec my = own_best(a, buf, rg, red, &s_rec);
-    put_rec(a.rec + b, my);
-    if (grid_barrier(a.gs, nCTA, a.limitNs)) goto out;
-    p = 1;
+    own_top2(a, buf, rg, red, &s_rec, s_top, &cnt, wsum);
+    publish(a, p, b, s_top, cnt);
+    if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
+    load_table(a, p - 1, T);
 
     while (k < nJoin) {
-        const BlockRec g = global_best(a.rec + ((p - 1) & 1) * nCTA, nCTA, red, &s_rec);
+        if (!table_best(T, nCTA, &s_best, red)) {
+            // a block's best is unknown: every CTA republishes from its slots
+            own_top2(a, buf, rg, red, &s_rec, s_top, &cnt, wsum);
+            publish(a, p, b, s_top, cnt);
+            nRefresh++;
+            if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
+            load_table(a, p - 1, T);
+            continue;
+        }
+        const BlockRec g = s_best;
         const u32 j1 = key_node(g.key), c1 = g.slot, j2 = g.partner;
         if (c1 >= rg.S || j1 >= a.nnode || j2 >= a.nnode) { fail = CASPHY_EINTERNAL; break; }
         if (threadIdx.x == 0) {
@@ -505,33 +668,55 @@ __global__ void __launch_bounds__(kThreads, 1) k_join(JoinArgs a) {
         if (stale) {
             // rescore j1 against every live slot (cu/joinEdgeIndel.cu:387-399)
             const int nE = build_query(a, a.nodeRow + (size_t)j1 * a.ncolP, nullptr, 0, nullptr, eSC, eW, wcount);
-            BlockRec pr = scan_own<INTP, false>(a, buf, rg, nE, eSC, eW, part, c1, 0u, red, &s_rec);
+            scan_own<INTP, false>(a, buf, rg, nE, eSC, eW, part, c1, 0u, red, &s_rec, s_top, nullptr, wsum);
             if (threadIdx.x == 0) {
-                asm volatile("st.global.cg.u64 [%0], %1;" ::"l"(a.partial + (p & 1) * nCTA + b), "l"(pr.key) : "memory");
+                asm volatile("st.global.cg.u64 [%0], %1;" ::"l"(a.partial + (p & 1) * nCTA + b), "l"(s_top[0].key)
+                             : "memory");
             }
-            put_rec(a.rec + (p & 1) * nCTA + b, my);
             nStale++;
             nPairs += (a.ntip - k) - 1;
-            if (grid_barrier(a.gs, nCTA, a.limitNs)) goto out;
-            p++;
-            // combine the partial argmaxes and store the new local max of c1
-            u64 pb = 0;
+            algBytes += 2ull * (u64)nE * ((a.ntip - k) - 1);
+            if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
+            u64 pb = make_key(ORD_F16_NEG1, 0u);
             for (u32 i = threadIdx.x; i < nCTA; i += kThreads) {
                 const u64 v = ld_cg_u64(a.partial + ((p - 1) & 1) * nCTA + i);
                 pb = v > pb ? v : pb;
             }
             pb = block_max_u64(pb, red);
-            if (c1 >= rg.lo && c1 < rg.hi) {
-                if (threadIdx.x == 0) {
-                    lmOrd_of(a, buf)[c1] = key_ord(pb);
-                    lmIdx_of(a, buf)[c1] = key_node(pb);
-                }
-                __syncthreads();
-                my = own_best(a, buf, rg, red, &s_rec);
+            const u32 vOrd = key_ord(pb), vIdx = key_node(pb);
+            const u32 ob = c1 / rg.R;  // owner CTA of c1
+            if (ob == b && threadIdx.x == 0) {
+                lmOrd_of(a, buf)[c1] = vOrd;
+                lmIdx_of(a, buf)[c1] = vIdx;
             }
-            put_rec(a.rec + (p & 1) * nCTA + b, my);
-            if (grid_barrier(a.gs, nCTA, a.limitNs)) goto out;
-            p++;
+            // replace c1's entry (the head of its owner's list) in the table
+            if (threadIdx.x == 0) {
+                BlockRec nr;
+                nr.key = make_key(vOrd, j1);
+                nr.slot = c1;
+                nr.partner = vIdx;
+                BlockRec* L = T.tab + 2 * ob;
+                unsigned char n = T.cnt[ob];
+                // drop the head (c1)
+                if (n == 2) L[0] = L[1];
+                n = n > 0 ? n - 1 : 0;
+                const bool real = vOrd != ORD_F16_NEG1;
+                if (T.exact[ob]) {
+                    if (real) {
+                        if (n == 0) L[0] = nr;
+                        else if (nr.key > L[0].key) { L[1] = L[0]; L[0] = nr; }
+                        else L[1] = nr;
+                        n++;
+                    }
+                    if (n > 2) n = 2;
+                } else if (n >= 1 && real && nr.key > L[n - 1].key) {
+                    if (nr.key > L[0].key) { L[1] = L[0]; L[0] = nr; }
+                    else L[1] = nr;
+                    n = 2;
+                }
+                T.cnt[ob] = n;
+            }
+            __syncthreads();
             continue;
         }
         // join j1 and j2 into node ntip+k (cu/joinEdgeIndel.cu:402-467)
@@ -569,12 +754,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_join(JoinArgs a) {
             lmOrd_of(a, buf)[c2] = ORD_F16_NEG1;
         }
         __syncthreads();
-        my = scan_own<INTP, true>(a, buf, rg, nE, eSC, eW, part, c1, newNode, red, &s_rec);
-        put_rec(a.rec + (p & 1) * nCTA + b, my);
+        scan_own<INTP, true>(a, buf, rg, nE, eSC, eW, part, c1, newNode, red, &s_rec, s_top, &cnt, wsum);
+        publish(a, p, b, s_top, cnt);
         nPairs += (a.ntip - k - 1) - 1;
+        algBytes += 2ull * (u64)nE * ((a.ntip - k - 1) - 1);
         k++;
-        if (grid_barrier(a.gs, nCTA, a.limitNs)) goto out;
-        p++;
+        if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
+        load_table(a, p - 1, T);
 
         // squeeze dead slots out when fewer than 3/4 are alive
         const u32 alive = a.ntip - k;
@@ -595,8 +781,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_join(JoinArgs a) {
                 }
                 __syncthreads();
             }
-            if (grid_barrier(a.gs, nCTA, a.limitNs)) goto out;
-            p++;
+            if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
             // C2: new positions = exclusive prefix of the per-CTA live counts
             if (threadIdx.x == 0) {
                 u32 off = 0, tot = 0;
@@ -628,8 +813,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_join(JoinArgs a) {
                 const u32 lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
                 for (int o = 1; o < 32; o <<= 1) {
-                    u32 n = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-                    if (lane >= (u32)o) incl += n;
+                    u32 nn = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                    if (lane >= (u32)o) incl += nn;
                 }
                 if (lane == 31) wcount[wid] = incl;
                 __syncthreads();
@@ -637,8 +822,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_join(JoinArgs a) {
                     u32 wv = threadIdx.x < kThreads / 32 ? wcount[threadIdx.x] : 0u, wi = wv;
 #pragma unroll
                     for (int o = 1; o < 32; o <<= 1) {
-                        u32 n = __shfl_up_sync(0xFFFFFFFFu, wi, o);
-                        if (lane >= (u32)o) wi += n;
+                        u32 nn = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+                        if (lane >= (u32)o) wi += nn;
                     }
                     if (threadIdx.x < kThreads / 32) wcount[16 + threadIdx.x] = wi - wv;
                 }
@@ -673,26 +858,26 @@ __global__ void __launch_bounds__(kThreads, 1) k_join(JoinArgs a) {
                 snN[Snew + threadIdx.x] = kDead;
                 loN[Snew + threadIdx.x] = ORD_F16_NEG1;
             }
-            if (grid_barrier(a.gs, nCTA, a.limitNs)) goto out;
-            p++;
-            // C3: switch to the compacted buffers
+            if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
+            // C3: switch to the compacted buffers and republish
             buf = nb;
             rg = make_range(Snew, nCTA, b);
-            my = own_best(a, buf, rg, red, &s_rec);
-            put_rec(a.rec + (p & 1) * nCTA + b, my);
+            own_top2(a, buf, rg, red, &s_rec, s_top, &cnt, wsum);
+            publish(a, p, b, s_top, cnt);
             nComp++;
-            if (grid_barrier(a.gs, nCTA, a.limitNs)) goto out;
-            p++;
+            if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
+            load_table(a, p - 1, T);
         }
     }
 out:
-    if (fail && threadIdx.x == 0) atomicCAS(&a.gs->err, 0, fail);
+    if (fail && threadIdx.x == 0) atomicCAS(a.err, 0, fail);
     if (b == 0 && threadIdx.x == 0) {
         a.statsOut[0] = nStale;
         a.statsOut[1] = nPairs;
         a.statsOut[2] = nComp;
         a.statsOut[3] = p;
-        a.statsOut[4] = buf;
+        a.statsOut[4] = nRefresh;
+        a.statsOut[5] = algBytes;
     }
 }
 
@@ -778,11 +963,12 @@ void preorder_relabel(u32 ntip, const u32* rawEdge, u32* edge_out, std::vector<u
 // integer path: every weight a non-negative integer and the largest reachable
 // score (sum over sites of the site's largest weight) at most 2048.
 static int convert_weights(u32 nState, u32 ncol, const double* w, std::vector<u16>& hbits, std::vector<u16>& wint,
-                           bool& intPath) {
+                           bool& intPath, bool& unitW) {
     const size_t n = (size_t)nState * ncol;
     hbits.resize(n ? n : 1);
     wint.resize(n ? n : 1);
     intPath = true;
+    unitW = true;
     double maxSum = 0;
     std::vector<double> colMax(ncol, 0.0);
     for (size_t i = 0; i < n; i++) {
@@ -797,11 +983,13 @@ static int convert_weights(u32 nState, u32 ncol, const double* w, std::vector<u1
         const float hf = __half2float(h);
         if (!(hf == std::floor(hf) && hf <= 2048.0f)) intPath = false;
         wint[i] = intPath ? (u16)hf : 0;
+        if (hf != 1.0f) unitW = false;
         colMax[i % ncol] = std::max(colMax[i % ncol], (double)hf);
     }
     for (u32 i = 0; i < ncol; i++) maxSum += colMax[i];
     if (maxSum > 2048.0) intPath = false;
     if ((u64)nState + 1 > 0x7FFFu) intPath = false;  // packed-lane compare needs codes < 0x8000
+    if (!intPath) unitW = false;
     return CASPHY_OK;
 }
 
@@ -815,8 +1003,8 @@ static int join_indel_impl(u32 ntip, u32 ncol, const u32* d_codes, u32 nState, c
         return CASPHY_ERANGE;
     }
     std::vector<u16> hbits, wint;
-    bool intPath = false;
-    int rc = convert_weights(nState, ncol, weight, hbits, wint, intPath);
+    bool intPath = false, unitW = false;
+    int rc = convert_weights(nState, ncol, weight, hbits, wint, intPath, unitW);
     if (rc) return rc;
     casphy_join_stats lst{};
     lst.int_path = intPath ? 1 : 0;
@@ -834,7 +1022,7 @@ static int join_indel_impl(u32 ntip, u32 ncol, const u32* d_codes, u32 nState, c
         struct L {
             u32* codes; u16* Wsel; u16* nodeRow; u16* colT0; u16* colT1; u32* lm[6];
             u32* node2slot; u32* nodeDeath; u32* nodeSize; u32* rawEdge; u32* eSC; u16* eW; u32* eLen;
-            unsigned long long* initKey; BlockRec* rec; u64* partial; u32* counts; GridSync* gs;
+            unsigned long long* initKey; BlockRec* pub; u32* pubCnt; u64* partial; u32* counts; u32* flags; int* jerr;
             unsigned long long* tileCounter; u64* chunkStart; unsigned long long* stats; u32* order; u32* tipSize;
             u32* stateOut; int* err;
         } l;
@@ -852,10 +1040,12 @@ static int join_indel_impl(u32 ntip, u32 ncol, const u32* d_codes, u32 nState, c
         l.eW = c.take<u16>((size_t)ntip * ncol);
         l.eLen = c.take<u32>(ntip);
         l.initKey = c.take<unsigned long long>(ntip);
-        l.rec = c.take<BlockRec>(2 * nCTA);
+        l.pub = c.take<BlockRec>(4 * nCTA);
+        l.pubCnt = c.take<u32>(2 * nCTA);
         l.partial = c.take<u64>(2 * nCTA);
         l.counts = c.take<u32>(nCTA);
-        l.gs = c.take<GridSync>(1);
+        l.flags = c.take<u32>(16 * nCTA);
+        l.jerr = c.take<int>(1);
         l.tileCounter = c.take<unsigned long long>(1);
         l.chunkStart = c.take<u64>(1024);
         l.stats = c.take<unsigned long long>(8);
@@ -884,7 +1074,8 @@ static int join_indel_impl(u32 ntip, u32 ncol, const u32* d_codes, u32 nState, c
                                     cudaMemcpyHostToDevice, st));
     CASPHY_CUDA_TRY(cudaMemcpyAsync(L.tipSize, tipSize, sizeof(u32) * ntip, cudaMemcpyHostToDevice, st));
     CASPHY_CUDA_TRY(cudaMemsetAsync(L.err, 0, sizeof(int), st));
-    CASPHY_CUDA_TRY(cudaMemsetAsync(L.gs, 0, sizeof(GridSync), st));
+    CASPHY_CUDA_TRY(cudaMemsetAsync(L.flags, 0, sizeof(u32) * 16 * nCTA, st));
+    CASPHY_CUDA_TRY(cudaMemsetAsync(L.jerr, 0, sizeof(int), st));
     CASPHY_CUDA_TRY(cudaMemsetAsync(L.tileCounter, 0, sizeof(unsigned long long), st));
     CASPHY_CUDA_TRY(cudaMemsetAsync(L.stats, 0, sizeof(unsigned long long) * 8, st));
     u64 launches = 0;
@@ -929,16 +1120,17 @@ static int join_indel_impl(u32 ntip, u32 ncol, const u32* d_codes, u32 nState, c
     launches++;
     JoinArgs ja{};
     ja.ntip = ntip; ja.ncol = ncol; ja.ncolP = ncolP; ja.nState = nState; ja.nnode = nnode; ja.nCTA = nCTA;
-    ja.minSize = minSize; ja.minRatio = minRatio; ja.Wsel = L.Wsel; ja.nodeRow = L.nodeRow;
+    ja.minSize = minSize; ja.minRatio = minRatio; ja.unitW = unitW ? 1 : 0; ja.Wsel = L.Wsel; ja.nodeRow = L.nodeRow;
     ja.colT[0] = L.colT0; ja.colT[1] = L.colT1;
     ja.lmOrd[0] = L.lm[0]; ja.lmIdx[0] = L.lm[1]; ja.slotNode[0] = L.lm[2];
     ja.lmOrd[1] = L.lm[3]; ja.lmIdx[1] = L.lm[4]; ja.slotNode[1] = L.lm[5];
     ja.node2slot = L.node2slot; ja.nodeDeath = L.nodeDeath; ja.nodeSize = L.nodeSize; ja.rawEdge = L.rawEdge;
-    ja.rec = L.rec; ja.partial = L.partial; ja.counts = L.counts; ja.gs = L.gs;
+    ja.pub = L.pub; ja.pubCnt = L.pubCnt; ja.partial = L.partial; ja.counts = L.counts; ja.flags = L.flags;
+    ja.err = L.jerr;
     ja.limitNs = 20ull * 1000 * 1000 * 1000;
-    ja.statsOut = L.stats; ja.Sp0 = Sp; ja.Rmax = Rmax;
-    const size_t smemBytes = sizeof(u16) * kCap + sizeof(u32) * ncol + sizeof(u32) * Rmax +
-                             sizeof(u16) * (((ncol + 7u) & ~7u) + ncolP) + 64;
+    ja.statsOut = L.stats; ja.Rmax = Rmax;
+    const size_t smemBytes = sizeof(u16) * kCap + sizeof(BlockRec) * 2 * nCTA + sizeof(u32) * ncol +
+                             sizeof(u32) * Rmax + sizeof(u16) * (((ncol + 7u) & ~7u) + ncolP) + 2 * nCTA + 64;
     if (ntip >= 2) {
         void* fn = intPath ? (void*)k_join<true> : (void*)k_join<false>;
         CASPHY_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemBytes));
@@ -953,23 +1145,25 @@ static int join_indel_impl(u32 ntip, u32 ncol, const u32* d_codes, u32 nState, c
         launches++;
     }
     CASPHY_CUDA_TRY(cudaEventRecord(ev[3], st));
+    std::vector<u32> eLenH(ntip);
+    CASPHY_CUDA_TRY(cudaMemcpyAsync(eLenH.data(), L.eLen, sizeof(u32) * ntip, cudaMemcpyDeviceToHost, st));
     std::vector<u32> raw((size_t)2 * nedge + 2);
     unsigned long long hst[8] = {0};
     int herr = 0;
-    GridSync hgs{};
+    int hjerr = 0;
     CASPHY_CUDA_TRY(cudaMemcpyAsync(raw.data(), L.rawEdge, sizeof(u32) * 2 * nedge, cudaMemcpyDeviceToHost, st));
     CASPHY_CUDA_TRY(cudaMemcpyAsync(hst, L.stats, sizeof(hst), cudaMemcpyDeviceToHost, st));
     CASPHY_CUDA_TRY(cudaMemcpyAsync(&herr, L.err, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CASPHY_CUDA_TRY(cudaMemcpyAsync(&hgs, L.gs, sizeof(GridSync), cudaMemcpyDeviceToHost, st));
+    CASPHY_CUDA_TRY(cudaMemcpyAsync(&hjerr, L.jerr, sizeof(int), cudaMemcpyDeviceToHost, st));
     CASPHY_CUDA_TRY(cudaStreamSynchronize(st));
     if (herr) {
         casphy_set_last_error_msg("cell codes exceed nState+1 (or 65535)");
         return herr;
     }
-    if (hgs.err) {
-        casphy_set_last_error_msg(hgs.err == CASPHY_ETIMEOUT ? "join loop grid barrier timed out"
-                                                              : "join loop invariant violated");
-        return hgs.err;
+    if (hjerr) {
+        casphy_set_last_error_msg(hjerr == CASPHY_ETIMEOUT ? "join loop grid barrier timed out"
+                                                            : "join loop invariant violated");
+        return hjerr;
     }
     std::vector<u32> order;
     const u32 nrows = std::max(ntip - 1, 1u);
@@ -1003,6 +1197,10 @@ static int join_indel_impl(u32 ntip, u32 ncol, const u32* d_codes, u32 nState, c
     lst.init_scan_ms = t12;
     lst.join_loop_ms = t23;
     lst.total_ms = t04;
+    for (u32 i = 0; i + 1 < ntip; i++) lst.alg_bytes_init += 2ull * eLenH[i] * (u64)(ntip - 1 - i);
+    lst.alg_bytes_join = hst[5];
+    lst.phases = hst[3];
+    lst.refreshes = hst[4];
     if (stats) *stats = lst;
     return CASPHY_OK;
 }

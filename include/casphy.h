@@ -34,6 +34,10 @@ int casphy_abi_version(void);
 const char *casphy_strerror(int status);
 /* Text of the last CUDA failure seen by this thread ("" if none). */
 const char *casphy_last_error(void);
+/* Number of visible CUDA devices (0 if none) and selection of the device the
+ * calling thread's subsequent calls run on. */
+int casphy_device_count(void);
+int casphy_set_device(int device);
 
 /* Statistics of one greedy join. */
 typedef struct {
@@ -47,6 +51,10 @@ typedef struct {
     double init_scan_ms;         /* device time, initial all-pairs scan */
     double join_loop_ms;         /* device time, persistent join loop */
     double total_ms;             /* device time of the whole call */
+    uint64_t alg_bytes_init;     /* algorithmic bytes of the initial scan */
+    uint64_t alg_bytes_join;     /* algorithmic bytes of the join-loop scans */
+    uint64_t phases;             /* grid-wide phases of the join loop */
+    uint64_t refreshes;          /* republish phases (exhausted per-CTA lists) */
 } casphy_join_stats;
 
 /*
@@ -73,21 +81,6 @@ int casphy_join_indel_dev(uint32_t ntip, uint32_t ncol, const uint32_t *d_codes,
                           uint32_t nState, const double *weight, const uint32_t *tipSize,
                           uint32_t minSize, float minRatio, uint32_t *edge_out,
                           uint32_t *d_state_out, casphy_join_stats *stats, void *stream);
-
-/*
- * Greedy join of bit-coded cells.  Replaces `joinEdgeBitReverse <prefix>
- * <wfile> <ancestralType>` (cu/joinEdgeBitReverse.cu:285-615).
- *   words     ntip x nbin u32 bit rows (bit j of word k = site 32k+j)
- *   weight    nbin*32 float64 per-site weights
- *   ancestralType 0 (updateAncestralKernel) or non-zero (updateAncestralKernel2)
- *   edge_out  (2*ntip-2) x 2 u32; state_out max(ntip-1,1) x nbin u32
- */
-int casphy_join_bit(uint32_t ntip, uint32_t nbin, const uint32_t *words,
-                    const double *weight, int ancestralType, uint32_t *edge_out,
-                    uint32_t *state_out, casphy_join_stats *stats);
-int casphy_join_bit_dev(uint32_t ntip, uint32_t nbin, const uint32_t *d_words,
-                        const double *weight, int ancestralType, uint32_t *edge_out,
-                        uint32_t *d_state_out, casphy_join_stats *stats, void *stream);
 
 #ifdef __cplusplus
 }
