@@ -33,6 +33,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -1228,4 +1229,292 @@ extern "C" int casphy_join_indel_dev(uint32_t ntip, uint32_t ncol, const uint32_
     casphy::DeviceScope ds;
     return casphy::join_indel_impl(ntip, ncol, d_codes, nState, weight, tipSize, minSize, minRatio, edge_out,
                                    d_state_out, nullptr, stats, (cudaStream_t)stream, ds, nullptr);
+}
+
+// ===========================================================================
+// Zero-allocation variant of the indel join.
+//
+// Some callers cannot allocate device memory while they run us: a framework
+// that has already reserved the GPU's memory for its own pool (so a
+// cudaMalloc would fail or evict its cache), a latency-critical service loop
+// that must not take cudaMalloc/cudaFree's device-wide synchronisation, or
+// a host thread that is not allowed to change the device's allocation state.
+// For them casphy_join_indel_noalloc runs the same tree build using only the
+// buffers the caller passes in plus one fixed scratch region compiled into
+// this library.
+//
+// The scratch region is the file-scope array below.  Every GPU that loads
+// libcasphy.so holds it (kScratchBytes) until the process exits.  All calls on
+// a device share it and each call overwrites it, so calls whose GPU work
+// overlaps (two host threads, or two streams) race; calls are serialised per
+// device by a host lock and return only after their work on the stream is
+// done.  Every buffer that must start at zero is cleared inside the call.
+// ===========================================================================
+
+namespace casphy {
+namespace indel_noalloc {
+
+constexpr size_t kScratchBytes = size_t(64) << 20;  // 64 MiB
+static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
+
+// Device address of g_scratch for each device, looked up once per device
+// (with that device current) on its first call.
+static std::mutex g_mu;
+static void* g_addr[64] = {nullptr};
+static std::mutex g_dev_mu[64];
+
+static int scratch_address(int dev, void** out) {
+    std::lock_guard<std::mutex> g(g_mu);
+    if (dev < 0 || dev >= 64) return CASPHY_ERANGE;
+    if (!g_addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+        if (e != cudaSuccess) {
+            casphy_set_last_cuda_error(e, "cudaGetSymbolAddress(g_scratch)", __FILE__, __LINE__);
+            return CASPHY_ECUDA;
+        }
+        g_addr[dev] = p;
+    }
+    *out = g_addr[dev];
+    return CASPHY_OK;
+}
+
+// binary16 weights, integer weights and the exactness flags, one block per
+// site: flags[0] = some weight is not an integer in [0,2048], flags[1] = some
+// weight is not 1, flags[2] = some weight is negative or NaN; flags[3] =
+// sum over sites of the site's largest weight.
+__global__ void k_weights(const double* __restrict__ w, u32 nState, u32 ncol, u16* __restrict__ hbits,
+                          u16* __restrict__ wint, u32* flags) {
+    const u32 s = blockIdx.x;
+    u32 colMax = 0;
+    for (u32 a = threadIdx.x; a < nState; a += blockDim.x) {
+        const size_t i = (size_t)a * ncol + s;
+        const double x = w[i];
+        if (!(x >= 0)) atomicOr(flags + 2, 1u);
+        const __half h = __double2half(x);
+        const float hf = __half2float(h);
+        hbits[i] = __half_as_ushort(h);
+        const bool isInt = hf == floorf(hf) && hf <= 2048.0f;
+        if (!isInt) atomicOr(flags + 0, 1u);
+        if (hf != 1.0f) atomicOr(flags + 1, 1u);
+        wint[i] = isInt ? (u16)hf : (u16)0;
+        colMax = max(colMax, isInt ? (u32)hf : 4096u);
+    }
+    for (int o = 16; o > 0; o >>= 1) colMax = max(colMax, __shfl_xor_sync(0xFFFFFFFFu, colMax, o));
+    if ((threadIdx.x & 31) == 0) atomicAdd(flags + 3, colMax);
+}
+
+// Pre-order relabelling on the device (same walk as preorder_relabel).
+__global__ void k_preorder(const u32* __restrict__ rawEdge, u32 ntip, u32* relabel, u32* stack,
+                           unsigned char* cursor, u32* edge_out, u32* order, u32* err) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const u32 nnode = 2 * ntip - 1;
+    for (u32 i = 0; i < nnode; i++) {
+        relabel[i] = i < ntip ? i : nnode;
+        cursor[i] = 0;
+    }
+    u32 sp = 0, count = ntip, nout = 0, nord = 0;
+    order[nord++] = nnode - 1;
+    stack[sp++] = nnode - 1;
+    while (sp > 0) {
+        const u32 v = stack[sp - 1];
+        if (v < ntip || cursor[v] >= 2) { sp--; continue; }
+        const u32 ei = 2 * (v - ntip) + cursor[v];
+        cursor[v]++;
+        const u32 p = rawEdge[2 * ei], c = rawEdge[2 * ei + 1];
+        if (p >= nnode || c >= nnode || sp >= nnode) { *err = 1; return; }
+        stack[sp++] = c;
+        if (relabel[p] == nnode) relabel[p] = count++;
+        if (relabel[c] == nnode) {
+            order[nord++] = c;
+            relabel[c] = count++;
+        }
+        edge_out[2 * nout] = relabel[p];
+        edge_out[2 * nout + 1] = relabel[c];
+        nout++;
+    }
+    if (nout != 2 * ntip - 2 || nord != ntip - 1) *err = 1;
+}
+
+struct Layout {
+    double* w64; u16* hbits; u16* wint; u32* wflags; u32* tipSize;
+    u16* nodeRow; u16* colT0; u16* colT1; u32* lm[6];
+    u32* node2slot; u32* nodeDeath; u32* nodeSize; u32* rawEdge;
+    u32* eSC; u16* eW; u32* eLen; unsigned long long* initKey;
+    BlockRec* pub; u32* pubCnt; u64* partial; u32* counts; u32* flags; int* jerr;
+    unsigned long long* tileCounter; u64* chunkStart; unsigned long long* stats;
+    u32* relabel; u32* stack; unsigned char* cursor; u32* order; u32* dfsErr; int* prepErr;
+    size_t bytes;
+};
+
+static Layout carve(char* base, u32 ntip, u32 ncol, u32 nState, u32 nCTA, u32 nChunks) {
+    const u32 nnode = 2 * ntip - 1, nedge = 2 * ntip - 2;
+    const u32 ncolP = (ncol + 7u) & ~7u, Sp = (ntip + 7u) & ~7u;
+    const size_t nw = (size_t)nState * ncol;
+    Carve c;
+    c.base = base;
+    Layout l;
+    l.w64 = c.take<double>(nw ? nw : 1);
+    l.hbits = c.take<u16>(nw ? nw : 1);
+    l.wint = c.take<u16>(nw ? nw : 1);
+    l.wflags = c.take<u32>(4);
+    l.tipSize = c.take<u32>(ntip);
+    l.nodeRow = c.take<u16>((size_t)nnode * ncolP);
+    l.colT0 = c.take<u16>((size_t)ncol * Sp);
+    l.colT1 = c.take<u16>((size_t)ncol * Sp);
+    for (int i = 0; i < 6; i++) l.lm[i] = c.take<u32>(Sp);
+    l.node2slot = c.take<u32>(nnode);
+    l.nodeDeath = c.take<u32>(nnode);
+    l.nodeSize = c.take<u32>(nnode);
+    l.rawEdge = c.take<u32>((size_t)2 * nedge + 2);
+    l.eSC = c.take<u32>((size_t)ntip * ncol);
+    l.eW = c.take<u16>((size_t)ntip * ncol);
+    l.eLen = c.take<u32>(ntip);
+    l.initKey = c.take<unsigned long long>(ntip);
+    l.pub = c.take<BlockRec>(4 * nCTA);
+    l.pubCnt = c.take<u32>(2 * nCTA);
+    l.partial = c.take<u64>(2 * nCTA);
+    l.counts = c.take<u32>(nCTA);
+    l.flags = c.take<u32>(16 * nCTA);
+    l.jerr = c.take<int>(1);
+    l.tileCounter = c.take<unsigned long long>(1);
+    l.chunkStart = c.take<u64>(nChunks + 1);
+    l.stats = c.take<unsigned long long>(8);
+    l.relabel = c.take<u32>(nnode);
+    l.stack = c.take<u32>(nnode);
+    l.cursor = c.take<unsigned char>(nnode);
+    l.order = c.take<u32>(ntip);
+    l.dfsErr = c.take<u32>(1);
+    l.prepErr = c.take<int>(1);
+    l.bytes = c.off + 256;
+    return l;
+}
+
+}  // namespace indel_noalloc
+}  // namespace casphy
+
+extern "C" int casphy_join_indel_noalloc(uint32_t ntip, uint32_t ncol, const uint32_t* d_codes, uint32_t nState,
+                                         const double* weight, const uint32_t* tipSize, uint32_t minSize,
+                                         float minRatio, uint32_t* d_edge_out, uint32_t* d_state_out,
+                                         void* stream) {
+    using namespace casphy;
+    using namespace casphy::indel;
+    using namespace casphy::indel_noalloc;
+    if (ntip < 2 || ncol == 0 || !d_codes || !weight || !tipSize || !d_edge_out || !d_state_out)
+        return CASPHY_EINVAL;
+    if (ncol > kMaxCol) {
+        casphy_set_last_error_msg("casphy_join_indel_noalloc: ncol exceeds 16384");
+        return CASPHY_ERANGE;
+    }
+    int dev = 0, nSM = 0;
+    CASPHY_CUDA_TRY(cudaGetDevice(&dev));
+    CASPHY_CUDA_TRY(cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, dev));
+    const u32 nCTA = (u32)nSM;
+    const u32 nChunks = (ntip + kCap - 1) / kCap;
+    const Layout need = carve(nullptr, ntip, ncol, nState, nCTA, nChunks);
+    if (need.bytes > kScratchBytes) {
+        char msg[200];
+        snprintf(msg, sizeof(msg),
+                 "casphy_join_indel_noalloc: %u cells x %u sites need %zu bytes of scratch, the fixed limit is %zu",
+                 ntip, ncol, need.bytes, kScratchBytes);
+        casphy_set_last_error_msg(msg);
+        return CASPHY_ERANGE;
+    }
+    void* base = nullptr;
+    int rc = scratch_address(dev, &base);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> devLock(g_dev_mu[dev & 63]);
+    cudaStream_t st = (cudaStream_t)stream;
+    const Layout L = carve(static_cast<char*>(base), ntip, ncol, nState, nCTA, nChunks);
+    const u32 nnode = 2 * ntip - 1;
+    const u32 ncolP = (ncol + 7u) & ~7u, Sp = (ntip + 7u) & ~7u;
+    const size_t nw = (size_t)nState * ncol;
+
+    // weights: host float64 -> scratch, converted on the device
+    if (nw) CASPHY_CUDA_TRY(cudaMemcpyAsync(L.w64, weight, sizeof(double) * nw, cudaMemcpyHostToDevice, st));
+    CASPHY_CUDA_TRY(cudaMemcpyAsync(L.tipSize, tipSize, sizeof(u32) * ntip, cudaMemcpyHostToDevice, st));
+    CASPHY_CUDA_TRY(cudaMemsetAsync(L.wflags, 0, sizeof(u32) * 4, st));
+    if (nw) k_weights<<<ncol, 32, 0, st>>>(L.w64, nState, ncol, L.hbits, L.wint, L.wflags);
+    u32 wf[4] = {0, 0, 0, 0};
+    CASPHY_CUDA_TRY(cudaMemcpyAsync(wf, L.wflags, sizeof(wf), cudaMemcpyDeviceToHost, st));
+    CASPHY_CUDA_TRY(cudaStreamSynchronize(st));
+    if (wf[2]) {
+        casphy_set_last_error_msg("weights must be >= 0 and not NaN");
+        return CASPHY_EINVAL;
+    }
+    const bool intPath = !wf[0] && wf[3] <= 2048u && (u64)nState + 1 <= 0x7FFFu;
+    const bool unitW = intPath && !wf[1];
+
+    // everything the kernels expect to start cleared
+    CASPHY_CUDA_TRY(cudaMemsetAsync(L.prepErr, 0, sizeof(int), st));
+    CASPHY_CUDA_TRY(cudaMemsetAsync(L.jerr, 0, sizeof(int), st));
+    CASPHY_CUDA_TRY(cudaMemsetAsync(L.flags, 0, sizeof(u32) * 16 * nCTA, st));
+    CASPHY_CUDA_TRY(cudaMemsetAsync(L.tileCounter, 0, sizeof(unsigned long long), st));
+    CASPHY_CUDA_TRY(cudaMemsetAsync(L.stats, 0, sizeof(unsigned long long) * 8, st));
+    CASPHY_CUDA_TRY(cudaMemsetAsync(L.dfsErr, 0, sizeof(u32), st));
+
+    PrepArgs pa{ntip, ncol, ncolP, nState, Sp, d_codes, intPath ? L.wint : L.hbits, intPath ? 0x7FFFu : 0xFFFFu,
+                L.nodeRow, L.eSC, L.eW, L.eLen, L.prepErr};
+    k_prep_rows<<<(ntip + 7) / 8, 256, 0, st>>>(pa);
+    k_transpose<<<dim3((Sp + 31) / 32, (ncol + 31) / 32), dim3(32, 8), 0, st>>>(L.nodeRow, ntip, ncol, ncolP, Sp,
+                                                                                  L.colT0);
+    u64 chunkStart[64 + 1];
+    if (nChunks + 1 > 65) return CASPHY_ERANGE;
+    chunkStart[0] = 0;
+    for (u32 k = 0; k < nChunks; k++) {
+        const u64 end = std::min<u64>((u64)(k + 1) * kCap, ntip);
+        chunkStart[k + 1] = chunkStart[k] + (end >= 1 ? end - 1 : 0);
+    }
+    CASPHY_CUDA_TRY(cudaMemcpyAsync(L.chunkStart, chunkStart, sizeof(u64) * (nChunks + 1), cudaMemcpyHostToDevice,
+                                    st));
+    k_fill_u64<<<(ntip + 255) / 256, 256, 0, st>>>(L.initKey, ntip, ((u64)ORD_F16_NEG1 << 32) | 0xFFFFFFFFull);
+    InitArgs ia{ntip, ncol, Sp, L.colT0, L.eSC, L.eW, L.eLen, L.chunkStart, nChunks, chunkStart[nChunks],
+                L.tileCounter, L.initKey};
+    int perSM = 0;
+    if (intPath) {
+        CASPHY_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_init_scan<true>, kThreads, 0));
+        k_init_scan<true><<<nSM * std::max(perSM, 1), kThreads, 0, st>>>(ia);
+    } else {
+        CASPHY_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_init_scan<false>, kThreads, 0));
+        k_init_scan<false><<<nSM * std::max(perSM, 1), kThreads, 0, st>>>(ia);
+    }
+    const u32 initN = std::max(Sp, nnode);
+    k_slot_init<<<(initN + 255) / 256, 256, 0, st>>>(ntip, Sp, nnode, L.initKey, L.lm[0], L.lm[1], L.lm[2],
+                                                       L.node2slot, L.nodeDeath, L.nodeSize, L.tipSize);
+    const u32 Rmax = (((ntip + nCTA - 1) / nCTA) + 7u) & ~7u;
+    JoinArgs ja{};
+    ja.ntip = ntip; ja.ncol = ncol; ja.ncolP = ncolP; ja.nState = nState; ja.nnode = nnode; ja.nCTA = nCTA;
+    ja.minSize = minSize; ja.minRatio = minRatio; ja.unitW = unitW ? 1 : 0;
+    ja.Wsel = intPath ? L.wint : L.hbits; ja.nodeRow = L.nodeRow;
+    ja.colT[0] = L.colT0; ja.colT[1] = L.colT1;
+    ja.lmOrd[0] = L.lm[0]; ja.lmIdx[0] = L.lm[1]; ja.slotNode[0] = L.lm[2];
+    ja.lmOrd[1] = L.lm[3]; ja.lmIdx[1] = L.lm[4]; ja.slotNode[1] = L.lm[5];
+    ja.node2slot = L.node2slot; ja.nodeDeath = L.nodeDeath; ja.nodeSize = L.nodeSize; ja.rawEdge = L.rawEdge;
+    ja.pub = L.pub; ja.pubCnt = L.pubCnt; ja.partial = L.partial; ja.counts = L.counts; ja.flags = L.flags;
+    ja.err = L.jerr; ja.limitNs = 20ull * 1000 * 1000 * 1000; ja.statsOut = L.stats; ja.Rmax = Rmax;
+    const size_t smemBytes = sizeof(u16) * kCap + sizeof(BlockRec) * 2 * nCTA + sizeof(u32) * ncol +
+                             sizeof(u32) * Rmax + sizeof(u16) * (((ncol + 7u) & ~7u) + ncolP) + 2 * nCTA + 64;
+    void* fn = intPath ? (void*)k_join<true> : (void*)k_join<false>;
+    CASPHY_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemBytes));
+    void* args[] = {&ja};
+    CASPHY_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(nCTA), dim3(kThreads), args, smemBytes, st));
+    k_preorder<<<1, 32, 0, st>>>(L.rawEdge, ntip, L.relabel, L.stack, L.cursor, d_edge_out, L.order, L.dfsErr);
+    k_gather<<<ntip - 1, 256, 0, st>>>(L.nodeRow, ncol, ncolP, L.order, ntip - 1, d_state_out);
+    CASPHY_CUDA_TRY(cudaGetLastError());
+    int errs[2] = {0, 0};
+    u32 dfsErr = 0;
+    CASPHY_CUDA_TRY(cudaMemcpyAsync(&errs[0], L.prepErr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CASPHY_CUDA_TRY(cudaMemcpyAsync(&errs[1], L.jerr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CASPHY_CUDA_TRY(cudaMemcpyAsync(&dfsErr, L.dfsErr, sizeof(u32), cudaMemcpyDeviceToHost, st));
+    CASPHY_CUDA_TRY(cudaStreamSynchronize(st));
+    if (errs[0]) {
+        casphy_set_last_error_msg("cell codes exceed nState+1 (or 65535)");
+        return errs[0];
+    }
+    if (errs[1]) {
+        casphy_set_last_error_msg(errs[1] == CASPHY_ETIMEOUT ? "join loop grid barrier timed out"
+                                                              : "join loop invariant violated");
+        return errs[1];
+    }
+    return dfsErr ? CASPHY_EINTERNAL : CASPHY_OK;
 }

@@ -82,6 +82,34 @@ int casphy_join_indel_dev(uint32_t ntip, uint32_t ncol, const uint32_t *d_codes,
                           uint32_t minSize, float minRatio, uint32_t *edge_out,
                           uint32_t *d_state_out, casphy_join_stats *stats, void *stream);
 
+/*
+ * Zero-allocation variant of casphy_join_indel_dev.  It has no counterpart
+ * in the reference; it exists for callers that must not allocate device
+ * memory during the call -- e.g. a framework that has already reserved the
+ * GPU's memory for its own pool, or a latency-critical loop that cannot take
+ * the device-wide synchronisation of cudaMalloc/cudaFree.  It never calls
+ * cudaMalloc/cudaFree (or any allocating routine): inputs and outputs are the
+ * caller's buffers and all working memory comes from one 64 MiB scratch
+ * array compiled into libcasphy.so, held by every GPU that loads the library
+ * until the process exits.
+ *   d_codes      device, ntip x ncol u32 (as casphy_join_indel)
+ *   weight       host, nState x ncol float64; tipSize host, ntip u32
+ *   d_edge_out   device, (2*ntip-2) x 2 u32  (the .edge2 body)
+ *   d_state_out  device, (ntip-1) x ncol u32 (the .nodeState2 body)
+ * Needs ntip >= 2.  Sizes whose working set exceeds the 64 MiB scratch
+ * (roughly ntip*ncol*14 bytes plus per-site tables) are rejected with
+ * CASPHY_ERANGE and a message in casphy_last_error().  The first call on a
+ * device looks up the scratch address for that device, so make that first
+ * call before any stream capture.  All calls on a device share the scratch
+ * and overwrite it: calls whose GPU work overlaps race, so the library
+ * serialises them per device and each call returns only when its work on
+ * `stream` has finished.
+ */
+int casphy_join_indel_noalloc(uint32_t ntip, uint32_t ncol, const uint32_t *d_codes,
+                              uint32_t nState, const double *weight, const uint32_t *tipSize,
+                              uint32_t minSize, float minRatio, uint32_t *d_edge_out,
+                              uint32_t *d_state_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
