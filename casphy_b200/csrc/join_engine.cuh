@@ -1,0 +1,565 @@
+// Persistent greedy-join engine shared by the indel and bit joins.
+//
+// The reference joins (cu/joinEdgeIndel.cu:376-468, cu/joinEdgeBitReverse.cu:
+// 404-505) repeat: take the global best local maximum (larger value, then
+// smaller node index; reduction seeded with (-1, 0)); if that row's partner
+// is already joined, rescore the row against every live row and retry;
+// otherwise join the two rows into a new node stored in the first row's
+// slot, score the new node against every live row and raise the local maxima
+// it strictly improves.
+//
+// Here one cooperative launch runs the whole loop, one CTA per SM.  CTA b
+// owns a contiguous range of slots and everything stored per slot.  Each
+// phase ends with an all-to-all flag barrier whose waits are bounded by
+// %globaltimer.  After every join each CTA publishes the two best (key,
+// slot, partner) records of its range; every CTA keeps an identical table of
+// all published records, so it derives the next join by itself.  A stale
+// partner costs one scoring phase: the owner stores the row's new maximum and
+// every CTA patches its copy of the owner's list (the list keeps its
+// invariant "every unlisted live slot ranks below the last entry"; when it
+// runs dry the CTAs republish).  When fewer than half the slots are alive
+// the slots are renumbered densely (compaction).
+//
+// A Model supplies the data-specific parts: how a query is built (stale row
+// or merged children), where node and slot data live, how one pass of
+// candidate scores is computed, and how slot data moves in a compaction.
+#pragma once
+#include "common.cuh"
+
+namespace casphy {
+namespace joinx {
+
+constexpr int kThreads = 512;
+constexpr u32 kDead = 0xFFFFFFFFu;
+constexpr u32 kNone = 0xFFFFFFFFu;
+constexpr u32 kMaxCap = 4096;  // candidates per scoring pass (ordOut in smem)
+
+struct BlockRec {
+    u64 key;
+    u32 slot;
+    u32 partner;
+};
+
+struct Common {
+    u32 ntip, nnode, nCTA;
+    u32 align;            // slot ranges start at multiples of this (8 or 32)
+    u32* lmOrd[2];
+    u32* lmIdx[2];
+    u32* slotNode[2];
+    u32* node2slot;
+    u32* nodeDeath;
+    u32* nodeSize;
+    u32* rawEdge;
+    BlockRec* pub;        // 2 phases x nCTA x 2
+    u32* pubCnt;          // 2 phases x nCTA
+    u64* partial;         // 2 phases x nCTA
+    u32* counts;          // nCTA
+    u32* flags;           // nCTA x 16
+    int* err;
+    u64 limitNs;
+    unsigned long long* statsOut;  // [0] stale [1] pairs [2] compactions [3] phases [4] refreshes [5] alg bytes
+    u32 Rmax;
+    u32 ordNeg1;          // ordered key of the value -1
+    u32 compactMin;       // do not compact below this many slots
+    u32 compactQ8;        // compact when alive*256 < slots*compactQ8
+    u32 bytesPerPairSite; // algorithmic bytes per (candidate, query entry), x1000
+};
+
+struct Range {
+    u32 S, Sp, R, lo, hi;
+};
+
+__device__ __forceinline__ Range make_range(u32 S, u32 nCTA, u32 b, u32 align) {
+    Range r;
+    r.S = S;
+    r.Sp = (S + align - 1) / align * align;
+    const u32 per = (S + nCTA - 1) / nCTA;
+    r.R = (per + align - 1) / align * align;
+    r.lo = min(b * r.R, S);
+    r.hi = min(r.lo + r.R, S);
+    return r;
+}
+
+__device__ __forceinline__ u32* lmOrd_of(const Common& a, u32 buf) { return buf ? a.lmOrd[1] : a.lmOrd[0]; }
+__device__ __forceinline__ u32* lmIdx_of(const Common& a, u32 buf) { return buf ? a.lmIdx[1] : a.lmIdx[0]; }
+__device__ __forceinline__ u32* slotNode_of(const Common& a, u32 buf) { return buf ? a.slotNode[1] : a.slotNode[0]; }
+
+// All-to-all flag barrier for a co-resident grid: CTA b publishes `epoch`
+// in its own flag; threads 0..nCTA-1 each wait for one CTA's flag.  Every
+// wait gives up after limit_ns and records CASPHY_ETIMEOUT.
+__device__ __forceinline__ int flag_barrier(u32* flags, u32 nCTA, u32 epoch, int* err, u64 limit_ns) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        st_release_u32(flags + blockIdx.x * 16u, epoch);
+    }
+    int fail = 0;
+    if (threadIdx.x < nCTA) {
+        const u32* f = flags + threadIdx.x * 16u;
+        if (ld_acquire_u32(f) < epoch) {
+            const u64 t0 = globaltimer_ns();
+            while (ld_acquire_u32(f) < epoch) {
+                if (*(volatile int*)err) { fail = 1; break; }
+                if (globaltimer_ns() - t0 > limit_ns) {
+                    atomicCAS(err, 0, CASPHY_ETIMEOUT);
+                    fail = 1;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+    }
+    return __syncthreads_or(fail);
+}
+
+struct Top2 {
+    u64 k0, k1;
+    u32 s0, s1, p0, p1;
+    __device__ __forceinline__ void init() {
+        k0 = k1 = 0ull;
+        s0 = s1 = kNone;
+        p0 = p1 = 0u;
+    }
+    __device__ __forceinline__ void push(u64 k, u32 s, u32 p) {
+        if (k > k0) {
+            k1 = k0; s1 = s0; p1 = p0;
+            k0 = k; s0 = s; p0 = p;
+        } else if (k > k1) {
+            k1 = k; s1 = s; p1 = p;
+        }
+    }
+};
+
+// Block-wide argmax of records (keys are unique among live slots).
+__device__ __forceinline__ BlockRec block_best_rec(u64 best, u32 bslot, u32 bpart, u64* red, BlockRec* s_rec) {
+    if (threadIdx.x == 0) { s_rec->slot = kNone; s_rec->partner = 0; }
+    const u64 m = block_max_u64(best, red);
+    if (best == m && bslot != kNone && m != 0ull) { s_rec->slot = bslot; s_rec->partner = bpart; }
+    __syncthreads();
+    BlockRec r;
+    r.key = m;
+    r.slot = s_rec->slot;
+    r.partner = s_rec->partner;
+    __syncthreads();
+    return r;
+}
+
+__device__ __forceinline__ void block_top2(Top2 t, u64* red, BlockRec* s_rec, BlockRec* out) {
+    const BlockRec r0 = block_best_rec(t.k0, t.s0, t.p0, red, s_rec);
+    if (t.k0 == r0.key && t.s0 == r0.slot && r0.key != 0ull) {
+        t.k0 = t.k1; t.s0 = t.s1; t.p0 = t.p1;
+        t.k1 = 0ull; t.s1 = kNone;
+    }
+    const BlockRec r1 = block_best_rec(t.k0, t.s0, t.p0, red, s_rec);
+    if (threadIdx.x == 0) {
+        out[0] = r0;
+        out[1] = r1;
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ u32 block_sum_u32(u32 v, u32* wsum) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = v;
+    __syncthreads();
+    u32 t = 0;
+    for (int w = 0; w < kThreads / 32; w++) t += wsum[w];
+    __syncthreads();
+    return t;
+}
+
+__device__ __forceinline__ void publish(const Common& a, u32 p, u32 b, const BlockRec* top, u32 cnt) {
+    if (threadIdx.x < 2) {
+        BlockRec* dst = a.pub + ((size_t)(p & 1) * a.nCTA + b) * 2 + threadIdx.x;
+        const BlockRec r = top[threadIdx.x];
+        asm volatile("st.global.cg.v2.u64 [%0], {%1, %2};" ::"l"(dst), "l"(r.key),
+                     "l"(((u64)r.partner << 32) | r.slot)
+                     : "memory");
+    }
+    if (threadIdx.x == 2) a.pubCnt[(p & 1) * a.nCTA + b] = cnt;
+}
+
+struct Table {
+    BlockRec* tab;
+    unsigned char* cnt;
+    unsigned char* exact;
+};
+
+__device__ inline void load_table(const Common& a, u32 p, Table t) {
+    for (u32 i = threadIdx.x; i < a.nCTA * 2; i += kThreads) {
+        const uint4 v = ld_cg_v4(a.pub + (size_t)(p & 1) * a.nCTA * 2 + i);
+        BlockRec r;
+        r.key = ((u64)v.y << 32) | v.x;
+        r.slot = v.z;
+        r.partner = v.w;
+        t.tab[i] = r;
+    }
+    for (u32 i = threadIdx.x; i < a.nCTA; i += kThreads) {
+        const u32 n = ld_cg_u32(a.pubCnt + (p & 1) * a.nCTA + i);
+        t.cnt[i] = (unsigned char)min(n, 2u);
+        t.exact[i] = n <= 2;
+    }
+    __syncthreads();
+}
+
+// Top-2 of the stored local maxima of this CTA's slots (refresh/compaction).
+__device__ inline void own_top2(const Common& a, u32 buf, const Range& rg, u64* red, BlockRec* s_rec, BlockRec* out,
+                         u32* cntOut, u32* wsum) {
+    Top2 t;
+    t.init();
+    u32 n = 0;
+    const u32* sn = slotNode_of(a, buf);
+    const u32* lo = lmOrd_of(a, buf);
+    const u32* li = lmIdx_of(a, buf);
+    for (u32 c = rg.lo + threadIdx.x; c < rg.hi; c += kThreads) {
+        const u32 node = ld_cg_u32(sn + c);
+        if (node == kDead) continue;
+        const u32 o = ld_cg_u32(lo + c);
+        if (o == a.ordNeg1) continue;
+        n++;
+        t.push(make_key(o, node), c, ld_cg_u32(li + c));
+    }
+    *cntOut = block_sum_u32(n, wsum);
+    block_top2(t, red, s_rec, out);
+}
+
+// The best published record over all blocks; false when some block's best
+// is unknown (its list ran dry under stale patches).
+__device__ inline bool table_best(const Table& t, u32 nCTA, BlockRec* s_best, u64* red, int* s_flag) {
+    if (threadIdx.x == 0) *s_flag = 0;
+    __syncthreads();
+    u64 best = 0ull;
+    u32 bi = kNone;
+    for (u32 i = threadIdx.x; i < nCTA; i += kThreads) {
+        if (t.cnt[i] == 0) {
+            if (!t.exact[i]) *s_flag = 1;
+            continue;
+        }
+        if (t.tab[2 * i].key > best) { best = t.tab[2 * i].key; bi = i; }
+    }
+    const u64 m = block_max_u64(best, red);
+    if (best == m && bi != kNone) *s_best = t.tab[2 * bi];
+    __syncthreads();
+    return *s_flag == 0 && m != 0ull;
+}
+
+// Exclusive ranks of this CTA's live slots (ordered), written to ranks[c-lo]
+// (kNone for dead); also moves the per-slot engine arrays to buffer nb.
+__device__ inline void compact_slots(const Common& a, u32 buf, u32 nb, const Range& rg, u32 off, u32* ranks, u32* wcount) {
+    const u32* sn = slotNode_of(a, buf);
+    u32* snN = slotNode_of(a, nb);
+    u32* loN = lmOrd_of(a, nb);
+    u32* liN = lmIdx_of(a, nb);
+    const u32* lo = lmOrd_of(a, buf);
+    const u32* li = lmIdx_of(a, buf);
+    const u32 R = rg.hi - rg.lo;
+    const u32 per = (R + kThreads - 1) / kThreads;
+    const u32 c0 = rg.lo + threadIdx.x * per;
+    const u32 cEnd = min(c0 + per, rg.hi);
+    u32 v = 0;
+    for (u32 c = c0; c < cEnd; c++) v += ld_cg_u32(sn + c) != kDead;
+    u32 incl = v;
+    const u32 lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const u32 n = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= (u32)o) incl += n;
+    }
+    if (lane == 31) wcount[wid] = incl;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const u32 wv = threadIdx.x < kThreads / 32 ? wcount[threadIdx.x] : 0u;
+        u32 wi = wv;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const u32 n = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+            if (lane >= (u32)o) wi += n;
+        }
+        if (threadIdx.x < kThreads / 32) wcount[16 + threadIdx.x] = wi - wv;
+    }
+    __syncthreads();
+    u32 r = off + wcount[16 + wid] + incl - v;
+    for (u32 c = c0; c < cEnd; c++) {
+        const u32 node = ld_cg_u32(sn + c);
+        if (node != kDead) {
+            ranks[c - rg.lo] = r;
+            snN[r] = node;
+            loN[r] = ld_cg_u32(lo + c);
+            liN[r] = ld_cg_u32(li + c);
+            a.node2slot[node] = r;
+            r++;
+        } else {
+            ranks[c - rg.lo] = kNone;
+        }
+    }
+    __syncthreads();
+}
+
+template <class M>
+__global__ void __launch_bounds__(kThreads, 1) k_join(Common a, typename M::Args m) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    u32* ordOut = reinterpret_cast<u32*>(smem);                        // kMaxCap
+    BlockRec* tabRec = reinterpret_cast<BlockRec*>(ordOut + kMaxCap);  // 2*nCTA
+    u32* ranks = reinterpret_cast<u32*>(tabRec + 2 * a.nCTA);          // Rmax
+    unsigned char* tabCnt = reinterpret_cast<unsigned char*>(ranks + a.Rmax);
+    unsigned char* tabExact = tabCnt + a.nCTA;
+    unsigned char* msm = smem + M::engine_smem_bytes(a.nCTA, a.Rmax);  // model shared memory
+    typename M::Smem ms;
+    M::carve_smem(m, msm, ms);
+    __shared__ u64 red[32];
+    __shared__ BlockRec s_rec, s_best;
+    __shared__ BlockRec s_top[2];
+    __shared__ u32 wcount[40];
+    __shared__ u32 wsum[16];
+    __shared__ u32 s_val[4];
+    __shared__ int s_flag;
+
+    const Table T{tabRec, tabCnt, tabExact};
+    const u32 b = blockIdx.x, nCTA = a.nCTA;
+    u32 buf = 0;
+    Range rg = make_range(a.ntip, nCTA, b, a.align);
+    u32 k = 0, p = 0;
+    unsigned long long nStale = 0, nPairs = 0, nComp = 0, nRefresh = 0, algMilli = 0;
+    const u32 nJoin = a.ntip - 1;
+    int fail = 0;
+    u32 cnt = 0;
+
+    own_top2(a, buf, rg, red, &s_rec, s_top, &cnt, wsum);
+    publish(a, p, b, s_top, cnt);
+    if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
+    load_table(a, p - 1, T);
+
+    while (k < nJoin) {
+        if (!table_best(T, nCTA, &s_best, red, &s_flag)) {
+            own_top2(a, buf, rg, red, &s_rec, s_top, &cnt, wsum);
+            publish(a, p, b, s_top, cnt);
+            nRefresh++;
+            if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
+            load_table(a, p - 1, T);
+            continue;
+        }
+        const BlockRec g = s_best;
+        const u32 j1 = key_node(g.key), c1 = g.slot, j2 = g.partner;
+        if (c1 >= rg.S || j1 >= a.nnode || j2 >= a.nnode) { fail = CASPHY_EINTERNAL; break; }
+        if (threadIdx.x == 0) {
+            s_val[0] = ld_cg_u32(a.nodeDeath + j2);
+            s_val[1] = ld_cg_u32(a.node2slot + j2);
+            s_val[2] = ld_cg_u32(a.nodeSize + j1);
+            s_val[3] = ld_cg_u32(a.nodeSize + j2);
+        }
+        __syncthreads();
+        const u32 death = s_val[0], c2 = s_val[1], s1 = s_val[2], s2 = s_val[3];
+        __syncthreads();
+        const bool stale = death < k || c2 >= rg.S;
+        if (stale) {
+            // rescore j1 against every live slot
+            const int nE = M::build_stale(m, ms, j1, wcount);
+            Top2 tt;
+            tt.init();
+            const u32* sn = slotNode_of(a, buf);
+            const u32 cap = M::pass_cap(m, rg.hi - rg.lo);
+            for (u32 base = rg.lo; base < rg.hi; base += cap) {
+                M::score_pass(m, ms, buf, rg, base, cap, nE, ordOut);
+                for (u32 x = threadIdx.x; x < cap && base + x < rg.hi; x += kThreads) {
+                    const u32 c = base + x;
+                    const u32 node = ld_cg_u32(sn + c);
+                    if (node == kDead || c == c1) continue;
+                    tt.push(make_key(ordOut[x], node), c, 0u);
+                }
+                __syncthreads();
+            }
+            const BlockRec pr = block_best_rec(tt.k0, tt.s0, 0u, red, &s_rec);
+            if (threadIdx.x == 0) {
+                asm volatile("st.global.cg.u64 [%0], %1;" ::"l"(a.partial + (p & 1) * nCTA + b), "l"(pr.key)
+                             : "memory");
+            }
+            nStale++;
+            nPairs += (a.ntip - k) - 1;
+            algMilli += (unsigned long long)a.bytesPerPairSite * (u64)nE * ((a.ntip - k) - 1);
+            if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
+            u64 pb = make_key(a.ordNeg1, 0u);
+            for (u32 i = threadIdx.x; i < nCTA; i += kThreads) {
+                const u64 v = ld_cg_u64(a.partial + ((p - 1) & 1) * nCTA + i);
+                pb = v > pb ? v : pb;
+            }
+            pb = block_max_u64(pb, red);
+            const u32 vOrd = key_ord(pb), vIdx = key_node(pb);
+            const u32 ob = c1 / rg.R;
+            if (ob == b && threadIdx.x == 0) {
+                lmOrd_of(a, buf)[c1] = vOrd;
+                lmIdx_of(a, buf)[c1] = vIdx;
+            }
+            if (threadIdx.x == 0) {
+                BlockRec nr;
+                nr.key = make_key(vOrd, j1);
+                nr.slot = c1;
+                nr.partner = vIdx;
+                BlockRec* L = T.tab + 2 * ob;
+                unsigned char n = T.cnt[ob];
+                if (n == 2) L[0] = L[1];
+                n = n > 0 ? n - 1 : 0;
+                const bool real = vOrd != a.ordNeg1;
+                if (T.exact[ob]) {
+                    if (real) {
+                        if (n == 0) L[0] = nr;
+                        else if (nr.key > L[0].key) { L[1] = L[0]; L[0] = nr; }
+                        else L[1] = nr;
+                        n++;
+                    }
+                } else if (n >= 1 && real && nr.key > L[n - 1].key) {
+                    if (nr.key > L[0].key) { L[1] = L[0]; L[0] = nr; }
+                    else L[1] = nr;
+                    n = 2;
+                }
+                T.cnt[ob] = n;
+            }
+            __syncthreads();
+            continue;
+        }
+        // join j1 and j2 into node ntip+k
+        const u32 newNode = a.ntip + k;
+        const int nE = M::build_join(m, ms, j1, j2, s1, s2, wcount);
+        if (b == 0) {
+            M::store_node(m, ms, newNode);
+            if (threadIdx.x == 0) {
+                a.nodeSize[newNode] = s1 + s2;
+                a.rawEdge[4 * k + 0] = newNode;
+                a.rawEdge[4 * k + 1] = j1;
+                a.rawEdge[4 * k + 2] = newNode;
+                a.rawEdge[4 * k + 3] = j2;
+                a.node2slot[newNode] = c1;
+                a.nodeDeath[j1] = k;
+                a.nodeDeath[j2] = k;
+            }
+        }
+        if (c1 >= rg.lo && c1 < rg.hi) {
+            M::store_slot(m, ms, buf, rg, c1, j1);
+            if (threadIdx.x == 0) {
+                slotNode_of(a, buf)[c1] = newNode;
+                lmOrd_of(a, buf)[c1] = a.ordNeg1;
+            }
+        }
+        if (c2 >= rg.lo && c2 < rg.hi && threadIdx.x == 0) {
+            slotNode_of(a, buf)[c2] = kDead;
+            lmOrd_of(a, buf)[c2] = a.ordNeg1;
+        }
+        __syncthreads();
+        {
+            Top2 tt;
+            tt.init();
+            u32 n = 0;
+            const u32* sn = slotNode_of(a, buf);
+            u32* lop = lmOrd_of(a, buf);
+            u32* lip = lmIdx_of(a, buf);
+            const u32 cap = M::pass_cap(m, rg.hi - rg.lo);
+            for (u32 base = rg.lo; base < rg.hi; base += cap) {
+                M::score_pass(m, ms, buf, rg, base, cap, nE, ordOut);
+                for (u32 x = threadIdx.x; x < cap && base + x < rg.hi; x += kThreads) {
+                    const u32 c = base + x;
+                    const u32 node = ld_cg_u32(sn + c);
+                    if (node == kDead || c == c1) continue;
+                    const u32 o = ordOut[x];
+                    u32 lo = ld_cg_u32(lop + c);
+                    u32 li;
+                    if (o > lo) {  // strict improvement
+                        lo = o;
+                        li = newNode;
+                        lop[c] = o;
+                        lip[c] = newNode;
+                    } else {
+                        li = ld_cg_u32(lip + c);
+                    }
+                    if (lo != a.ordNeg1) {
+                        n++;
+                        tt.push(make_key(lo, node), c, li);
+                    }
+                }
+                __syncthreads();
+            }
+            cnt = block_sum_u32(n, wsum);
+            block_top2(tt, red, &s_rec, s_top);
+        }
+        publish(a, p, b, s_top, cnt);
+        nPairs += (a.ntip - k - 1) - 1;
+        algMilli += (unsigned long long)a.bytesPerPairSite * (u64)nE * ((a.ntip - k - 1) - 1);
+        k++;
+        if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
+        load_table(a, p - 1, T);
+
+        // renumber slots densely when too few are alive
+        const u32 alive = a.ntip - k;
+        if (k < nJoin && rg.S >= a.compactMin && (u64)alive * 256 < (u64)rg.S * a.compactQ8) {
+            {
+                const u32* sn = slotNode_of(a, buf);
+                u32 v = 0;
+                for (u32 c = rg.lo + threadIdx.x; c < rg.hi; c += kThreads) v += ld_cg_u32(sn + c) != kDead;
+                v = block_sum_u32(v, wsum);
+                if (threadIdx.x == 0) a.counts[b] = v;
+                M::compact_prepare(m, ms, buf ^ 1u, make_range(alive, nCTA, b, a.align));
+            }
+            if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
+            if (threadIdx.x == 0) {
+                u32 off = 0, tot = 0;
+                for (u32 i = 0; i < nCTA; i++) {
+                    const u32 v = ld_cg_u32(a.counts + i);
+                    if (i < b) off += v;
+                    tot += v;
+                }
+                s_val[0] = off;
+                s_val[1] = tot;
+            }
+            __syncthreads();
+            const u32 off = s_val[0], Snew = s_val[1];
+            __syncthreads();
+            if (Snew != alive) { fail = CASPHY_EINTERNAL; break; }
+            const u32 nb = buf ^ 1u;
+            const Range nr = make_range(Snew, nCTA, b, a.align);
+            compact_slots(a, buf, nb, rg, off, ranks, wcount);
+            M::compact_move(m, ms, buf, nb, rg, nr.Sp, ranks);
+            if (b == 0) {
+                for (u32 x = Snew + threadIdx.x; x < nr.Sp; x += kThreads) {
+                    slotNode_of(a, nb)[x] = kDead;
+                    lmOrd_of(a, nb)[x] = a.ordNeg1;
+                }
+            }
+            if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
+            buf = nb;
+            rg = make_range(Snew, nCTA, b, a.align);
+            M::after_compact(m, ms, buf, rg);
+            own_top2(a, buf, rg, red, &s_rec, s_top, &cnt, wsum);
+            publish(a, p, b, s_top, cnt);
+            nComp++;
+            if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
+            load_table(a, p - 1, T);
+        }
+    }
+out:
+    if (fail && threadIdx.x == 0) atomicCAS(a.err, 0, fail);
+    if (b == 0 && threadIdx.x == 0) {
+        a.statsOut[0] = nStale;
+        a.statsOut[1] = nPairs;
+        a.statsOut[2] = nComp;
+        a.statsOut[3] = p;
+        a.statsOut[4] = nRefresh;
+        a.statsOut[5] = algMilli / 1000ull;
+    }
+}
+
+// Host: bytes of engine shared memory before the model's part.
+__host__ __device__ inline size_t engine_smem(u32 nCTA, u32 Rmax) {
+    size_t s = sizeof(u32) * kMaxCap + sizeof(BlockRec) * 2 * nCTA + sizeof(u32) * Rmax + 2 * nCTA;
+    return (s + 15) & ~size_t(15);
+}
+
+__global__ void k_slot_init(u32 ntip, u32 Sp, u32 nnode, const unsigned long long* initKey, u32 ordNeg1, u32* lmOrd,
+                            u32* lmIdx, u32* slotNode, u32* node2slot, u32* nodeDeath, u32* nodeSize,
+                            const u32* tipSize);
+__global__ void k_fill_u64(unsigned long long* p, u64 n, u64 v);
+
+// Pre-order walk of the raw join edges (cu/joinEdgeIndel.cu:488-558).
+void preorder_relabel(u32 ntip, const u32* rawEdge, u32* edge_out, u32* order);
+
+}  // namespace joinx
+}  // namespace casphy

@@ -83,6 +83,24 @@ int casphy_join_indel_dev(uint32_t ntip, uint32_t ncol, const uint32_t *d_codes,
                           uint32_t *d_state_out, casphy_join_stats *stats, void *stream);
 
 /*
+ * Greedy join of bit-coded cells.  Replaces `joinEdgeBitReverse <prefix>
+ * <wfile> <ancestralType>` (cu/joinEdgeBitReverse.cu:285-615).
+ *   words     ntip x nbin u32 bit rows (bit j of word k = site 32k+j; the
+ *             .tbmat body)
+ *   weight    nbin*32 float64 per-site weights (the .w file); >= 0, not NaN
+ *   ancestralType 0 (updateAncestralKernel) or non-zero (updateAncestralKernel2)
+ *   edge_out  (2*ntip-2) x 2 u32 (.edge2 body); state_out max(ntip-1,1) x nbin
+ *             u32 (.nodeState2 body: seq & ~bistate, root first)
+ */
+int casphy_join_bit(uint32_t ntip, uint32_t nbin, const uint32_t *words,
+                    const double *weight, int ancestralType, uint32_t *edge_out,
+                    uint32_t *state_out, casphy_join_stats *stats);
+/* Same with device-resident words / states. */
+int casphy_join_bit_dev(uint32_t ntip, uint32_t nbin, const uint32_t *d_words,
+                        const double *weight, int ancestralType, uint32_t *edge_out,
+                        uint32_t *d_state_out, casphy_join_stats *stats, void *stream);
+
+/*
  * Zero-allocation variant of casphy_join_indel_dev.  It has no counterpart
  * in the reference; it exists for callers that must not allocate device
  * memory during the call -- e.g. a framework that has already reserved the

@@ -1,0 +1,57 @@
+"""joinEdgeBitReverse on the GPU against the reference bytes and the oracle."""
+import numpy as np
+import pytest
+
+import golden_check
+import oracle as O
+from casphy_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+class _Impl:
+    def __init__(self, L):
+        self.L = L
+
+    def join_bit(self, *a, **k):
+        return self.L.join_bit(*a, **k)
+
+    def __getattr__(self, name):
+        return getattr(O, name)
+
+
+def test_golden_bit_joins(golden, gpu_lib):
+    cases, ref = golden
+    bad = [m for name, ok, m in golden_check.iter_checks(cases, ref, impl=_Impl(gpu_lib), kinds={"jb"})
+           if not ok and ("/t0" in name or "/t1" in name)]
+    assert not bad, "\n".join(bad)
+
+
+@pytest.mark.parametrize("at", [0, 1])
+@pytest.mark.parametrize("seed,ncell,nsite", [(201, 3000, 512), (202, 900, 96), (203, 6000, 64)])
+def test_random_bit_vs_oracle(gpu_lib, seed, ncell, nsite, at):
+    words = synth.binary_workload(ncell, nsite, 14, 0.04, 0.05, seed=seed)
+    e1, s1, st1 = gpu_lib.join_bit(words, None, at)
+    e0, s0, st0 = O.join_bit(words, None, at)
+    assert np.array_equal(e1, e0) and np.array_equal(s1, s0)
+    assert st1["stale_recomputes"] == st0[0]
+
+
+def test_integer_weight_planes(gpu_lib):
+    rng = np.random.default_rng(5)
+    words = synth.binary_workload(1500, 256, 12, 0.05, 0.05, seed=204)
+    w = rng.integers(0, 9, size=256).astype(float)
+    e1, s1, st = gpu_lib.join_bit(words, w, 1)
+    assert st["int_path"] == 1
+    e0, s0, _ = O.join_bit(words, w, 1)
+    assert np.array_equal(e1, e0) and np.array_equal(s1, s0)
+
+
+def test_float_weights(gpu_lib):
+    rng = np.random.default_rng(6)
+    words = synth.binary_workload(800, 128, 12, 0.05, 0.05, seed=205)
+    w = rng.uniform(0.01, 3.0, size=128)
+    e1, s1, st = gpu_lib.join_bit(words, w, 0)
+    assert st["int_path"] == 0
+    e0, s0, _ = O.join_bit(words, w, 0)
+    assert np.array_equal(e1, e0) and np.array_equal(s1, s0)
