@@ -263,7 +263,7 @@ struct BitModel {
     }
     __device__ static void compact_prepare(const Args&, Smem&, u32, const joinx::Range&) {}
     __device__ static void compact_move(const Args& m, Smem&, u32 buf, u32 nb, const joinx::Range& rg, u32 Spn,
-                                        const u32* ranks) {
+                                        const u32* ranks, const u32*) {
         const u32* src = col(m, buf);
         u32* dst = col(m, nb);
         const u32 R = rg.hi - rg.lo;

@@ -63,6 +63,28 @@ struct Common {
     u32 compactMin;       // do not compact below this many slots
     u32 compactQ8;        // compact when alive*256 < slots*compactQ8
     u32 bytesPerPairSite; // algorithmic bytes per (candidate, query entry), x1000
+    unsigned long long* prof;  // nullable: CTA 0 section times (ns), see PROF_*
+};
+
+// Sections timed by CTA 0 when Common::prof is set.
+enum { PROF_BARRIER = 0, PROF_TABLE, PROF_DECIDE, PROF_BUILD, PROF_SCAN, PROF_POST, PROF_STALE_POST, PROF_COMPACT,
+       PROF_N };
+
+struct Prof {
+    unsigned long long acc[PROF_N];
+    u64 t;
+    bool on;
+    __device__ __forceinline__ void init(bool enable) {
+        on = enable && blockIdx.x == 0 && threadIdx.x == 0;
+        for (int i = 0; i < PROF_N; i++) acc[i] = 0;
+        t = on ? globaltimer_ns() : 0;
+    }
+    __device__ __forceinline__ void mark(int sec) {
+        if (!on) return;
+        const u64 n = globaltimer_ns();
+        acc[sec] += n - t;
+        t = n;
+    }
 };
 
 struct Range {
@@ -89,10 +111,7 @@ __device__ __forceinline__ u32* slotNode_of(const Common& a, u32 buf) { return b
 // wait gives up after limit_ns and records CASPHY_ETIMEOUT.
 __device__ __forceinline__ int flag_barrier(u32* flags, u32 nCTA, u32 epoch, int* err, u64 limit_ns) {
     __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        st_release_u32(flags + blockIdx.x * 16u, epoch);
-    }
+    if (threadIdx.x == 0) st_release_u32(flags + blockIdx.x * 16u, epoch);  // gpu-scope release, cumulative
     int fail = 0;
     if (threadIdx.x < nCTA) {
         const u32* f = flags + threadIdx.x * 16u;
@@ -318,6 +337,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_join(Common a, typename M::Args
 
     const Table T{tabRec, tabCnt, tabExact};
     const u32 b = blockIdx.x, nCTA = a.nCTA;
+    Prof pf;
+    pf.init(a.prof != nullptr);
     u32 buf = 0;
     Range rg = make_range(a.ntip, nCTA, b, a.align);
     u32 k = 0, p = 0;
@@ -331,13 +352,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_join(Common a, typename M::Args
     if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
     load_table(a, p - 1, T);
 
+    pf.mark(PROF_COMPACT);
     while (k < nJoin) {
-        if (!table_best(T, nCTA, &s_best, red, &s_flag)) {
+        const bool known = table_best(T, nCTA, &s_best, red, &s_flag);
+        pf.mark(PROF_DECIDE);
+        if (!known) {
             own_top2(a, buf, rg, red, &s_rec, s_top, &cnt, wsum);
             publish(a, p, b, s_top, cnt);
             nRefresh++;
+            pf.mark(PROF_POST);
             if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
+            pf.mark(PROF_BARRIER);
             load_table(a, p - 1, T);
+            pf.mark(PROF_TABLE);
             continue;
         }
         const BlockRec g = s_best;
@@ -353,9 +380,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_join(Common a, typename M::Args
         const u32 death = s_val[0], c2 = s_val[1], s1 = s_val[2], s2 = s_val[3];
         __syncthreads();
         const bool stale = death < k || c2 >= rg.S;
+        pf.mark(PROF_DECIDE);
         if (stale) {
             // rescore j1 against every live slot
             const int nE = M::build_stale(m, ms, j1, wcount);
+            pf.mark(PROF_BUILD);
             Top2 tt;
             tt.init();
             const u32* sn = slotNode_of(a, buf);
@@ -371,6 +400,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_join(Common a, typename M::Args
                 __syncthreads();
             }
             const BlockRec pr = block_best_rec(tt.k0, tt.s0, 0u, red, &s_rec);
+            pf.mark(PROF_SCAN);
             if (threadIdx.x == 0) {
                 asm volatile("st.global.cg.u64 [%0], %1;" ::"l"(a.partial + (p & 1) * nCTA + b), "l"(pr.key)
                              : "memory");
@@ -379,6 +409,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_join(Common a, typename M::Args
             nPairs += (a.ntip - k) - 1;
             algMilli += (unsigned long long)a.bytesPerPairSite * (u64)nE * ((a.ntip - k) - 1);
             if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
+            pf.mark(PROF_BARRIER);
             u64 pb = make_key(a.ordNeg1, 0u);
             for (u32 i = threadIdx.x; i < nCTA; i += kThreads) {
                 const u64 v = ld_cg_u64(a.partial + ((p - 1) & 1) * nCTA + i);
@@ -416,11 +447,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_join(Common a, typename M::Args
                 T.cnt[ob] = n;
             }
             __syncthreads();
+            pf.mark(PROF_STALE_POST);
             continue;
         }
         // join j1 and j2 into node ntip+k
         const u32 newNode = a.ntip + k;
         const int nE = M::build_join(m, ms, j1, j2, s1, s2, wcount);
+        pf.mark(PROF_BUILD);
         if (b == 0) {
             M::store_node(m, ms, newNode);
             if (threadIdx.x == 0) {
@@ -459,17 +492,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_join(Common a, typename M::Args
                 for (u32 x = threadIdx.x; x < cap && base + x < rg.hi; x += kThreads) {
                     const u32 c = base + x;
                     const u32 node = ld_cg_u32(sn + c);
+                    u32 lo = ld_cg_u32(lop + c);
+                    u32 li = ld_cg_u32(lip + c);
                     if (node == kDead || c == c1) continue;
                     const u32 o = ordOut[x];
-                    u32 lo = ld_cg_u32(lop + c);
-                    u32 li;
                     if (o > lo) {  // strict improvement
                         lo = o;
                         li = newNode;
                         lop[c] = o;
                         lip[c] = newNode;
-                    } else {
-                        li = ld_cg_u32(lip + c);
                     }
                     if (lo != a.ordNeg1) {
                         n++;
@@ -478,15 +509,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_join(Common a, typename M::Args
                 }
                 __syncthreads();
             }
+            pf.mark(PROF_SCAN);
             cnt = block_sum_u32(n, wsum);
             block_top2(tt, red, &s_rec, s_top);
         }
         publish(a, p, b, s_top, cnt);
+        pf.mark(PROF_POST);
         nPairs += (a.ntip - k - 1) - 1;
         algMilli += (unsigned long long)a.bytesPerPairSite * (u64)nE * ((a.ntip - k - 1) - 1);
         k++;
         if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
+        pf.mark(PROF_BARRIER);
         load_table(a, p - 1, T);
+        pf.mark(PROF_TABLE);
 
         // renumber slots densely when too few are alive
         const u32 alive = a.ntip - k;
@@ -517,7 +552,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_join(Common a, typename M::Args
             const u32 nb = buf ^ 1u;
             const Range nr = make_range(Snew, nCTA, b, a.align);
             compact_slots(a, buf, nb, rg, off, ranks, wcount);
-            M::compact_move(m, ms, buf, nb, rg, nr.Sp, ranks);
+            M::compact_move(m, ms, buf, nb, rg, nr.Sp, ranks, slotNode_of(a, buf));
             if (b == 0) {
                 for (u32 x = Snew + threadIdx.x; x < nr.Sp; x += kThreads) {
                     slotNode_of(a, nb)[x] = kDead;
@@ -533,6 +568,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_join(Common a, typename M::Args
             nComp++;
             if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
             load_table(a, p - 1, T);
+            pf.mark(PROF_COMPACT);
         }
     }
 out:
@@ -545,6 +581,8 @@ out:
         a.statsOut[4] = nRefresh;
         a.statsOut[5] = algMilli / 1000ull;
     }
+    if (pf.on)
+        for (int i = 0; i < PROF_N; i++) a.prof[i] = pf.acc[i];
 }
 
 // Host: bytes of engine shared memory before the model's part.

@@ -28,6 +28,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -393,7 +394,7 @@ struct IndelDense {
     }
     __device__ static void compact_prepare(const Args&, Smem&, u32, const joinx::Range&) {}
     __device__ static void compact_move(const Args& m, Smem&, u32 buf, u32 nb, const joinx::Range& rg, u32 Spn,
-                                        const u32* ranks) {
+                                        const u32* ranks, const u32*) {
         const u16* src = col(m, buf);
         u16* dst = col(m, nb);
         const u32 R = rg.hi - rg.lo;
@@ -409,6 +410,318 @@ struct IndelDense {
 
 template struct IndelDense<true>;
 template struct IndelDense<false>;
+
+// ---------------------------------------------------------------------------
+// Allele bitsets (integer path).  Row (s, a) of Bits holds one bit per slot:
+// set when the slot's cell carries allele code a+2 at site s.  A query's
+// score for 32 slots at once is the weighted count, over its edited sites, of
+// set bits in the rows of its own alleles; the counts are kept bit-sliced
+// (plane k = bit k of every slot's count) so adding a 32-slot word costs a
+// few logic operations.  The integer path guarantees every score <= 2048.
+
+constexpr int kPlanes = 12;
+
+// c += x * w in bit-sliced form (w <= 2048)
+__device__ __forceinline__ void vadd(u32 (&c)[kPlanes], u32 x, u32 w) {
+    if (!x) return;
+    if (w == 1u) {
+        u32 carry = x;
+#pragma unroll
+        for (int k = 0; k < kPlanes; k++) {
+            const u32 t = c[k] & carry;
+            c[k] ^= carry;
+            carry = t;
+            if (!carry) break;
+        }
+        return;
+    }
+    while (w) {
+        const int k0 = __ffs(w) - 1;
+        w &= w - 1;
+        u32 carry = x;
+#pragma unroll
+        for (int k = 0; k < kPlanes; k++) {
+            if (k < k0) continue;
+            const u32 t = c[k] & carry;
+            c[k] ^= carry;
+            carry = t;
+            if (!carry) break;
+        }
+    }
+}
+
+__device__ __forceinline__ void vsum(u32 (&a)[kPlanes], const u32* b) {
+    u32 carry = 0;
+#pragma unroll
+    for (int k = 0; k < kPlanes; k++) {
+        const u32 x = a[k], y = b[k];
+        a[k] = x ^ y ^ carry;
+        carry = (x & y) | (carry & (x ^ y));
+    }
+}
+
+__device__ __forceinline__ u32 vget(const u32* p, u32 j) {
+    u32 v = 0;
+#pragma unroll
+    for (int k = 0; k < kPlanes; k++) v |= ((p[k] >> j) & 1u) << k;
+    return v;
+}
+
+// Bits[row][w] for the tips: one warp per (site, word), lanes = the word's 32
+// slots; every distinct allele among them gets one store of its lane mask.
+__global__ void k_build_bits(const u16* __restrict__ nodeRow, u32 ntip, u32 ncol, u32 ncolP, u32 nState, u32 Wd,
+                             u32* __restrict__ bits) {
+    __shared__ u16 tile[32][33];
+    const u32 w = blockIdx.x, s0 = blockIdx.y * 32;
+    for (u32 r = threadIdx.y; r < 32; r += blockDim.y) {
+        const u32 slot = w * 32 + r, s = s0 + threadIdx.x;
+        tile[r][threadIdx.x] = (slot < ntip && s < ncol) ? nodeRow[(size_t)slot * ncolP + s] : (u16)0;
+    }
+    __syncthreads();
+    for (u32 y = threadIdx.y; y < 32; y += blockDim.y) {
+        const u32 s = s0 + y;
+        if (s >= ncol) break;
+        const u32 code = tile[threadIdx.x][y];
+        const u32 mask = __match_any_sync(0xFFFFFFFFu, code);
+        if (code > 1 && (__ffs(mask) - 1) == (int)threadIdx.x)
+            bits[((size_t)s * nState + (code - 2)) * Wd + w] = mask;
+    }
+}
+
+struct InitBitsArgs {
+    u32 ntip, ncol, nState, Wd;
+    const u32* bits;
+    const u32* eSC;
+    const u16* eW;
+    const u32* eLen;
+    const u64* chunkStart;
+    u32 nChunks;
+    u64 nTiles;
+    unsigned long long* tileCounter;
+    unsigned long long* initKey;
+};
+
+// Initial local maxima with the bitsets: each 128-thread group takes its own
+// (4096-candidate chunk, query) tiles, one 32-slot word per thread.
+__global__ void __launch_bounds__(kThreads) k_init_bits(InitBitsArgs a) {
+    __shared__ unsigned long long s_tile[4];
+    __shared__ u64 red[16];
+    const u32 g = threadIdx.x >> 7, t = threadIdx.x & 127, lane = threadIdx.x & 31;
+    for (;;) {
+        if (t == 0) s_tile[g] = atomicAdd(a.tileCounter, 1ull);
+        asm volatile("bar.sync %0, 128;" ::"r"(1 + g));
+        const u64 tile = s_tile[g];
+        asm volatile("bar.sync %0, 128;" ::"r"(1 + g));
+        if (tile >= a.nTiles) break;
+        u32 k = 0;
+        while (k + 1 < a.nChunks && a.chunkStart[k + 1] <= tile) k++;
+        const u32 q = (u32)(tile - a.chunkStart[k]);
+        const u32 w = k * 128 + t;
+        u64 best = make_key(ORD_F16_NEG1, 0u);
+        if (w * 32 < a.ntip && w * 32 + 31 > q) {
+            u32 c[kPlanes];
+#pragma unroll
+            for (int i = 0; i < kPlanes; i++) c[i] = 0u;
+            const u32* es = a.eSC + (size_t)q * a.ncol;
+            const u16* ew = a.eW + (size_t)q * a.ncol;
+            const int nE = (int)a.eLen[q];
+            int e = 0;
+            for (; e + 7 < nE; e += 8) {
+                u32 x[8], wt[8];
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    const u32 sc = es[e + i];
+                    wt[i] = ew[e + i];
+                    x[i] = __ldg(a.bits + ((size_t)(sc & 0xFFFFu) * a.nState + (sc >> 16) - 2) * a.Wd + w);
+                }
+#pragma unroll
+                for (int i = 0; i < 8; i++) vadd(c, x[i], wt[i]);
+            }
+            for (; e < nE; e++) {
+                const u32 sc = es[e];
+                vadd(c, __ldg(a.bits + ((size_t)(sc & 0xFFFFu) * a.nState + (sc >> 16) - 2) * a.Wd + w), ew[e]);
+            }
+            u32 any = 0;
+#pragma unroll
+            for (int i = 0; i < kPlanes; i++) any |= c[i];
+            // zero-score slots still compete (score 0 beats the -1 seed)
+            for (u32 j = 0; j < 32; j++) {
+                const u32 slot = w * 32 + j;
+                if (slot <= q || slot >= a.ntip) continue;
+                const u32 cnt = ((any >> j) & 1u) ? vget(c, j) : 0u;
+                const u64 key = make_key(ord_f16((u16)half_bits_of_int(cnt)), slot);
+                best = key > best ? key : best;
+            }
+        }
+        best = warp_max_u64(best);
+        if (lane == 0) red[threadIdx.x >> 5] = best;
+        asm volatile("bar.sync %0, 128;" ::"r"(1 + g));
+        if (t == 0) {
+            u64 m = red[g * 4];
+            for (int i = 1; i < 4; i++) m = red[g * 4 + i] > m ? red[g * 4 + i] : m;
+            atomicMax(a.initKey + q, (unsigned long long)m);
+        }
+        asm volatile("bar.sync %0, 128;" ::"r"(1 + g));
+    }
+}
+
+struct IndelBits {
+    struct Args {
+        u32 ncol, ncolP, nState, minSize;
+        float minRatio;
+        int unitW;
+        const u16* Wsel;
+        u16* nodeRow;
+        u32* bits[2];
+    };
+    struct Smem {
+        u32* eSC;
+        u16* eW;
+        u16* mrow;
+        u16* orow;    // j1's row (the slot's previous occupant)
+        u32* planes;  // kThreads x kPlanes
+    };
+    __host__ __device__ static size_t engine_smem_bytes(u32 nCTA, u32 Rmax) { return joinx::engine_smem(nCTA, Rmax); }
+    __host__ static size_t model_smem_bytes(const Args& m) {
+        return sizeof(u32) * kThreads * kPlanes + sizeof(u32) * m.ncol +
+               sizeof(u16) * (((m.ncol + 7u) & ~7u) + 2 * m.ncolP) + 16;
+    }
+    __device__ static void carve_smem(const Args& m, unsigned char* p, Smem& s) {
+        s.planes = reinterpret_cast<u32*>(p);
+        s.eSC = s.planes + kThreads * kPlanes;
+        s.eW = reinterpret_cast<u16*>(s.eSC + m.ncol);
+        s.mrow = s.eW + ((m.ncol + 7u) & ~7u);
+        s.orow = s.mrow + m.ncolP;
+    }
+    __device__ static u32* bitsOf(const Args& m, u32 buf) { return buf ? m.bits[1] : m.bits[0]; }
+    __device__ static int build_stale(const Args& m, Smem& s, u32 j1, u32* wc) {
+        return build_indel_query(m.ncol, m.ncolP, m.unitW, m.Wsel, m.nodeRow + (size_t)j1 * m.ncolP, nullptr, 0,
+                                 nullptr, s.eSC, s.eW, wc);
+    }
+    __device__ static int build_join(const Args& m, Smem& s, u32 j1, u32 j2, u32 s1, u32 s2, u32* wc) {
+        int mode;
+        if (s1 < m.minSize && __uint2float_rn(s1) * m.minRatio < __uint2float_rn(s2)) mode = 1;
+        else if (s2 < m.minSize && __uint2float_rn(s2) * m.minRatio < __uint2float_rn(s1)) mode = 2;
+        else mode = 3;
+        const u16* r1 = m.nodeRow + (size_t)j1 * m.ncolP;
+        for (u32 i = threadIdx.x; i < m.ncolP; i += kThreads) s.orow[i] = ld_cg_u16(r1 + i);
+        return build_indel_query(m.ncol, m.ncolP, m.unitW, m.Wsel, r1, m.nodeRow + (size_t)j2 * m.ncolP, mode,
+                                 s.mrow, s.eSC, s.eW, wc);
+    }
+    __device__ static void store_node(const Args& m, Smem& s, u32 newNode) {
+        u16* dst = m.nodeRow + (size_t)newNode * m.ncolP;
+        for (u32 i = threadIdx.x; i < m.ncolP; i += kThreads) dst[i] = s.mrow[i];
+    }
+    // the new node replaces j1 in slot c1: flip c1's bit in the rows of the
+    // sites where the two states differ (fire-and-forget reductions; the word
+    // belongs to this CTA and nobody reads it before the next phase)
+    __device__ static void store_slot(const Args& m, Smem& s, u32 buf, const joinx::Range& rg, u32 c1, u32) {
+        u32* B = bitsOf(m, buf);
+        const u32 Wd = rg.Sp / 32, word = c1 >> 5, bit = 1u << (c1 & 31);
+        for (u32 i = threadIdx.x; i < m.ncol; i += kThreads) {
+            const u32 o = s.orow[i], n = s.mrow[i];
+            if (o == n) continue;
+            if (o > 1) atomicAnd(B + ((size_t)i * m.nState + o - 2) * Wd + word, ~bit);
+            if (n > 1) atomicOr(B + ((size_t)i * m.nState + n - 2) * Wd + word, bit);
+        }
+    }
+    __device__ static u32 pass_cap(const Args&, u32 R) { return min(4096u, (R + 31u) & ~31u); }
+    __device__ static void score_pass(const Args& m, Smem& s, u32 buf, const joinx::Range& rg, u32 base, u32 cap,
+                                      int nE, u32* ordOut) {
+        const u32 T = cap / 32;
+        const u32 TG = T <= 32 ? 32 : (T <= 64 ? 64 : 128);
+        const u32 F = kThreads / TG;
+        const u32 g = threadIdx.x / TG, t = threadIdx.x % TG;
+        const u32 Wd = rg.Sp / 32;
+        const u32 w = base / 32 + t;
+        const u32* B = bitsOf(m, buf);
+        u32 c[kPlanes];
+#pragma unroll
+        for (int i = 0; i < kPlanes; i++) c[i] = 0u;
+        if (t < T && w * 32 < rg.hi) {
+            int e = (int)g;
+            for (; e + 15 * (int)F < nE; e += 16 * (int)F) {
+                u32 x[16], wt[16];
+#pragma unroll
+                for (int i = 0; i < 16; i++) {
+                    const u32 sc = s.eSC[e + i * F];
+                    wt[i] = s.eW[e + i * F];
+                    x[i] = ld_cg_u32(B + ((size_t)(sc & 0xFFFFu) * m.nState + (sc >> 16) - 2) * Wd + w);
+                }
+#pragma unroll
+                for (int i = 0; i < 16; i++) vadd(c, x[i], wt[i]);
+            }
+            for (; e + 3 * (int)F < nE; e += 4 * (int)F) {
+                u32 x[4], wt[4];
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    const u32 sc = s.eSC[e + i * F];
+                    wt[i] = s.eW[e + i * F];
+                    x[i] = ld_cg_u32(B + ((size_t)(sc & 0xFFFFu) * m.nState + (sc >> 16) - 2) * Wd + w);
+                }
+#pragma unroll
+                for (int i = 0; i < 4; i++) vadd(c, x[i], wt[i]);
+            }
+            for (; e < nE; e += (int)F) {
+                const u32 sc = s.eSC[e];
+                vadd(c, ld_cg_u32(B + ((size_t)(sc & 0xFFFFu) * m.nState + (sc >> 16) - 2) * Wd + w), s.eW[e]);
+            }
+        }
+        // tree-reduce the F groups' bit-sliced counters
+        for (u32 h = F / 2; h >= 1; h /= 2) {
+            if (g >= h && g < 2 * h) {
+#pragma unroll
+                for (int i = 0; i < kPlanes; i++) s.planes[((g - h) * TG + t) * kPlanes + i] = c[i];
+            }
+            __syncthreads();
+            if (g < h) vsum(c, s.planes + (g * TG + t) * kPlanes);
+            __syncthreads();
+        }
+        if (g == 0) {
+#pragma unroll
+            for (int i = 0; i < kPlanes; i++) s.planes[t * kPlanes + i] = c[i];
+        }
+        __syncthreads();
+        for (u32 x = threadIdx.x; x < cap && base + x < rg.hi; x += kThreads) {
+            const u32 cnt = vget(s.planes + (x >> 5) * kPlanes, x & 31);
+            ordOut[x] = ord_f16((u16)half_bits_of_int(cnt));
+        }
+        __syncthreads();
+    }
+    // C1: clear this CTA's words of the new layout in every row
+    __device__ static void compact_prepare(const Args& m, Smem&, u32 nb, const joinx::Range& nr) {
+        u32* B = bitsOf(m, nb);
+        const u32 Wdn = nr.Sp / 32, w0 = nr.lo / 32, w1 = (nr.hi + 31) / 32;
+        if (w1 <= w0) return;
+        const u32 nw = w1 - w0;
+        const size_t rows = (size_t)m.ncol * m.nState;
+        for (size_t i = threadIdx.x; i < rows * nw; i += kThreads) {
+            const size_t row = i / nw;
+            B[row * Wdn + w0 + (u32)(i % nw)] = 0u;
+        }
+    }
+    // C2: set the bits of every live slot of this CTA at its new position
+    // (words may belong to another CTA in the new layout, hence atomics)
+    __device__ static void compact_move(const Args& m, Smem&, u32, u32 nb, const joinx::Range& rg, u32 Spn,
+                                        const u32* ranks, const u32* slotNodeOld) {
+        u32* B = bitsOf(m, nb);
+        const u32 Wdn = Spn / 32;
+        const u32 R = rg.hi - rg.lo;
+        const u32 lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        for (u32 x = wid; x < R; x += kThreads / 32) {
+            const u32 r = ranks[x];
+            if (r == kNone) continue;
+            const u32 node = ld_cg_u32(slotNodeOld + rg.lo + x);
+            const u16* row = m.nodeRow + (size_t)node * m.ncolP;
+            const u32 word = r >> 5, bit = 1u << (r & 31);
+            for (u32 i = lane; i < m.ncol; i += 32) {
+                const u32 code = ld_cg_u16(row + i);
+                if (code > 1) atomicOr(B + ((size_t)i * m.nState + code - 2) * Wdn + word, bit);
+            }
+        }
+    }
+    __device__ static void after_compact(const Args&, Smem&, u32, const joinx::Range&) {}
+};
 
 // state_out[r] = nodeRow[order[r]] widened to u32
 __global__ void k_gather(const u16* __restrict__ nodeRow, u32 ncol, u32 ncolP, const u32* __restrict__ order,
@@ -464,22 +777,31 @@ static int convert_weights(u32 nState, u32 ncol, const double* w, std::vector<u1
 // Device buffers of one indel join (shared by the allocating and the
 // zero-allocation entry points).
 struct IndelBuffers {
-    u16* Wsel; u16* nodeRow; u16* colT0; u16* colT1; u32* lm[6];
+    u16* Wsel; u16* nodeRow; u16* colT0; u16* colT1; u32* bits0; u32* bits1; size_t bitsWords; u32* lm[6];
     u32* node2slot; u32* nodeDeath; u32* nodeSize; u32* rawEdge;
     u32* eSC; u16* eW; u32* eLen; unsigned long long* initKey;
     joinx::BlockRec* pub; u32* pubCnt; u64* partial; u32* counts; u32* flags; int* jerr; int* prepErr;
     unsigned long long* tileCounter; u64* chunkStart; unsigned long long* stats; u32* tipSize;
 };
 
-static IndelBuffers carve_indel(Carve& c, u32 ntip, u32 ncol, u32 nState, u32 nCTA, u32 nChunks) {
+// Bytes of the two allele-bitset buffers for the bitset scan.
+static size_t bits_bytes(u32 ntip, u32 ncol, u32 nState) {
+    const size_t Wd = ((size_t)ntip + 31) / 32;
+    return 2 * (size_t)ncol * nState * Wd * sizeof(u32);
+}
+
+static IndelBuffers carve_indel(Carve& c, u32 ntip, u32 ncol, u32 nState, u32 nCTA, u32 nChunks, bool useBits) {
     const u32 nnode = 2 * ntip - 1, nedge = 2 * ntip - 2;
-    const u32 ncolP = (ncol + 7u) & ~7u, Sp = (ntip + 7u) & ~7u;
+    const u32 ncolP = (ncol + 7u) & ~7u, Sp = (ntip + 31u) & ~31u;
     const size_t nw = (size_t)nState * ncol;
     IndelBuffers l;
     l.Wsel = c.take<u16>(nw ? nw : 1);
     l.nodeRow = c.take<u16>((size_t)nnode * ncolP);
-    l.colT0 = c.take<u16>((size_t)ncol * Sp);
-    l.colT1 = c.take<u16>((size_t)ncol * Sp);
+    l.colT0 = c.take<u16>(useBits ? 0 : (size_t)ncol * Sp);
+    l.colT1 = c.take<u16>(useBits ? 0 : (size_t)ncol * Sp);
+    l.bitsWords = useBits ? (size_t)ncol * nState * (Sp / 32) : 0;
+    l.bits0 = c.take<u32>(l.bitsWords);
+    l.bits1 = c.take<u32>(l.bitsWords);
     for (int i = 0; i < 6; i++) l.lm[i] = c.take<u32>(Sp);
     l.node2slot = c.take<u32>(nnode);
     l.nodeDeath = c.take<u32>(nnode);
@@ -498,7 +820,7 @@ static IndelBuffers carve_indel(Carve& c, u32 ntip, u32 ncol, u32 nState, u32 nC
     l.prepErr = c.take<int>(1);
     l.tileCounter = c.take<unsigned long long>(1);
     l.chunkStart = c.take<u64>(nChunks + 1);
-    l.stats = c.take<unsigned long long>(8);
+    l.stats = c.take<unsigned long long>(8 + joinx::PROF_N);
     l.tipSize = c.take<u32>(ntip);
     return l;
 }
@@ -515,10 +837,13 @@ static void chunk_table(u32 ntip, u32 nChunks, u64* chunkStart) {
 // tipSize and chunkStart are already on the device; clears everything the
 // kernels expect at zero.  Returns the number of kernels launched.
 static int launch_indel(const IndelBuffers& L, u32 ntip, u32 ncol, u32 nState, const u32* codes, bool intPath,
-                        bool unitW, u32 minSize, float minRatio, u32 nSM, u32 nChunks, u64 nTiles, cudaStream_t st,
-                        cudaEvent_t evInit0, cudaEvent_t evInit1, int* launches) {
+                        bool unitW, bool useBits, u32 minSize, float minRatio, u32 nSM, u32 nChunks, u64 nTiles,
+                        cudaStream_t st, cudaEvent_t evInit0, cudaEvent_t evInit1, int* launches) {
     const u32 nnode = 2 * ntip - 1;
-    const u32 ncolP = (ncol + 7u) & ~7u, Sp = (ntip + 7u) & ~7u;
+    // slot stride: bitset words need multiples of 32 slots, the u16 column
+    // scan multiples of 8 (one 16-byte load); the engine uses the same rule
+    const u32 align = useBits ? 32u : 8u;
+    const u32 ncolP = (ncol + 7u) & ~7u, Sp = (ntip + align - 1) / align * align;
     const u32 nCTA = nSM;
     CASPHY_CUDA_TRY(cudaMemsetAsync(L.prepErr, 0, sizeof(int), st));
     CASPHY_CUDA_TRY(cudaMemsetAsync(L.jerr, 0, sizeof(int), st));
@@ -528,15 +853,26 @@ static int launch_indel(const IndelBuffers& L, u32 ntip, u32 ncol, u32 nState, c
     PrepArgs pa{ntip, ncol, ncolP, nState, Sp, codes, L.Wsel, intPath ? 0x7FFFu : 0xFFFFu,
                 L.nodeRow, L.eSC, L.eW, L.eLen, L.prepErr};
     k_prep_rows<<<(ntip + 7) / 8, 256, 0, st>>>(pa);
-    k_transpose<<<dim3((Sp + 31) / 32, (ncol + 31) / 32), dim3(32, 8), 0, st>>>(L.nodeRow, ntip, ncol, ncolP, Sp,
-                                                                                  L.colT0);
+    if (useBits) {
+        CASPHY_CUDA_TRY(cudaMemsetAsync(L.bits0, 0, sizeof(u32) * L.bitsWords, st));
+        k_build_bits<<<dim3(Sp / 32, (ncol + 31) / 32), dim3(32, 8), 0, st>>>(L.nodeRow, ntip, ncol, ncolP, nState,
+                                                                                Sp / 32, L.bits0);
+    } else {
+        k_transpose<<<dim3((Sp + 31) / 32, (ncol + 31) / 32), dim3(32, 8), 0, st>>>(L.nodeRow, ntip, ncol, ncolP,
+                                                                                      Sp, L.colT0);
+    }
     joinx::k_fill_u64<<<(ntip + 255) / 256, 256, 0, st>>>(L.initKey, ntip,
                                                            ((u64)ORD_F16_NEG1 << 32) | 0xFFFFFFFFull);
     int n = 3;
     if (evInit0) CASPHY_CUDA_TRY(cudaEventRecord(evInit0, st));
     InitArgs ia{ntip, ncol, Sp, L.colT0, L.eSC, L.eW, L.eLen, L.chunkStart, nChunks, nTiles, L.tileCounter, L.initKey};
     int perSM = 0;
-    if (intPath) {
+    if (useBits) {
+        InitBitsArgs ib{ntip, ncol, nState, Sp / 32, L.bits0, L.eSC, L.eW, L.eLen, L.chunkStart, nChunks, nTiles,
+                        L.tileCounter, L.initKey};
+        CASPHY_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_init_bits, kThreads, 0));
+        k_init_bits<<<nSM * std::max(perSM, 1), kThreads, 0, st>>>(ib);
+    } else if (intPath) {
         CASPHY_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_init_scan<true>, kThreads, 0));
         k_init_scan<true><<<nSM * std::max(perSM, 1), kThreads, 0, st>>>(ia);
     } else {
@@ -545,7 +881,7 @@ static int launch_indel(const IndelBuffers& L, u32 ntip, u32 ncol, u32 nState, c
     }
     n++;
     if (evInit1) CASPHY_CUDA_TRY(cudaEventRecord(evInit1, st));
-    const u32 initN = std::max(Sp, nnode);
+    const u32 initN = std::max(Sp, nnode);  // Sp: slots rounded up to 32
     joinx::k_slot_init<<<(initN + 255) / 256, 256, 0, st>>>(ntip, Sp, nnode, L.initKey, ORD_F16_NEG1, L.lm[0],
                                                               L.lm[1], L.lm[2], L.node2slot, L.nodeDeath, L.nodeSize,
                                                               L.tipSize);
@@ -557,9 +893,21 @@ static int launch_indel(const IndelBuffers& L, u32 ntip, u32 ncol, u32 nState, c
     c.node2slot = L.node2slot; c.nodeDeath = L.nodeDeath; c.nodeSize = L.nodeSize; c.rawEdge = L.rawEdge;
     c.pub = L.pub; c.pubCnt = L.pubCnt; c.partial = L.partial; c.counts = L.counts; c.flags = L.flags;
     c.err = L.jerr; c.limitNs = 20ull * 1000 * 1000 * 1000; c.statsOut = L.stats;
-    c.Rmax = (((ntip + nCTA - 1) / nCTA) + 7u) & ~7u;
+    c.prof = getenv("CASPHY_PROFILE") ? L.stats + 8 : nullptr;
+    c.Rmax = (((ntip + nCTA - 1) / nCTA) + 31u) & ~31u;
     c.ordNeg1 = ORD_F16_NEG1; c.compactMin = 4096; c.compactQ8 = 192; c.bytesPerPairSite = 2000;
-    if (intPath) {
+    if (useBits) {
+        using M = IndelBits;
+        c.align = 32;
+        c.compactQ8 = 128;
+        c.bytesPerPairSite = 125;  // one bit per (candidate, query site)
+        M::Args m{ncol, ncolP, nState, minSize, minRatio, unitW ? 1 : 0, L.Wsel, L.nodeRow, {L.bits0, L.bits1}};
+        const size_t smem = M::engine_smem_bytes(nCTA, c.Rmax) + M::model_smem_bytes(m);
+        void* fn = (void*)joinx::k_join<M>;
+        CASPHY_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        void* args[] = {&c, &m};
+        CASPHY_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(nCTA), dim3(kThreads), args, smem, st));
+    } else if (intPath) {
         using M = IndelDense<true>;
         M::Args m{ncol, ncolP, nState, minSize, minRatio, unitW ? 1 : 0, L.Wsel, L.nodeRow, {L.colT0, L.colT1}};
         const size_t smem = M::engine_smem_bytes(nCTA, c.Rmax) + M::model_smem_bytes(m);
@@ -600,8 +948,14 @@ static int join_indel_impl(u32 ntip, u32 ncol, const u32* d_codes, u32 nState, c
     int nSM = 0;
     CASPHY_CUDA_TRY(cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, ds.dev));
     const u32 nChunks = (ntip + kCap - 1) / kCap;
+    // allele-bitset scan on the integer path when the two bitset buffers fit
+    // a 48 GiB budget (CASPHY_INDEL_SCAN=dense forces the column scan)
+    const char* scanEnv = getenv("CASPHY_INDEL_SCAN");
+    bool useBits = intPath && ntip >= 2 && bits_bytes(ntip, ncol, nState) <= (size_t(48) << 30);
+    if (scanEnv && !strcmp(scanEnv, "dense")) useBits = false;
+    lst.scan_path = useBits ? 1u : 0u;
     Carve cv;
-    carve_indel(cv, ntip, ncol, nState, (u32)nSM, nChunks);
+    carve_indel(cv, ntip, ncol, nState, (u32)nSM, nChunks, useBits);
     u32* dCodesCopy = cv.take<u32>(h_codes ? (size_t)ntip * ncol : 0);
     u32* dOrder = cv.take<u32>(nrows);
     u32* dState = cv.take<u32>(h_state_out ? (size_t)nrows * ncol : 0);
@@ -610,7 +964,7 @@ static int join_indel_impl(u32 ntip, u32 ncol, const u32* d_codes, u32 nState, c
     if (rc) return rc;
     Carve c2;
     c2.base = static_cast<char*>(base);
-    const IndelBuffers L = carve_indel(c2, ntip, ncol, nState, (u32)nSM, nChunks);
+    const IndelBuffers L = carve_indel(c2, ntip, ncol, nState, (u32)nSM, nChunks, useBits);
     dCodesCopy = c2.take<u32>(h_codes ? (size_t)ntip * ncol : 0);
     dOrder = c2.take<u32>(nrows);
     dState = c2.take<u32>(h_state_out ? (size_t)nrows * ncol : 0);
@@ -635,8 +989,8 @@ static int join_indel_impl(u32 ntip, u32 ncol, const u32* d_codes, u32 nState, c
     std::vector<u32> order(nrows, 0u);
     unsigned long long hst[8] = {0};
     if (ntip >= 2) {
-        rc = launch_indel(L, ntip, ncol, nState, codes, intPath, unitW, minSize, minRatio, (u32)nSM, nChunks,
-                          chunkStart[nChunks], st, ev[1], ev[2], &launches);
+        rc = launch_indel(L, ntip, ncol, nState, codes, intPath, unitW, useBits, minSize, minRatio, (u32)nSM,
+                          nChunks, chunkStart[nChunks], st, ev[1], ev[2], &launches);
         if (rc) return rc;
         CASPHY_CUDA_TRY(cudaEventRecord(ev[3], st));
         std::vector<u32> eLenH(ntip), raw((size_t)2 * nedge);
@@ -644,6 +998,9 @@ static int join_indel_impl(u32 ntip, u32 ncol, const u32* d_codes, u32 nState, c
         CASPHY_CUDA_TRY(cudaMemcpyAsync(eLenH.data(), L.eLen, sizeof(u32) * ntip, cudaMemcpyDeviceToHost, st));
         CASPHY_CUDA_TRY(cudaMemcpyAsync(raw.data(), L.rawEdge, sizeof(u32) * 2 * nedge, cudaMemcpyDeviceToHost, st));
         CASPHY_CUDA_TRY(cudaMemcpyAsync(hst, L.stats, sizeof(hst), cudaMemcpyDeviceToHost, st));
+        unsigned long long prof[joinx::PROF_N] = {0};
+        if (getenv("CASPHY_PROFILE"))
+            CASPHY_CUDA_TRY(cudaMemcpyAsync(prof, L.stats + 8, sizeof(prof), cudaMemcpyDeviceToHost, st));
         CASPHY_CUDA_TRY(cudaMemcpyAsync(&errs[0], L.prepErr, sizeof(int), cudaMemcpyDeviceToHost, st));
         CASPHY_CUDA_TRY(cudaMemcpyAsync(&errs[1], L.jerr, sizeof(int), cudaMemcpyDeviceToHost, st));
         CASPHY_CUDA_TRY(cudaStreamSynchronize(st));
@@ -657,6 +1014,13 @@ static int join_indel_impl(u32 ntip, u32 ncol, const u32* d_codes, u32 nState, c
             return errs[1];
         }
         joinx::preorder_relabel(ntip, raw.data(), edge_out, order.data());
+        if (getenv("CASPHY_PROFILE")) {
+            static const char* names[joinx::PROF_N] = {"barrier", "table", "decide", "build",
+                                                       "scan", "post", "stale_post", "compact"};
+            fprintf(stderr, "join-loop sections (CTA 0, ms):");
+            for (int i = 0; i < joinx::PROF_N; i++) fprintf(stderr, " %s=%.1f", names[i], prof[i] / 1e6);
+            fprintf(stderr, "\n");
+        }
         for (u32 i = 0; i + 1 < ntip; i++) lst.alg_bytes_init += 2ull * eLenH[i] * (u64)(ntip - 1 - i);
     } else {
         // one cell: no joins; the root row is the cell itself
@@ -868,7 +1232,7 @@ extern "C" int casphy_join_indel_noalloc(uint32_t ntip, uint32_t ncol, const uin
     CASPHY_CUDA_TRY(cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, dev));
     const u32 nChunks = (ntip + kCap - 1) / kCap;
     Carve need;
-    carve_indel(need, ntip, ncol, nState, (u32)nSM, nChunks);
+    carve_indel(need, ntip, ncol, nState, (u32)nSM, nChunks, false);
     carve_extra(need, ntip, ncol, nState);
     const size_t bytes = need.off + 256;
     if (bytes > kScratchBytes || nChunks > 64) {
@@ -886,7 +1250,7 @@ extern "C" int casphy_join_indel_noalloc(uint32_t ntip, uint32_t ncol, const uin
     cudaStream_t st = (cudaStream_t)stream;
     Carve c;
     c.base = static_cast<char*>(base);
-    const IndelBuffers L = carve_indel(c, ntip, ncol, nState, (u32)nSM, nChunks);
+    const IndelBuffers L = carve_indel(c, ntip, ncol, nState, (u32)nSM, nChunks, false);
     const Extra X = carve_extra(c, ntip, ncol, nState);
     const size_t nw = (size_t)nState * ncol;
 
@@ -911,7 +1275,7 @@ extern "C" int casphy_join_indel_noalloc(uint32_t ntip, uint32_t ncol, const uin
                                     st));
     CASPHY_CUDA_TRY(cudaMemsetAsync(X.dfsErr, 0, sizeof(u32), st));
     int launches = 0;
-    rc = launch_indel(L, ntip, ncol, nState, d_codes, intPath, unitW, minSize, minRatio, (u32)nSM, nChunks,
+    rc = launch_indel(L, ntip, ncol, nState, d_codes, intPath, unitW, false, minSize, minRatio, (u32)nSM, nChunks,
                       chunkStart[nChunks], st, nullptr, nullptr, &launches);
     if (rc) return rc;
     k_preorder<<<1, 32, 0, st>>>(L.rawEdge, ntip, X.relabel, X.stack, X.cursor, d_edge_out, X.order, X.dfsErr);

@@ -23,12 +23,12 @@ _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 class JoinStats(C.Structure):
     _fields_ = [("joins", C.c_uint64), ("stale_recomputes", C.c_uint64), ("pair_scores", C.c_uint64),
                 ("compactions", C.c_uint64), ("kernel_launches", C.c_uint64), ("int_path", C.c_uint32),
-                ("reserved", C.c_uint32), ("init_scan_ms", C.c_double), ("join_loop_ms", C.c_double),
+                ("scan_path", C.c_uint32), ("init_scan_ms", C.c_double), ("join_loop_ms", C.c_double),
                 ("total_ms", C.c_double), ("alg_bytes_init", C.c_uint64), ("alg_bytes_join", C.c_uint64),
                 ("phases", C.c_uint64), ("refreshes", C.c_uint64)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        return {k: getattr(self, k) for k, _ in self._fields_ }
 
 
 class CasphyError(RuntimeError):

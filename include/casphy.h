@@ -47,7 +47,7 @@ typedef struct {
     uint64_t compactions;        /* slot-matrix compactions */
     uint64_t kernel_launches;    /* kernels launched by this call */
     uint32_t int_path;           /* 1: exact integer accumulation was used */
-    uint32_t reserved;
+    uint32_t scan_path;          /* indel: 0 column-major codes, 1 allele bitsets */
     double init_scan_ms;         /* device time, initial all-pairs scan */
     double join_loop_ms;         /* device time, persistent join loop */
     double total_ms;             /* device time of the whole call */

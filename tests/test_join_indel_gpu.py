@@ -10,7 +10,7 @@ from casphy_b200 import synth
 pytestmark = pytest.mark.gpu
 
 
-def test_golden_indel_joins(golden, gpu_lib):
+def test_golden_indel_joins(golden, gpu_lib, scan_path):
     cases, ref = golden
     bad = [m for name, ok, m in golden_check.iter_checks(cases, ref, impl=_Impl(gpu_lib), kinds={"ji"})
            if not ok]
@@ -29,13 +29,22 @@ class _Impl:
         return getattr(O, name)
 
 
+@pytest.fixture(params=["bits", "dense"])
+def scan_path(request, monkeypatch):
+    """Run a test once per indel scan: allele bitsets (default) and the
+    column-major code scan."""
+    monkeypatch.setenv("CASPHY_INDEL_SCAN", request.param)
+    return request.param
+
+
 @pytest.mark.parametrize("seed,ncell,nsite,nallele,pm", [
     (101, 700, 96, 24, 0.1), (102, 1500, 40, 8, 0.3), (103, 64, 500, 200, 0.0), (104, 5000, 64, 16, 0.15)])
-def test_random_indel_vs_oracle(gpu_lib, seed, ncell, nsite, nallele, pm):
+def test_random_indel_vs_oracle(gpu_lib, scan_path, seed, ncell, nsite, nallele, pm):
     raw = synth.lineage_states(ncell, nsite, 13, 0.05, nallele, 1.4, pm, seed=seed)
     codes, ns = synth.regularize(raw)
     w = np.ones((ns, nsite))
     e1, s1, st1 = gpu_lib.join_indel(codes, ns, w)
+    assert st1["scan_path"] == (1 if scan_path == "bits" else 0)
     e0, s0, st0 = O.join_indel(codes, ns, w)
     assert np.array_equal(e1, e0)
     assert np.array_equal(s1, s0)
@@ -54,7 +63,7 @@ def test_half_path_random_weights(gpu_lib):
     assert np.array_equal(e1, e0) and np.array_equal(s1, s0)
 
 
-def test_integer_weights_and_min_size(gpu_lib):
+def test_integer_weights_and_min_size(gpu_lib, scan_path):
     rng = np.random.default_rng(8)
     raw = synth.lineage_states(800, 64, 11, 0.05, 12, 1.3, 0.1, seed=78)
     codes, ns = synth.regularize(raw)
@@ -80,7 +89,7 @@ def test_rejects_codes_beyond_nstate(gpu_lib):
     assert ei.value.status == 2
 
 
-def test_large_compaction_properties(gpu_lib):
+def test_large_compaction_properties(gpu_lib, scan_path):
     """6,000 cells: exercises slot compaction; checked against the oracle."""
     raw = synth.lineage_states(6000, 96, 16, 0.03, 64, 1.3, 0.15, seed=55)
     codes, ns = synth.regularize(raw)
