@@ -1,0 +1,410 @@
+// Radius neighbour search on B200: radiusNeighbor, radiusNeighborDNA,
+// tryRadius and tryRadiusDNA (replaces the cu/ files of those names).
+//
+// The reference tests one query row at a time against the rows after its
+// 32-row block and mirrors the hits on the host (cu/radiusNeighbor.cu:
+// 331-425); its output is, for every row i, the ascending list of rows j with
+// score(i, j) >= radius (the score is symmetric), and the list sizes.
+//   bit rows:  score = sum of w[b] over the bits set in both rows, binary32,
+//              ascending bit order (:33-41); unit weights -> popcount.
+//   DNA rows:  score = number of positions whose 4-bit IUPAC codes intersect
+//              (cu/radiusNeighborDNA.cu:55-87).
+// Here the whole neighbour relation is produced as a bit matrix in one
+// tiled all-pairs launch (32 query rows per CTA in shared memory x 256
+// candidate rows, one warp ballot per 32 candidates), rows are counted, and
+// a second launch expands the bits into the ascending index lists.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "runtime.h"
+
+namespace casphy {
+namespace radius {
+
+constexpr int kThreads = 256;  // candidates per CTA
+constexpr int kQ = 32;         // query rows per CTA
+enum { SC_UNIT = 0, SC_FLOAT = 1, SC_DNA = 2 };
+
+// rows are column-major: word k of row t at col[k * ld + t]
+template <int MODE>
+__global__ void __launch_bounds__(kThreads) k_mask(const u32* __restrict__ col, u32 nwords, u32 ld, u32 ntip,
+                                                   const float* __restrict__ wf, float radius, u32 uradius,
+                                                   u32 maskWords, u32* __restrict__ mask) {
+    extern __shared__ u32 qs[];  // kQ x nwords query words
+    const u32 q0 = blockIdx.y * kQ;
+    const u32 t = blockIdx.x * kThreads + threadIdx.x;
+    for (u32 i = threadIdx.x; i < kQ * nwords; i += kThreads) {
+        const u32 q = i / nwords, k = i % nwords;
+        qs[q * nwords + k] = q0 + q < ntip ? col[(size_t)k * ld + q0 + q] : 0u;
+    }
+    __syncthreads();
+    u32 acc[kQ];
+    float facc[kQ];
+#pragma unroll
+    for (int q = 0; q < kQ; q++) {
+        acc[q] = 0u;
+        facc[q] = 0.0f;
+    }
+    if (t < ntip) {
+        for (u32 k = 0; k < nwords; k++) {
+            const u32 c = col[(size_t)k * ld + t];
+            if (MODE == SC_UNIT) {
+#pragma unroll
+                for (int q = 0; q < kQ; q++) acc[q] += (u32)__popc(qs[q * nwords + k] & c);
+            } else if (MODE == SC_DNA) {
+#pragma unroll
+                for (int q = 0; q < kQ; q++) {
+                    u32 x = qs[q * nwords + k] & c;
+                    x |= x >> 1;
+                    x |= x >> 2;
+                    acc[q] += (u32)__popc(x & 0x11111111u);
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < kQ; q++) {
+                    u32 m = qs[q * nwords + k] & c;
+                    while (m) {
+                        const int b = __ffs(m) - 1;
+                        facc[q] += __ldg(wf + k * 32 + b);
+                        m &= m - 1;
+                    }
+                }
+            }
+        }
+    }
+    const u32 lane = threadIdx.x & 31;
+#pragma unroll
+    for (int q = 0; q < kQ; q++) {
+        bool hit;
+        if (MODE == SC_UNIT) hit = (float)acc[q] >= radius;
+        else if (MODE == SC_DNA) hit = acc[q] >= uradius;
+        else hit = facc[q] >= radius;
+        hit = hit && t < ntip;
+        const u32 bal = __ballot_sync(0xFFFFFFFFu, hit);
+        if (lane == 0 && q0 + q < ntip && (t >> 5) < maskWords) mask[(size_t)(q0 + q) * maskWords + (t >> 5)] = bal;
+    }
+}
+
+// counts[i] = popcount of row i of the mask
+__global__ void k_count(const u32* __restrict__ mask, u32 ntip, u32 maskWords, u32* __restrict__ counts) {
+    const u32 row = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const u32 lane = threadIdx.x & 31;
+    if (row >= ntip) return;
+    u32 n = 0;
+    for (u32 w = lane; w < maskWords; w += 32) n += (u32)__popc(mask[(size_t)row * maskWords + w]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xFFFFFFFFu, n, o);
+    if (lane == 0) counts[row] = n;
+}
+
+// idx[off[i] ...] = ascending set bits of row i (one warp per row)
+__global__ void k_expand(const u32* __restrict__ mask, u32 ntip, u32 maskWords, const u64* __restrict__ off,
+                         u32* __restrict__ idx) {
+    const u32 row = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const u32 lane = threadIdx.x & 31;
+    if (row >= ntip) return;
+    u64 o = off[row];
+    for (u32 w0 = 0; w0 < maskWords; w0 += 32) {
+        const u32 w = w0 + lane;
+        u32 m = w < maskWords ? mask[(size_t)row * maskWords + w] : 0u;
+        const u32 c = __popc(m);
+        u32 incl = c;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const u32 v = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+            if (lane >= (u32)d) incl += v;
+        }
+        u64 p = o + incl - c;
+        while (m) {
+            const int b = __ffs(m) - 1;
+            idx[p++] = w * 32 + b;
+            m &= m - 1;
+        }
+        o += __shfl_sync(0xFFFFFFFFu, incl, 31);
+    }
+}
+
+// fasta2bin bytes -> column-major 4-bit nibbles, 8 positions per word
+// (packMatKernel, cu/radiusNeighborDNA.cu:27-53): nibble j of packed word k
+// is the low nibble of the code of position 8k+j.
+__global__ void k_pack_dna(const u32* __restrict__ raw, u32 ntip, u32 nbinRaw, u32 npk, u32 ld,
+                           u32* __restrict__ col) {
+    const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
+    const u32 k = blockIdx.y;
+    if (t >= ntip || k >= npk) return;
+    u32 v = 0;
+    for (u32 h = 0; h < 2; h++) {
+        const u32 wi = 2 * k + h;
+        if (wi < nbinRaw) {
+            const u32 r = raw[(size_t)t * nbinRaw + wi];
+#pragma unroll
+            for (int j = 0; j < 4; j++) v |= ((r >> (8 * j)) & 0xFu) << (4 * (4 * h + j));
+        }
+    }
+    col[(size_t)k * ld + t] = v;
+}
+
+// tryRadius: counts[r] = #{t < ntip : score(q_r, t) >= radius}; bit rows
+// with radius <= 0 also count the idle threads of the last 128-thread block
+// (cu/tryRadius.cu:44-49).
+template <int MODE>
+__global__ void k_try(const u32* __restrict__ col, u32 nwords, u32 ld, u32 ntip, const float* __restrict__ wf,
+                      float radius, u32 uradius, const u32* __restrict__ qidx, u32* __restrict__ counts) {
+    const u32 r = blockIdx.y;
+    const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
+    const u32 q = qidx[r];
+    bool hit = false;
+    if (t < ntip) {
+        u32 acc = 0;
+        float facc = 0.f;
+        for (u32 k = 0; k < nwords; k++) {
+            const u32 x = col[(size_t)k * ld + q] & col[(size_t)k * ld + t];
+            if (MODE == SC_UNIT) acc += (u32)__popc(x);
+            else if (MODE == SC_DNA) {
+                u32 y = x | (x >> 1);
+                y |= y >> 2;
+                acc += (u32)__popc(y & 0x11111111u);
+            } else {
+                u32 m = x;
+                while (m) {
+                    const int b = __ffs(m) - 1;
+                    facc += __ldg(wf + k * 32 + b);
+                    m &= m - 1;
+                }
+            }
+        }
+        if (MODE == SC_UNIT) hit = (float)acc >= radius;
+        else if (MODE == SC_DNA) hit = acc >= uradius;
+        else hit = facc >= radius;
+    }
+    const u32 bal = __ballot_sync(0xFFFFFFFFu, hit);
+    if ((threadIdx.x & 31) == 0 && bal) atomicAdd(counts + r, (u32)__popc(bal));
+}
+
+}  // namespace radius
+
+using namespace radius;
+
+struct RadiusInput {
+    bool dna;
+    u32 ntip, nwords;  // words per row (bit rows: nrow; DNA: packed nibble words)
+    const u32* hostWordPlane;  // bit rows, word-plane-major (the .bmat body)
+    const u32* hostRaw;        // DNA rows, fasta2bin layout
+    u32 nbinRaw;
+    std::vector<float> wf;
+    int mode;
+    float radius;
+    u32 uradius;
+};
+
+// Uploads rows column-major (ld = ntip); returns the device pointer.
+static int upload_rows(const RadiusInput& in, Carve& c, u32** col, float** wf, cudaStream_t st) {
+    *col = c.take<u32>((size_t)in.nwords * in.ntip);
+    *wf = c.take<float>(in.wf.size() ? in.wf.size() : 1);
+    if (in.dna) {
+        u32* raw = c.take<u32>((size_t)in.ntip * in.nbinRaw);
+        CASPHY_CUDA_TRY(cudaMemcpyAsync(raw, in.hostRaw, sizeof(u32) * (size_t)in.ntip * in.nbinRaw,
+                                        cudaMemcpyHostToDevice, st));
+        k_pack_dna<<<dim3((in.ntip + 255) / 256, in.nwords), 256, 0, st>>>(raw, in.ntip, in.nbinRaw, in.nwords, in.ntip,
+                                                                           *col);
+    } else {
+        CASPHY_CUDA_TRY(cudaMemcpyAsync(*col, in.hostWordPlane, sizeof(u32) * (size_t)in.nwords * in.ntip,
+                                        cudaMemcpyHostToDevice, st));
+    }
+    if (in.wf.size())
+        CASPHY_CUDA_TRY(cudaMemcpyAsync(*wf, in.wf.data(), sizeof(float) * in.wf.size(), cudaMemcpyHostToDevice, st));
+    return CASPHY_OK;
+}
+
+static int prep_bit(RadiusInput& in, u32 nrow, u32 ntip, const u32* bmat, const double* w, int32_t radius) {
+    if (!bmat || !w || ntip == 0 || nrow == 0) return CASPHY_EINVAL;
+    in.dna = false;
+    in.ntip = ntip;
+    in.nwords = nrow;
+    in.hostWordPlane = bmat;
+    in.wf.resize((size_t)nrow * 32);
+    bool unit = true;
+    for (size_t i = 0; i < in.wf.size(); i++) {
+        in.wf[i] = (float)w[i];
+        if (in.wf[i] != 1.0f) unit = false;
+    }
+    in.mode = unit ? SC_UNIT : SC_FLOAT;
+    if (unit) in.wf.clear();
+    in.radius = (float)radius;
+    in.uradius = 0;
+    return CASPHY_OK;
+}
+
+static int prep_dna(RadiusInput& in, u32 ntip, u32 nbinRaw, const u32* raw, u32 radius) {
+    if (!raw || ntip == 0 || nbinRaw == 0) return CASPHY_EINVAL;
+    in.dna = true;
+    in.ntip = ntip;
+    in.nbinRaw = nbinRaw;
+    in.hostRaw = raw;
+    in.nwords = (nbinRaw - 1) / 2 + 1;
+    in.mode = SC_DNA;
+    in.radius = 0;
+    in.uradius = radius;
+    return CASPHY_OK;
+}
+
+static int radius_impl(RadiusInput& in, u32* counts, u32* idx, u64 cap, u64* total) {
+    if (!counts) return CASPHY_EINVAL;
+    const u32 ntip = in.ntip;
+    const u32 maskWords = (ntip + 31) / 32;
+    const size_t smem = sizeof(u32) * kQ * in.nwords;
+    if (smem > 200 * 1024) {
+        casphy_set_last_error_msg("radius: rows too wide for the shared-memory query tile");
+        return CASPHY_ERANGE;
+    }
+    DeviceScope ds;
+    cudaStream_t st = 0;
+    auto lay = [&](Carve& c) {
+        struct B { u32* mask; u32* counts; u64* off; } b;
+        b.mask = c.take<u32>((size_t)ntip * maskWords);
+        b.counts = c.take<u32>(ntip);
+        b.off = c.take<u64>(ntip);
+        return b;
+    };
+    // sizes: rows + mask first; index space after counting
+    Carve cv;
+    u32* dcol;
+    float* dwf;
+    cv.take<u32>((size_t)in.nwords * ntip);
+    cv.take<float>(in.wf.size() ? in.wf.size() : 1);
+    if (in.dna) cv.take<u32>((size_t)ntip * in.nbinRaw);
+    lay(cv);
+    const size_t base0 = cv.off;
+    void* base = nullptr;
+    int rc = ds.reserve(base0 + 256, &base);
+    if (rc) return rc;
+    Carve c2;
+    c2.base = static_cast<char*>(base);
+    rc = upload_rows(in, c2, &dcol, &dwf, st);
+    if (rc) return rc;
+    auto L = lay(c2);
+    dim3 grid((ntip + kThreads - 1) / kThreads, (ntip + kQ - 1) / kQ);
+    void* fn = in.mode == SC_UNIT ? (void*)k_mask<SC_UNIT> : in.mode == SC_DNA ? (void*)k_mask<SC_DNA>
+                                                                                  : (void*)k_mask<SC_FLOAT>;
+    CASPHY_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (in.mode == SC_UNIT)
+        k_mask<SC_UNIT><<<grid, kThreads, smem, st>>>(dcol, in.nwords, ntip, ntip, dwf, in.radius, in.uradius,
+                                                       maskWords, L.mask);
+    else if (in.mode == SC_DNA)
+        k_mask<SC_DNA><<<grid, kThreads, smem, st>>>(dcol, in.nwords, ntip, ntip, dwf, in.radius, in.uradius,
+                                                      maskWords, L.mask);
+    else
+        k_mask<SC_FLOAT><<<grid, kThreads, smem, st>>>(dcol, in.nwords, ntip, ntip, dwf, in.radius, in.uradius,
+                                                        maskWords, L.mask);
+    k_count<<<(ntip + 7) / 8, 256, 0, st>>>(L.mask, ntip, maskWords, L.counts);
+    CASPHY_CUDA_TRY(cudaGetLastError());
+    CASPHY_CUDA_TRY(cudaMemcpyAsync(counts, L.counts, sizeof(u32) * ntip, cudaMemcpyDeviceToHost, st));
+    CASPHY_CUDA_TRY(cudaStreamSynchronize(st));
+    std::vector<u64> off(ntip);
+    u64 tot = 0;
+    for (u32 i = 0; i < ntip; i++) {
+        off[i] = tot;
+        tot += counts[i];
+    }
+    if (total) *total = tot;
+    if (!idx) return CASPHY_OK;
+    if (tot > cap) return CASPHY_ERANGE;
+    // the index lists get their own buffer: their size is only known now
+    u32* didx = nullptr;
+    CASPHY_CUDA_TRY(cudaMalloc(&didx, sizeof(u32) * (tot ? tot : 1)));
+    CASPHY_CUDA_TRY(cudaMemcpyAsync(L.off, off.data(), sizeof(u64) * ntip, cudaMemcpyHostToDevice, st));
+    k_expand<<<(ntip + 7) / 8, 256, 0, st>>>(L.mask, ntip, maskWords, L.off, didx);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && tot) e = cudaMemcpyAsync(idx, didx, sizeof(u32) * tot, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(didx);
+    CASPHY_CUDA_TRY(e);
+    return CASPHY_OK;
+}
+
+static int try_impl(RadiusInput& in, u32 nrep, const u32* qidx, u32* counts) {
+    if (!counts || (nrep && !qidx)) return CASPHY_EINVAL;
+    for (u32 r = 0; r < nrep; r++)
+        if (qidx[r] >= in.ntip) return CASPHY_ERANGE;
+    if (nrep == 0) return CASPHY_OK;
+    DeviceScope ds;
+    cudaStream_t st = 0;
+    Carve cv;
+    cv.take<u32>((size_t)in.nwords * in.ntip);
+    cv.take<float>(in.wf.size() ? in.wf.size() : 1);
+    if (in.dna) cv.take<u32>((size_t)in.ntip * in.nbinRaw);
+    cv.take<u32>(nrep);
+    cv.take<u32>(nrep);
+    void* base = nullptr;
+    int rc = ds.reserve(cv.off + 256, &base);
+    if (rc) return rc;
+    Carve c2;
+    c2.base = static_cast<char*>(base);
+    u32* dcol;
+    float* dwf;
+    rc = upload_rows(in, c2, &dcol, &dwf, st);
+    if (rc) return rc;
+    u32* dq = c2.take<u32>(nrep);
+    u32* dc = c2.take<u32>(nrep);
+    CASPHY_CUDA_TRY(cudaMemcpyAsync(dq, qidx, sizeof(u32) * nrep, cudaMemcpyHostToDevice, st));
+    CASPHY_CUDA_TRY(cudaMemsetAsync(dc, 0, sizeof(u32) * nrep, st));
+    dim3 grid((in.ntip + 255) / 256, nrep);
+    if (in.mode == SC_UNIT)
+        k_try<SC_UNIT><<<grid, 256, 0, st>>>(dcol, in.nwords, in.ntip, in.ntip, dwf, in.radius, in.uradius, dq, dc);
+    else if (in.mode == SC_DNA)
+        k_try<SC_DNA><<<grid, 256, 0, st>>>(dcol, in.nwords, in.ntip, in.ntip, dwf, in.radius, in.uradius, dq, dc);
+    else
+        k_try<SC_FLOAT><<<grid, 256, 0, st>>>(dcol, in.nwords, in.ntip, in.ntip, dwf, in.radius, in.uradius, dq, dc);
+    CASPHY_CUDA_TRY(cudaGetLastError());
+    CASPHY_CUDA_TRY(cudaMemcpyAsync(counts, dc, sizeof(u32) * nrep, cudaMemcpyDeviceToHost, st));
+    CASPHY_CUDA_TRY(cudaStreamSynchronize(st));
+    if (!in.dna && in.radius <= 0.0f) {
+        const u32 pad = (in.ntip + 127u) / 128u * 128u - in.ntip;
+        for (u32 r = 0; r < nrep; r++) counts[r] += pad;
+    }
+    return CASPHY_OK;
+}
+
+}  // namespace casphy
+
+extern "C" int casphy_radius_bit(uint32_t nrow, uint32_t ntip, const uint32_t* bmat, const double* weight,
+                                 int32_t radius, uint32_t* counts, uint32_t* idx, uint64_t idx_cap, uint64_t* total) {
+    int rc = casphy::require_device();
+    if (rc) return rc;
+    casphy::RadiusInput in;
+    rc = casphy::prep_bit(in, nrow, ntip, bmat, weight, radius);
+    if (rc) return rc;
+    return casphy::radius_impl(in, counts, idx, idx_cap, total);
+}
+
+extern "C" int casphy_radius_dna(uint32_t ntip, uint32_t nbinRaw, const uint32_t* raw, uint32_t radius,
+                                 uint32_t* counts, uint32_t* idx, uint64_t idx_cap, uint64_t* total) {
+    int rc = casphy::require_device();
+    if (rc) return rc;
+    casphy::RadiusInput in;
+    rc = casphy::prep_dna(in, ntip, nbinRaw, raw, radius);
+    if (rc) return rc;
+    return casphy::radius_impl(in, counts, idx, idx_cap, total);
+}
+
+extern "C" int casphy_try_radius_bit(uint32_t nrow, uint32_t ntip, const uint32_t* bmat, const double* weight,
+                                     int32_t radius, uint32_t nrep, const uint32_t* qidx, uint32_t* counts) {
+    int rc = casphy::require_device();
+    if (rc) return rc;
+    casphy::RadiusInput in;
+    rc = casphy::prep_bit(in, nrow, ntip, bmat, weight, radius);
+    if (rc) return rc;
+    return casphy::try_impl(in, nrep, qidx, counts);
+}
+
+extern "C" int casphy_try_radius_dna(uint32_t ntip, uint32_t nbinRaw, const uint32_t* raw, uint32_t radius,
+                                     uint32_t nrep, const uint32_t* qidx, uint32_t* counts) {
+    int rc = casphy::require_device();
+    if (rc) return rc;
+    casphy::RadiusInput in;
+    rc = casphy::prep_dna(in, ntip, nbinRaw, raw, radius);
+    if (rc) return rc;
+    return casphy::try_impl(in, nrep, qidx, counts);
+}

@@ -55,6 +55,14 @@ def lib():
                                         C.POINTER(JoinStats)]
         L.casphy_join_indel_dev.argtypes = [u32, u32, vp, u32, _f64p, _u32p, u32, f32, _u32p, vp,
                                             C.POINTER(JoinStats), vp]
+        for name in ("casphy_node_keep_indel", "casphy_node_keep_bit"):
+            getattr(L, name).argtypes = [u32, u32, _u32p, u32, _u32p, u32, _u32p, u32, _u32p, C.POINTER(u32)]
+        L.casphy_radius_bit.argtypes = [u32, u32, _u32p, _f64p, C.c_int32, _u32p, vp, C.c_uint64,
+                                        C.POINTER(C.c_uint64)]
+        L.casphy_radius_dna.argtypes = [u32, u32, _u32p, u32, _u32p, vp, C.c_uint64, C.POINTER(C.c_uint64)]
+        L.casphy_try_radius_bit.argtypes = [u32, u32, _u32p, _f64p, C.c_int32, u32, _u32p, _u32p]
+        L.casphy_try_radius_dna.argtypes = [u32, u32, _u32p, u32, u32, _u32p, _u32p]
+        L.casphy_transfer_dis.argtypes = [u32, u32, u32, u32, _u32p, _u32p, _u32p, _u32p, _u32p, _u32p]
         if hasattr(L, "casphy_join_bit"):
             L.casphy_join_bit.argtypes = [u32, u32, _u32p, _f64p, C.c_int, _u32p, _u32p, C.POINTER(JoinStats)]
             L.casphy_join_bit_dev.argtypes = [u32, u32, vp, _f64p, C.c_int, _u32p, vp, C.POINTER(JoinStats), vp]
@@ -98,3 +106,68 @@ def join_bit(words, w=None, ancestral_type=1):
     _chk(lib().casphy_join_bit(ntip, nbin, words, w, ancestral_type, edge, state, C.byref(st)),
          "casphy_join_bit")
     return edge[: 2 * nedge].reshape(nedge, 2), state.reshape(-1, nbin), st.as_dict()
+
+
+def node_keep(node_state, edge, outmat, cutoff, bit=False):
+    """nodeKeepIndel / nodeKeepBit: retained node ids in .retainNode order."""
+    node_state, edge, outmat = _u32(node_state), _u32(edge), _u32(outmat)
+    nnode, ncol = node_state.shape
+    out = np.zeros(max(edge.shape[0], 1), dtype=np.uint32)
+    n = C.c_uint32(0)
+    f = lib().casphy_node_keep_bit if bit else lib().casphy_node_keep_indel
+    om = outmat.reshape(-1) if outmat.size else np.zeros(1, np.uint32)
+    _chk(f(nnode, ncol, node_state, edge.shape[0], edge.reshape(-1), outmat.shape[0] if outmat.size else 0, om,
+           cutoff, out, C.byref(n)), "casphy_node_keep")
+    return out[: n.value].copy()
+
+
+def _lists(call, ntip):
+    counts = np.zeros(ntip, dtype=np.uint32)
+    tot = C.c_uint64(0)
+    _chk(call(counts, None, 0, C.byref(tot)), "casphy_radius")
+    idx = np.zeros(max(tot.value, 1), dtype=np.uint32)
+    _chk(call(counts, idx.ctypes.data_as(C.c_void_p), tot.value, C.byref(tot)), "casphy_radius")
+    return counts, idx[: tot.value]
+
+
+def radius_bit(bmat, w, radius):
+    """radiusNeighbor: bmat (nrow words, ntip) word-plane-major -> (counts, idx)."""
+    bmat = _u32(bmat)
+    nrow, ntip = bmat.shape
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    return _lists(lambda c, i, cap, t: lib().casphy_radius_bit(nrow, ntip, bmat, w, int(radius), c, i, cap, t), ntip)
+
+
+def radius_dna(raw, radius):
+    """radiusNeighborDNA on fasta2bin rows -> (counts, idx)."""
+    raw = _u32(raw)
+    ntip, nb = raw.shape
+    return _lists(lambda c, i, cap, t: lib().casphy_radius_dna(ntip, nb, raw, int(radius), c, i, cap, t), ntip)
+
+
+def try_radius_bit(bmat, w, radius, qidx):
+    bmat, qidx = _u32(bmat), _u32(qidx)
+    nrow, ntip = bmat.shape
+    counts = np.zeros(len(qidx), dtype=np.uint32)
+    _chk(lib().casphy_try_radius_bit(nrow, ntip, bmat, np.ascontiguousarray(w, dtype=np.float64), int(radius),
+                                     len(qidx), qidx, counts), "casphy_try_radius_bit")
+    return counts
+
+
+def try_radius_dna(raw, radius, qidx):
+    raw, qidx = _u32(raw), _u32(qidx)
+    counts = np.zeros(len(qidx), dtype=np.uint32)
+    _chk(lib().casphy_try_radius_dna(raw.shape[0], raw.shape[1], raw, int(radius), len(qidx), qidx, counts),
+         "casphy_try_radius_dna")
+    return counts
+
+
+def transfer_dis(y, x, ntip):
+    """TransferDisStream -> (ymin, ysize, xmin, xsize)."""
+    y, x = _u32(y), _u32(x)
+    ny, ncol = y.shape
+    nx = x.shape[0]
+    ymin, ysize = np.zeros(max(ny, 1), np.uint32), np.zeros(max(ny, 1), np.uint32)
+    xmin, xsize = np.zeros(max(nx, 1), np.uint32), np.zeros(max(nx, 1), np.uint32)
+    _chk(lib().casphy_transfer_dis(ny, nx, ncol, ntip, y, x, ymin, ysize, xmin, xsize), "casphy_transfer_dis")
+    return ymin[:ny], ysize[:ny], xmin[:nx], xsize[:nx]

@@ -101,6 +101,55 @@ int casphy_join_bit_dev(uint32_t ntip, uint32_t nbin, const uint32_t *d_words,
                         uint32_t *d_state_out, casphy_join_stats *stats, void *stream);
 
 /*
+ * nodeKeepIndel / nodeKeepBit (cu/nodeKeepIndel.cu:51-169,
+ * cu/nodeKeepBit.cu:77-230).  nodeState: (ntip-1) x ncol u32 (the
+ * .nodeState2 body; ncol = nbin words for the bit version), edge: nedge x 2
+ * u32 (the .edge2 body), outmat: nRetain x ncol u32 (the .tboutmat body).
+ * Writes the retained node ids in the order the reference prints them to
+ * .retainNode (out_nodes must hold nedge entries) and their count.
+ */
+int casphy_node_keep_indel(uint32_t nnodeRows, uint32_t ncol, const uint32_t *nodeState,
+                           uint32_t nedge, const uint32_t *edge, uint32_t nRetain,
+                           const uint32_t *outmat, uint32_t cutoff, uint32_t *out_nodes,
+                           uint32_t *nout);
+int casphy_node_keep_bit(uint32_t nnodeRows, uint32_t nbin, const uint32_t *nodeState,
+                         uint32_t nedge, const uint32_t *edge, uint32_t nRetain,
+                         const uint32_t *outmat, uint32_t cutoff, uint32_t *out_nodes,
+                         uint32_t *nout);
+
+/*
+ * radiusNeighbor (cu/radiusNeighbor.cu:162-470): bmat is the .bmat body,
+ * word-plane-major (nrow words x ntip), weight the .w file (nrow*32 float64),
+ * radius the integer argv value.  counts[ntip] receives the .nNeighbor body;
+ * when idx is non-NULL and idx_cap >= the total, idx receives the .idx body
+ * (for every row the ascending rows j with score >= radius).  *total gets the
+ * list length either way (call once with idx = NULL to size the buffer).
+ */
+int casphy_radius_bit(uint32_t nrow, uint32_t ntip, const uint32_t *bmat, const double *weight,
+                      int32_t radius, uint32_t *counts, uint32_t *idx, uint64_t idx_cap,
+                      uint64_t *total);
+/* radiusNeighborDNA (cu/radiusNeighborDNA.cu:111-380): raw is the fasta2bin
+ * .bin body (ntip x nbinRaw u32, four 8-bit codes per word). */
+int casphy_radius_dna(uint32_t ntip, uint32_t nbinRaw, const uint32_t *raw, uint32_t radius,
+                      uint32_t *counts, uint32_t *idx, uint64_t idx_cap, uint64_t *total);
+/* tryRadius / tryRadiusDNA (cu/tryRadius.cu:52-189, cu/tryRadiusDNA.cu:76-178)
+ * with the query rows given in qidx (the tools draw them with rand()). */
+int casphy_try_radius_bit(uint32_t nrow, uint32_t ntip, const uint32_t *bmat, const double *weight,
+                          int32_t radius, uint32_t nrep, const uint32_t *qidx, uint32_t *counts);
+int casphy_try_radius_dna(uint32_t ntip, uint32_t nbinRaw, const uint32_t *raw, uint32_t radius,
+                          uint32_t nrep, const uint32_t *qidx, uint32_t *counts);
+
+/*
+ * TransferDisStream (cu/TransferDisStream.cu:130-344): y and x are clade
+ * bitset rows (nrow x ncol u32, the bodies of the two input files); outputs
+ * are the value arrays of <out>_ymin.bin / <out>_xmin.bin (min transfer
+ * distance and clade size per row).
+ */
+int casphy_transfer_dis(uint32_t nrow_y, uint32_t nrow_x, uint32_t ncol, uint32_t ntip,
+                        const uint32_t *y, const uint32_t *x, uint32_t *ymin, uint32_t *ysize,
+                        uint32_t *xmin, uint32_t *xsize);
+
+/*
  * Zero-allocation variant of casphy_join_indel_dev.  It has no counterpart
  * in the reference; it exists for callers that must not allocate device
  * memory during the call -- e.g. a framework that has already reserved the

@@ -249,18 +249,19 @@ def _run(args, cwd, timeout=300):
     return r.stdout.decode(errors="replace")
 
 
-def _bin(name):
-    return os.path.join(REF_BIN, name)
-
-
-def run_ref(outdir: str):
+def run_tools(bindir: str) -> dict:
+    """Runs every golden case through the executables in `bindir` (the
+    reference build in oracle/_ref, or the drop-ins in casphy_b200/bin) and
+    returns their output files as arrays.  Tools missing from `bindir` are
+    skipped."""
+    _bin = lambda name: os.path.join(bindir, name)  # noqa: E731
+    have = lambda name: os.path.exists(_bin(name))  # noqa: E731
     cases = _cases()
     res = {}
-    os.makedirs(outdir, exist_ok=True)
     with tempfile.TemporaryDirectory() as d:
         p = lambda n: os.path.join(d, n)  # noqa: E731
         for (kind, name), c in sorted(cases.items()):
-            if kind == "ji":
+            if kind == "ji" and have("joinEdgeIndel"):
                 formats.write_mat(p(name + ".tbmat"), c["codes"])
                 formats.write_mat(p(name + ".tipSize"), c["tip"].reshape(-1, 1))
                 formats.write_f64(p(name + ".w"), c["w"])
@@ -269,12 +270,12 @@ def run_ref(outdir: str):
                 res[f"ji/{name}/edge2"] = formats.read_mat(p(name + ".edge2"))
                 res[f"ji/{name}/nodeState2"] = np.fromfile(p(name + ".nodeState2"), dtype=np.uint32)
                 om = cases.get(("nk", name))
-                if om is not None:
+                if om is not None and have("nodeKeepIndel"):
                     formats.write_mat(p(name + ".tboutmat"), om["outmat"])
                     for cut in (1, 3):
                         _run([_bin("nodeKeepIndel"), name, str(cut)], d)
                         res[f"nk/{name}/retain{cut}"] = formats.read_retain(p(name + ".retainNode"))
-            elif kind == "jb":
+            elif kind == "jb" and have("joinEdgeBitReverse"):
                 formats.write_mat(p(name + ".tbmat"), c["words"])
                 formats.write_f64(p(name + ".w"), c["w"])
                 for at in (0, 1):
@@ -282,7 +283,7 @@ def run_ref(outdir: str):
                     res[f"jb/{name}/edge2_t{at}"] = formats.read_mat(p(name + ".edge2"))
                     res[f"jb/{name}/nodeState2_t{at}"] = np.fromfile(p(name + ".nodeState2"), dtype=np.uint32)
                     om = cases.get(("nkb", name))
-                    if om is not None and at == 1:
+                    if om is not None and at == 1 and have("nodeKeepBit"):
                         formats.write_mat(p(name + ".tboutmat"), om["outmat"])
                         for cut in (1, 2):
                             _run([_bin("nodeKeepBit"), name, str(cut)], d)
@@ -306,9 +307,10 @@ def run_ref(outdir: str):
                 res[f"trd/{name}/nNeighbor{lv - 20}"] = np.fromfile(p(name + ".nNeighbor"), dtype=np.uint32)
                 # bootstrap column resampler on the fasta2bin matrix
                 formats.write_mat(p(name + ".bin"), c["raw"])
-                _run([_bin("Felsenstein"), name, "7"], d)
-                res[f"fs/{name}/B7bin"] = np.fromfile(p(name + "B7.bin"), dtype=np.uint32)
-                res[f"fs/{name}/B7idx"] = np.fromfile(p(name + "B7.idx"), dtype=np.uint32)
+                if have("Felsenstein"):
+                    _run([_bin("Felsenstein"), name, "7"], d)
+                    res[f"fs/{name}/B7bin"] = np.fromfile(p(name + "B7.bin"), dtype=np.uint32)
+                    res[f"fs/{name}/B7idx"] = np.fromfile(p(name + "B7.idx"), dtype=np.uint32)
             elif kind == "td":
                 formats.write_mat(p(name + "_y"), c["y"])
                 formats.write_mat(p(name + "_x"), c["x"])
@@ -316,6 +318,12 @@ def run_ref(outdir: str):
                 res[f"td/{name}/ymin"] = np.fromfile(p(name + "_ymin.bin"), dtype=np.uint32)
                 res[f"td/{name}/xmin"] = np.fromfile(p(name + "_xmin.bin"), dtype=np.uint32)
             print("ran", kind, name, flush=True)
+    return res
+
+
+def run_ref(outdir: str):
+    os.makedirs(outdir, exist_ok=True)
+    res = run_tools(REF_BIN)
     path = os.path.join(outdir, "reference_outputs.npz")
     np.savez_compressed(path, **res)
     print(f"wrote {path} with {len(res)} arrays")
