@@ -67,6 +67,31 @@ __device__ __forceinline__ u64 globaltimer_ns() {
     return t;
 }
 
+// All-to-all flag barrier for a co-resident grid: CTA b publishes `epoch`
+// in its own flag; threads 0..nCTA-1 each wait for one CTA's flag.  Every
+// wait gives up after limit_ns and records CASPHY_ETIMEOUT.
+__device__ __forceinline__ int flag_barrier(u32* flags, u32 nCTA, u32 epoch, int* err, u64 limit_ns) {
+    __syncthreads();
+    if (threadIdx.x == 0) st_release_u32(flags + blockIdx.x * 16u, epoch);  // gpu-scope release, cumulative
+    int fail = 0;
+    if (threadIdx.x < nCTA) {
+        const u32* f = flags + threadIdx.x * 16u;
+        if (ld_acquire_u32(f) < epoch) {
+            const u64 t0 = globaltimer_ns();
+            while (ld_acquire_u32(f) < epoch) {
+                if (*(volatile int*)err) { fail = 1; break; }
+                if (globaltimer_ns() - t0 > limit_ns) {
+                    atomicCAS(err, 0, CASPHY_ETIMEOUT);
+                    fail = 1;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+    }
+    return __syncthreads_or(fail);
+}
+
 // ---------------------------------------------------------------------------
 // Grid barrier for a cooperatively launched grid (all CTAs co-resident).
 // The wait gives up after `limit_ns`, records CASPHY_ETIMEOUT in *err and

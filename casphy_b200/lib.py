@@ -31,6 +31,26 @@ class JoinStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ }
 
 
+class FelModel(C.Structure):
+    _fields_ = [("model", C.c_uint32), ("nallele", C.c_uint32), ("kappa", C.c_double),
+                ("pi", C.c_double * 4), ("rate", C.c_double), ("allele_freq", C.c_void_p),
+                ("mem_budget", C.c_uint64)]
+
+
+class BloptStats(C.Structure):
+    _fields_ = [("iterations", C.c_uint32), ("evaluations", C.c_uint32), ("site_chunks", C.c_uint32),
+                ("levels_inside", C.c_uint32), ("levels_outside", C.c_uint32), ("reserved", C.c_uint32),
+                ("loglik_start", C.c_double), ("loglik_end", C.c_double), ("seconds", C.c_double),
+                ("launches_per_eval", C.c_uint64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+MODEL_HKY85, MODEL_IRREVERSIBLE = 0, 1
+GRAD_ADJOINT, GRAD_CENTRAL_DIFF = 0, 1
+
+
 class CasphyError(RuntimeError):
     def __init__(self, status, what):
         lib = _LIB
@@ -63,6 +83,11 @@ def lib():
         L.casphy_try_radius_bit.argtypes = [u32, u32, _u32p, _f64p, C.c_int32, u32, _u32p, _u32p]
         L.casphy_try_radius_dna.argtypes = [u32, u32, _u32p, u32, u32, _u32p, _u32p]
         L.casphy_transfer_dis.argtypes = [u32, u32, u32, u32, _u32p, _u32p, _u32p, _u32p, _u32p, _u32p]
+        L.casphy_resample_columns.argtypes = [u32, u32, _u32p, u32, _u32p, _u32p]
+        L.casphy_felsenstein_loglik.argtypes = [u32, u32, _u32p, _f64p, u32, _u32p, vp, C.POINTER(FelModel),
+                                                C.POINTER(C.c_double), vp]
+        L.casphy_felsenstein_optimize.argtypes = [u32, u32, _u32p, _f64p, u32, _u32p, vp, C.POINTER(FelModel),
+                                                  C.c_int, u32, C.c_double, C.POINTER(BloptStats)]
         if hasattr(L, "casphy_join_bit"):
             L.casphy_join_bit.argtypes = [u32, u32, _u32p, _f64p, C.c_int, _u32p, _u32p, C.POINTER(JoinStats)]
             L.casphy_join_bit_dev.argtypes = [u32, u32, vp, _f64p, C.c_int, _u32p, vp, C.POINTER(JoinStats), vp]
@@ -171,3 +196,67 @@ def transfer_dis(y, x, ntip):
     xmin, xsize = np.zeros(max(nx, 1), np.uint32), np.zeros(max(nx, 1), np.uint32)
     _chk(lib().casphy_transfer_dis(ny, nx, ncol, ntip, y, x, ymin, ysize, xmin, xsize), "casphy_transfer_dis")
     return ymin[:ny], ysize[:ny], xmin[:nx], xsize[:nx]
+
+
+def resample_columns(raw, idx):
+    """Felsenstein bootstrap gather: byte idx[4i+j] of every row of the
+    fasta2bin body `raw` (ntip x nbin u32) into byte j of word i."""
+    raw, idx = _u32(raw), _u32(idx)
+    ntip, nbin = raw.shape
+    out = np.zeros((ntip, (len(idx) + 3) // 4), np.uint32)
+    _chk(lib().casphy_resample_columns(ntip, nbin, raw, len(idx), idx, out), "casphy_resample_columns")
+    return out
+
+
+def _fel_model(model, kappa, pi, rate, nallele, allele_freq, mem_budget):
+    m = FelModel()
+    m.model = {"hky85": MODEL_HKY85, "irreversible": MODEL_IRREVERSIBLE}[model]
+    m.nallele = int(nallele)
+    m.kappa = float(kappa)
+    for i, v in enumerate(pi):
+        m.pi[i] = float(v)
+    m.rate = float(rate)
+    keep = None
+    if allele_freq is not None:
+        keep = np.ascontiguousarray(allele_freq, dtype=np.float64)
+        m.allele_freq = keep.ctypes.data
+    m.mem_budget = int(mem_budget)
+    return m, keep
+
+
+def _fel_args(edge, brlen, codes, weights):
+    edge = _u32(edge).reshape(-1, 2)
+    brlen = np.ascontiguousarray(brlen, dtype=np.float64)
+    codes = _u32(codes)
+    ntip, nsite = codes.shape
+    wk = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+    return edge, brlen, codes, ntip, nsite, wk
+
+
+def felsenstein_loglik(edge, brlen, codes, model="hky85", kappa=2.0, pi=(0.25, 0.25, 0.25, 0.25), rate=1.0,
+                       nallele=1, allele_freq=None, weights=None, grad=False, mem_budget=0):
+    """log L of the tree (.edge2 rows, tips 0..ntip-1) and, with grad=True,
+    d log L / d brlen by the adjoint pass."""
+    edge, brlen, codes, ntip, nsite, wk = _fel_args(edge, brlen, codes, weights)
+    m, _keep = _fel_model(model, kappa, pi, rate, nallele, allele_freq, mem_budget)
+    ll = C.c_double(0)
+    g = np.zeros(len(brlen)) if grad else None
+    _chk(lib().casphy_felsenstein_loglik(ntip, len(edge), edge, brlen, nsite, codes,
+                                         None if wk is None else wk.ctypes.data, C.byref(m), C.byref(ll),
+                                         None if g is None else g.ctypes.data), "casphy_felsenstein_loglik")
+    return (ll.value, g) if grad else ll.value
+
+
+def felsenstein_optimize(edge, brlen, codes, model="hky85", kappa=2.0, pi=(0.25, 0.25, 0.25, 0.25), rate=1.0,
+                         nallele=1, allele_freq=None, weights=None, gradient="adjoint", max_iter=200,
+                         rel_tol=1e-9, mem_budget=0):
+    """L-BFGS branch lengths; returns (optimised brlen, stats dict)."""
+    edge, brlen, codes, ntip, nsite, wk = _fel_args(edge, brlen, codes, weights)
+    m, _keep = _fel_model(model, kappa, pi, rate, nallele, allele_freq, mem_budget)
+    t = brlen.copy()
+    st = BloptStats()
+    mode = {"adjoint": GRAD_ADJOINT, "central_diff": GRAD_CENTRAL_DIFF}[gradient]
+    _chk(lib().casphy_felsenstein_optimize(ntip, len(edge), edge, t, nsite, codes,
+                                           None if wk is None else wk.ctypes.data, C.byref(m), mode, max_iter,
+                                           rel_tol, C.byref(st)), "casphy_felsenstein_optimize")
+    return t, st.as_dict()

@@ -194,3 +194,33 @@ def dna_to_fasta2bin(states: np.ndarray):
         cnt = (states == b).sum(axis=0)
         var |= (cnt > 0) & (cnt < n)
     return formats.encode_dna_codes(codes[:, var]), var
+
+
+def dna_nibbles(states: np.ndarray) -> np.ndarray:
+    """States 0..3 (A,C,G,T) / 4 gap -> the fasta2bin 4-bit nibble per site
+    as u32 (A=1, T=2, C=4, G=8; a gap has an empty nibble = missing)."""
+    lut = np.array([0x1, 0x4, 0x8, 0x2, 0x0], dtype=np.uint32)
+    return lut[states]
+
+
+def edit_alignment(ntip: int, nsite: int, rate: float, nallele: int, zipf_s: float,
+                   mean_bl: float, p_missing: float, seed: int):
+    """Irreversible CRISPR edits simulated on a Yule tree: the root is
+    unedited, along an edge of length t an unedited site is edited with
+    probability 1 - exp(-rate t) into allele a with Zipf(zipf_s) frequency,
+    and edited sites never change.  Returns .tbmat-coded tips (u32: 0
+    missing, 1 unedited, a+1 allele a) and the tree (parent, child, length)."""
+    rng = np.random.default_rng(seed)
+    par, ch, bl = yule_tree(ntip, mean_bl, rng)
+    nn = 2 * ntip - 1
+    q = 1.0 / np.arange(1, nallele + 1) ** zipf_s
+    q /= q.sum()
+    st = np.zeros((nn, nsite), dtype=np.int64)
+    for e in range(len(ch)):
+        s = st[par[e]].copy()
+        hit = (s == 0) & (rng.random(nsite) < -np.expm1(-rate * bl[e]))
+        s[hit] = 1 + rng.choice(nallele, size=int(hit.sum()), p=q)
+        st[ch[e]] = s
+    codes = (st[:ntip] + 1).astype(np.uint32)
+    codes[rng.random(codes.shape) < p_missing] = 0
+    return codes, (par, ch, bl)

@@ -150,6 +150,70 @@ int casphy_transfer_dis(uint32_t nrow_y, uint32_t nrow_x, uint32_t ncol, uint32_
                         uint32_t *xmin, uint32_t *xsize);
 
 /*
+ * Bootstrap column resampling of a fasta2bin matrix (the gather of
+ * cu/Felsenstein.cu:34-54): in is ntip x nbin u32 (4 byte codes per word),
+ * idx holds nidx byte positions; out (ntip x ceil(nidx/4) u32) gets, in byte
+ * j of word i of each row, the input byte at idx[4i+j] (0 for a position
+ * past the row; bytes past nidx in the last word are 0).
+ */
+int casphy_resample_columns(uint32_t ntip, uint32_t nbin, const uint32_t *in, uint32_t nidx,
+                            const uint32_t *idx, uint32_t *out);
+
+/*
+ * Felsenstein pruning and branch-length optimisation.  No counterpart in the
+ * reference (its cu/Felsenstein.cu is the column resampler above and its
+ * branch lengths are parsimony change counts, src/functions.cpp:3480-3542).
+ * The tree is given as an .edge2 body: nedge = 2*ntip-2 rows (parent, child),
+ * tips 0..ntip-1, internal nodes ntip..2*ntip-2, every internal node with two
+ * children; brlen[e] is the length of edge row e.  tip_codes is ntip x nsite
+ * u32: for HKY85 the fasta2bin nibble (bit 0 A, 1 T, 2 C, 3 G, 0 = missing),
+ * for the irreversible edit model the .tbmat coding (0 missing, 1 unedited,
+ * c >= 2 allele c-1).  site_weights may be NULL (all 1).
+ */
+#define CASPHY_MODEL_HKY85 0
+#define CASPHY_MODEL_IRREVERSIBLE 1
+#define CASPHY_GRAD_ADJOINT 0       /* one outside (pre-order) pass per gradient */
+#define CASPHY_GRAD_CENTRAL_DIFF 1  /* per-edge central differences, 2 evaluations per edge */
+
+typedef struct {
+    uint32_t model;             /* CASPHY_MODEL_* */
+    uint32_t nallele;           /* irreversible: alleles 1..nallele */
+    double kappa;               /* HKY85 transition/transversion rate ratio */
+    double pi[4];               /* HKY85 base frequencies, order A, T, C, G */
+    double rate;                /* irreversible: edit rate per unit length */
+    const double *allele_freq;  /* irreversible: nsite x (nallele+1), column 0
+                                   unused; NULL = the tips' allele frequencies */
+    uint64_t mem_budget;        /* device bytes for partials (0 = no limit);
+                                   sites are processed in chunks that fit */
+} casphy_felsenstein_model;
+
+typedef struct {
+    uint32_t iterations;        /* accepted L-BFGS steps */
+    uint32_t evaluations;       /* likelihood evaluations (graph launches) */
+    uint32_t site_chunks;
+    uint32_t levels_inside;     /* tree height (inside launches per chunk) */
+    uint32_t levels_outside;    /* depth levels (outside launches per chunk) */
+    uint32_t reserved;
+    double loglik_start, loglik_end;
+    double seconds;             /* device time of the whole optimisation */
+    uint64_t launches_per_eval; /* kernels in one evaluation graph */
+} casphy_blopt_stats;
+
+/* log L (FP32 partials with per-site power-of-two scaling, FP64 site sums) and,
+ * when grad is non-NULL, d log L / d brlen for every edge by the adjoint pass. */
+int casphy_felsenstein_loglik(uint32_t ntip, uint32_t nedge, const uint32_t *edge,
+                              const double *brlen, uint32_t nsite, const uint32_t *tip_codes,
+                              const double *site_weights, const casphy_felsenstein_model *model,
+                              double *loglik, double *grad);
+/* L-BFGS over log branch lengths (FP64 step on the device) until the relative
+ * change of log L in one step is <= rel_tol or max_iter steps; brlen is
+ * updated in place (clamped to [1e-8, 10]). */
+int casphy_felsenstein_optimize(uint32_t ntip, uint32_t nedge, const uint32_t *edge, double *brlen,
+                                uint32_t nsite, const uint32_t *tip_codes, const double *site_weights,
+                                const casphy_felsenstein_model *model, int gradient_mode,
+                                uint32_t max_iter, double rel_tol, casphy_blopt_stats *stats);
+
+/*
  * Zero-allocation variant of casphy_join_indel_dev.  It has no counterpart
  * in the reference; it exists for callers that must not allocate device
  * memory during the call -- e.g. a framework that has already reserved the

@@ -1,0 +1,145 @@
+"""Felsenstein pruning on the GPU (FP32 partials, FP64 sums) against the FP64
+oracle: log L to 1e-6 relative, the adjoint gradient against the oracle's
+gradient and central differences, reproducibility, site chunking, and the
+branch-length optimiser (adjoint against per-edge central differences)."""
+import numpy as np
+import pytest
+
+import felsenstein as F
+from casphy_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+PI = [0.3, 0.2, 0.2, 0.3]
+LL_RTOL = 1e-6  # |log L - log L_fp64| / |log L_fp64|
+
+
+def _edge(par, ch):
+    return np.stack([par, ch], axis=1).astype(np.uint32)
+
+
+def _hky_case(ntip, nsite, seed, mean_bl=0.05, p_gap=0.02):
+    states, (par, ch, t) = synth.hky85_alignment(ntip, nsite, 4.0, PI, mean_bl, p_gap, seed=seed)
+    return synth.dna_nibbles(states), par, ch, t
+
+
+def _edit_case(ntip, nsite, seed):
+    codes, (par, ch, t) = synth.edit_alignment(ntip, nsite, 1.0, 30, 1.5, 0.15, 0.1, seed=seed)
+    return codes, par, ch, t
+
+
+@pytest.mark.parametrize("ntip,nsite,seed", [(2, 5, 1), (17, 130, 2), (200, 300, 3), (1000, 257, 4)])
+def test_hky85_loglik_and_gradient(gpu_lib, ntip, nsite, seed):
+    codes, par, ch, t = _hky_case(ntip, nsite, seed)
+    w = np.random.default_rng(seed).integers(0, 4, nsite).astype(np.float64)
+    ll, g = gpu_lib.felsenstein_loglik(_edge(par, ch), t, codes, kappa=4.0, pi=PI, weights=w, grad=True)
+    ll0, g0 = F.loglik_hky85(ntip, par, ch, t, codes, w, 4.0, PI, grad=True)
+    assert abs(ll - ll0) <= LL_RTOL * abs(ll0)
+    scale = np.abs(g0).max()
+    assert np.allclose(g, g0, rtol=2e-4, atol=2e-5 * scale)
+
+
+@pytest.mark.parametrize("ntip,nsite,seed", [(2, 4, 1), (33, 150, 5), (400, 260, 6)])
+def test_irreversible_loglik_and_gradient(gpu_lib, ntip, nsite, seed):
+    codes, par, ch, t = _edit_case(ntip, nsite, seed)
+    q = F.allele_freqs(codes)
+    nallele = q.shape[1] - 1
+    ll, g = gpu_lib.felsenstein_loglik(_edge(par, ch), t, codes, model="irreversible", rate=1.0,
+                                       nallele=nallele, grad=True)
+    ll0, g0 = F.loglik_irreversible(ntip, par, ch, t, codes, None, 1.0, q, grad=True)
+    assert abs(ll - ll0) <= LL_RTOL * abs(ll0)
+    scale = np.abs(g0).max()
+    assert np.allclose(g, g0, rtol=2e-4, atol=2e-5 * scale)
+
+
+def test_gradient_against_central_differences(gpu_lib):
+    codes, par, ch, t = _hky_case(24, 200, 9, mean_bl=0.1)
+    _, g = gpu_lib.felsenstein_loglik(_edge(par, ch), t, codes, kappa=4.0, pi=PI, grad=True)
+    fd = F.central_differences(lambda tt: F.loglik_hky85(24, par, ch, tt, codes, None, 4.0, PI), t)
+    assert np.allclose(g, fd, rtol=1e-3, atol=1e-4 * np.abs(fd).max())
+
+
+def test_site_chunks_and_repeat_are_bitwise_identical(gpu_lib):
+    codes, par, ch, t = _hky_case(300, 1000, 11)
+    e = _edge(par, ch)
+    a = gpu_lib.felsenstein_loglik(e, t, codes, kappa=4.0, pi=PI, grad=True)
+    b = gpu_lib.felsenstein_loglik(e, t, codes, kappa=4.0, pi=PI, grad=True)
+    # 299 internal nodes x 36 B per site: a 3 MB budget gives 256-site chunks
+    c = gpu_lib.felsenstein_loglik(e, t, codes, kappa=4.0, pi=PI, grad=True, mem_budget=3_000_000)
+    assert a[0] == b[0] == c[0]
+    assert np.array_equal(a[1], b[1]) and np.array_equal(a[1], c[1])
+    codes, par, ch, t = _edit_case(300, 700, 12)
+    q = F.allele_freqs(codes)
+    kw = dict(model="irreversible", rate=1.0, nallele=q.shape[1] - 1, grad=True)
+    a = gpu_lib.felsenstein_loglik(_edge(par, ch), t, codes, **kw)
+    c = gpu_lib.felsenstein_loglik(_edge(par, ch), t, codes, mem_budget=1_500_000, **kw)
+    assert a[0] == c[0] and np.array_equal(a[1], c[1])
+
+
+def test_given_allele_frequencies(gpu_lib):
+    codes, par, ch, t = _edit_case(50, 90, 13)
+    nallele = int(codes.max()) - 1
+    q = np.random.default_rng(1).random((90, nallele + 1)) + 0.05
+    q[:, 0] = 0
+    q /= q.sum(axis=1, keepdims=True)
+    ll = gpu_lib.felsenstein_loglik(_edge(par, ch), t, codes, model="irreversible", rate=0.7,
+                                    nallele=nallele, allele_freq=q)
+    ll0 = F.loglik_irreversible(50, par, ch, t, codes, None, 0.7, q)
+    assert abs(ll - ll0) <= LL_RTOL * abs(ll0)
+
+
+def test_optimizer_adjoint_matches_central_differences(gpu_lib):
+    codes, par, ch, t_true = _hky_case(20, 400, 21, mean_bl=0.08)
+    e = _edge(par, ch)
+    t0 = np.full(len(t_true), 0.05)
+    kw = dict(kappa=4.0, pi=PI, rel_tol=1e-10, max_iter=300)
+    ta, sa = gpu_lib.felsenstein_optimize(e, t0, codes, gradient="adjoint", **kw)
+    tf, sf = gpu_lib.felsenstein_optimize(e, t0, codes, gradient="central_diff", **kw)
+    la = F.loglik_hky85(20, par, ch, ta, codes, None, 4.0, PI)
+    lf = F.loglik_hky85(20, par, ch, tf, codes, None, 4.0, PI)
+    l0 = F.loglik_hky85(20, par, ch, t0, codes, None, 4.0, PI)
+    assert la > l0 + 1.0
+    assert abs(la - lf) <= 1e-6 * abs(la)
+    # the reported final log L is the GPU value at the returned lengths
+    assert abs(sa["loglik_end"] - la) <= LL_RTOL * abs(la)
+    assert sa["evaluations"] < sf["evaluations"]
+    # near-stationary: oracle gradient (in log t) small against its start
+    _, g = F.loglik_hky85(20, par, ch, ta, codes, None, 4.0, PI, grad=True)
+    _, g0 = F.loglik_hky85(20, par, ch, t0, codes, None, 4.0, PI, grad=True)
+    assert np.abs(g * ta).max() < 1e-2 * np.abs(g0 * t0).max()
+
+
+def test_optimizer_irreversible(gpu_lib):
+    codes, par, ch, _ = _edit_case(60, 200, 22)
+    q = F.allele_freqs(codes)
+    t0 = np.full(2 * 60 - 2, 0.1)
+    t, st = gpu_lib.felsenstein_optimize(_edge(par, ch), t0, codes, model="irreversible", rate=1.0,
+                                         nallele=q.shape[1] - 1, rel_tol=1e-10, max_iter=500)
+    l1 = F.loglik_irreversible(60, par, ch, t, codes, None, 1.0, q)
+    assert l1 >= F.loglik_irreversible(60, par, ch, t0, codes, None, 1.0, q)
+    assert abs(st["loglik_end"] - l1) <= LL_RTOL * abs(l1)
+
+
+def test_bad_trees_raise(gpu_lib):
+    codes, par, ch, t = _hky_case(8, 10, 1)
+    e = _edge(par, ch)
+    bad = e.copy()
+    bad[3, 0] = bad[0, 0]  # a node with three children
+    with pytest.raises(gpu_lib.CasphyError):
+        gpu_lib.felsenstein_loglik(bad, t, codes, kappa=4.0, pi=PI)
+    with pytest.raises(gpu_lib.CasphyError):
+        gpu_lib.felsenstein_loglik(e[:-1], t[:-1], codes, kappa=4.0, pi=PI)
+    with pytest.raises(gpu_lib.CasphyError):
+        gpu_lib.felsenstein_loglik(e, -t, codes, kappa=4.0, pi=PI)
+
+
+def test_resample_columns_matches_gather(gpu_lib):
+    rng = np.random.default_rng(3)
+    raw = rng.integers(0, 2**32, size=(37, 11), dtype=np.uint64).astype(np.uint32)
+    idx = np.sort(rng.integers(0, 44, size=41)).astype(np.uint32)
+    out = gpu_lib.resample_columns(raw, idx)
+    b = raw.view(np.uint8).reshape(37, 44)
+    exp = np.zeros((37, 44), np.uint8)
+    exp[:, :41] = b[:, idx]
+    assert np.array_equal(out.view(np.uint8).reshape(37, -1)[:, :41], exp[:, :41])
+    assert np.all(out.view(np.uint8).reshape(37, -1)[:, 41:] == 0)
