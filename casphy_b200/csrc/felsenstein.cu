@@ -40,6 +40,8 @@
 // vector is (U0, X, Y, allele) with U(a) = X q_a + Y [a == allele].
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -105,7 +107,9 @@ __global__ void k_pmat_hky(const double* __restrict__ t, u32 nedge, Hky m, float
                 a += m.V[i * 4 + k] * ex[k] * m.Vi[k * 4 + j];
                 b += m.V[i * 4 + k] * dx[k] * m.Vi[k * 4 + j];
             }
-            P[e * 16 + i * 4 + j] = (float)fmax(a, 0.0);
+            // store P - I: O(t) entries with full relative precision, so the
+            // binary32 rounding is not one shared error across all sites
+            P[e * 16 + i * 4 + j] = (float)(i == j ? a - 1.0 : fmax(a, 0.0));
             dP[e * 16 + i * 4 + j] = (float)b;
         }
 }
@@ -123,11 +127,17 @@ __device__ __forceinline__ float4 matvec(const float* __restrict__ P, float4 x) 
                        P[12] * x.x + P[13] * x.y + P[14] * x.z + P[15] * x.w);
 }
 
-__device__ __forceinline__ float4 vecmat(float4 r, const float* __restrict__ P) {  // r^T P
-    return make_float4(r.x * P[0] + r.y * P[4] + r.z * P[8] + r.w * P[12],
-                       r.x * P[1] + r.y * P[5] + r.z * P[9] + r.w * P[13],
-                       r.x * P[2] + r.y * P[6] + r.z * P[10] + r.w * P[14],
-                       r.x * P[3] + r.y * P[7] + r.z * P[11] + r.w * P[15]);
+// (I + D) x and r^T (I + D) for D = P - I
+__device__ __forceinline__ float4 pmatvec(const float* __restrict__ D, float4 x) {
+    const float4 d = matvec(D, x);
+    return make_float4(x.x + d.x, x.y + d.y, x.z + d.z, x.w + d.w);
+}
+
+__device__ __forceinline__ float4 pvecmat(float4 r, const float* __restrict__ D) {
+    return make_float4(r.x + (r.x * D[0] + r.y * D[4] + r.z * D[8] + r.w * D[12]),
+                       r.y + (r.x * D[1] + r.y * D[5] + r.z * D[9] + r.w * D[13]),
+                       r.z + (r.x * D[2] + r.y * D[6] + r.z * D[10] + r.w * D[14]),
+                       r.w + (r.x * D[3] + r.y * D[7] + r.z * D[11] + r.w * D[15]));
 }
 
 __device__ __forceinline__ float dot4(float4 a, float4 b) { return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w; }
@@ -149,8 +159,8 @@ struct HkyBuf {
     float4* L;         // nint x W
     int* E;            // nint x W
     float4* U;         // nint x W
-    const float* P;
-    const float* dP;
+    const float* P;   // per edge P - I (row-major 4x4)
+    const float* dP;  // per edge dP/dt
 };
 
 __device__ __forceinline__ float4 child_hky(const Tree& T, const HkyBuf& B, const Chunk& C, u32 c, u32 s, int* e) {
@@ -170,8 +180,8 @@ __global__ void __launch_bounds__(kSites) k_inside_hky(Tree T, HkyBuf B, Chunk C
     int ea, eb;
     const float4 la = child_hky(T, B, C, T.kidA[vi], s, &ea);
     const float4 lb = child_hky(T, B, C, T.kidB[vi], s, &eb);
-    const float4 ma = matvec(B.P + 16 * T.edgeA[vi], la);
-    const float4 mb = matvec(B.P + 16 * T.edgeB[vi], lb);
+    const float4 ma = pmatvec(B.P + 16 * T.edgeA[vi], la);
+    const float4 mb = pmatvec(B.P + 16 * T.edgeB[vi], lb);
     float4 l = make_float4(ma.x * mb.x, ma.y * mb.y, ma.z * mb.z, ma.w * mb.w);
     const int e = renorm4(l);
     B.L[(size_t)vi * C.W + s] = l;
@@ -209,7 +219,7 @@ __global__ void __launch_bounds__(kSites) k_outside_hky(u32 root, Tree T, HkyBuf
     const u32 eA = T.edgeA[vi], eB = T.edgeB[vi];
     const float4 la = child_hky(T, B, C, ca, ss, &e);
     const float4 lb = child_hky(T, B, C, cb, ss, &e);
-    const float4 ma = matvec(B.P + 16 * eA, la), mb = matvec(B.P + 16 * eB, lb);
+    const float4 ma = pmatvec(B.P + 16 * eA, la), mb = pmatvec(B.P + 16 * eB, lb);
     const double ws = ok ? w[C.s0 + s] : 0.0;
 #pragma unroll
     for (int side = 0; side < 2; side++) {
@@ -225,7 +235,7 @@ __global__ void __launch_bounds__(kSites) k_outside_hky(u32 root, Tree T, HkyBuf
         g = block_sum(g, red);
         if (threadIdx.x == 0) gpart[(size_t)ec * C.nblkTot + C.blk0 + blockIdx.x] = g;
         if (ok && c >= T.ntip) {
-            float4 uc = vecmat(r, B.P + 16 * ec);
+            float4 uc = pvecmat(r, B.P + 16 * ec);
             renorm4(uc);
             B.U[(size_t)(c - T.ntip) * C.W + s] = uc;
         }
@@ -280,8 +290,8 @@ __global__ void __launch_bounds__(kSites) k_inside_irr(Tree T, IrrBuf B, Chunk C
     const float4 la = child_irr(T, B, C, T.kidA[vi], s);
     const float4 lb = child_irr(T, B, C, T.kidB[vi], s);
     const float2 pa = B.p[T.edgeA[vi]], pb = B.p[T.edgeB[vi]];
-    const float m0a = pa.x * la.x + pa.y * qsum(B, gs, la);
-    const float m0b = pb.x * lb.x + pb.y * qsum(B, gs, lb);
+    const float m0a = la.x + pa.y * (qsum(B, gs, la) - la.x);
+    const float m0b = lb.x + pb.y * (qsum(B, gs, lb) - lb.x);
     const int aa = __float_as_int(la.z), ab = __float_as_int(lb.z);
     float l0 = m0a * m0b, lA = 0.f;
     int a = kNoneA;
@@ -341,7 +351,7 @@ __global__ void __launch_bounds__(kSites) k_outside_irr(u32 root, Tree T, IrrBuf
         l[i] = child_irr(T, B, C, kids[i], ss);
         pp[i] = B.p[eds[i]];
         qs[i] = qsum(B, gs, l[i]);
-        m0[i] = pp[i].x * l[i].x + pp[i].y * qs[i];
+        m0[i] = l[i].x + pp[i].y * (qs[i] - l[i].x);
     }
     const double ws = ok ? w[gs] : 0.0;
 #pragma unroll
@@ -1018,15 +1028,18 @@ static int lb_check_err(FelProblem& F) {
     return CASPHY_OK;
 }
 
-// per-edge central differences of log L into F.grad
+// Per-edge central differences of log L into F.grad (as d log L / d t).
+// The step is taken in x = log t: t e^{+-h} with h = 1e-3, large enough that
+// the binary32 rounding of the partials (about 1e-7 of |log L|) stays well
+// below the difference, small enough that the O(h^2) truncation does too.
 static int fd_gradient(FelProblem& F, casphy_blopt_stats& st) {
     const u32 n = F.th.nedge;
+    const double h = 1e-3;
     std::vector<double> t(n), g(n);
     CASPHY_CUDA_TRY(cudaMemcpyAsync(t.data(), F.t, 8ull * n, cudaMemcpyDeviceToHost, F.st));
     CASPHY_CUDA_TRY(cudaStreamSynchronize(F.st));
     for (u32 i = 0; i < n; i++) {
-        const double h = 1e-5 * std::max(t[i], 1e-3);
-        const double tp = t[i] + h, tm = std::max(t[i] - h, 0.0);
+        const double tp = t[i] * std::exp(h), tm = t[i] * std::exp(-h);
         double lp = 0, lm = 0;
         int rc;
         CASPHY_CUDA_TRY(cudaMemcpyAsync(F.t + i, &tp, 8, cudaMemcpyHostToDevice, F.st));
@@ -1035,7 +1048,7 @@ static int fd_gradient(FelProblem& F, casphy_blopt_stats& st) {
         if ((rc = F.eval(false, &lm))) return rc;
         CASPHY_CUDA_TRY(cudaMemcpyAsync(F.t + i, &t[i], 8, cudaMemcpyHostToDevice, F.st));
         st.evaluations += 2;
-        g[i] = (lp - lm) / (tp - tm);
+        g[i] = (lp - lm) / (2 * h) / t[i];
     }
     CASPHY_CUDA_TRY(cudaMemcpyAsync(F.grad, g.data(), 8ull * n, cudaMemcpyHostToDevice, F.st));
     CASPHY_CUDA_TRY(cudaStreamSynchronize(F.st));
@@ -1078,6 +1091,7 @@ extern "C" int casphy_felsenstein_optimize(uint32_t ntip, uint32_t nedge, const 
     rc = setup_problem(F, ds, ntip, nedge, edge, brlen, nsite, tip_codes, site_weights, model, M);
     if (rc) return rc;
     const bool adj = gradient_mode == CASPHY_GRAD_ADJOINT;
+    const bool trace = std::getenv("CASPHY_TRACE") != nullptr;
     const u32 n = nedge, nb = (n + 255) / 256;
     casphy_blopt_stats st{};
     Lb a = F.lb;
@@ -1141,6 +1155,9 @@ extern "C" int casphy_felsenstein_optimize(uint32_t ntip, uint32_t nedge, const 
             else first = (first + 1) % a.Mr;
         }
         const double rel = std::fabs(f - fn) / std::max(std::fabs(f), 1e-300);
+        if (trace)
+            std::fprintf(stderr, "blopt it %u f %.10f df %.3e gd %.3e step %.3e hist %u sy %.3e\n", it, fn, fn - f, gd,
+                         step, count, sy);
         f = fn;
         if (rel <= rel_tol) break;
     }

@@ -88,7 +88,20 @@ def test_given_allele_frequencies(gpu_lib):
     assert abs(ll - ll0) <= LL_RTOL * abs(ll0)
 
 
-def test_optimizer_adjoint_matches_central_differences(gpu_lib):
+def _fp64_optimum(f_and_g, t0):
+    from scipy.optimize import minimize
+
+    def fun(x):
+        ll, g = f_and_g(np.exp(x))
+        return -ll, -g * np.exp(x)
+
+    r = minimize(fun, np.log(t0), jac=True, method="L-BFGS-B",
+                 bounds=[(np.log(1e-8), np.log(10.0))] * len(t0),
+                 options=dict(maxiter=5000, ftol=1e-15, gtol=1e-10))
+    return -r.fun
+
+
+def test_optimizer_reaches_fp64_optimum_and_beats_central_differences(gpu_lib):
     codes, par, ch, t_true = _hky_case(20, 400, 21, mean_bl=0.08)
     e = _edge(par, ch)
     t0 = np.full(len(t_true), 0.05)
@@ -98,15 +111,13 @@ def test_optimizer_adjoint_matches_central_differences(gpu_lib):
     la = F.loglik_hky85(20, par, ch, ta, codes, None, 4.0, PI)
     lf = F.loglik_hky85(20, par, ch, tf, codes, None, 4.0, PI)
     l0 = F.loglik_hky85(20, par, ch, t0, codes, None, 4.0, PI)
-    assert la > l0 + 1.0
-    assert abs(la - lf) <= 1e-6 * abs(la)
+    best = _fp64_optimum(lambda t: F.loglik_hky85(20, par, ch, t, codes, None, 4.0, PI, grad=True), t0)
+    # the adjoint optimiser lands within 1e-6 (relative) of the FP64 optimum
+    assert abs(la - best) <= 1e-6 * abs(best)
+    assert lf > l0 + 1.0 and la >= lf - 1e-6 * abs(la)
     # the reported final log L is the GPU value at the returned lengths
     assert abs(sa["loglik_end"] - la) <= LL_RTOL * abs(la)
-    assert sa["evaluations"] < sf["evaluations"]
-    # near-stationary: oracle gradient (in log t) small against its start
-    _, g = F.loglik_hky85(20, par, ch, ta, codes, None, 4.0, PI, grad=True)
-    _, g0 = F.loglik_hky85(20, par, ch, t0, codes, None, 4.0, PI, grad=True)
-    assert np.abs(g * ta).max() < 1e-2 * np.abs(g0 * t0).max()
+    assert sa["evaluations"] * 10 < sf["evaluations"]
 
 
 def test_optimizer_irreversible(gpu_lib):
@@ -118,6 +129,8 @@ def test_optimizer_irreversible(gpu_lib):
     l1 = F.loglik_irreversible(60, par, ch, t, codes, None, 1.0, q)
     assert l1 >= F.loglik_irreversible(60, par, ch, t0, codes, None, 1.0, q)
     assert abs(st["loglik_end"] - l1) <= LL_RTOL * abs(l1)
+    best = _fp64_optimum(lambda tt: F.loglik_irreversible(60, par, ch, tt, codes, None, 1.0, q, grad=True), t0)
+    assert abs(l1 - best) <= 1e-6 * abs(best)
 
 
 def test_bad_trees_raise(gpu_lib):
