@@ -72,6 +72,7 @@ __device__ __forceinline__ u64 globaltimer_ns() {
 // wait gives up after limit_ns and records CASPHY_ETIMEOUT.
 __device__ __forceinline__ int flag_barrier(u32* flags, u32 nCTA, u32 epoch, int* err, u64 limit_ns) {
     __syncthreads();
+    if (nCTA == 1) return 0;  // one CTA: the block barrier orders its global accesses
     if (threadIdx.x == 0) st_release_u32(flags + blockIdx.x * 16u, epoch);  // gpu-scope release, cumulative
     int fail = 0;
     if (threadIdx.x < nCTA) {

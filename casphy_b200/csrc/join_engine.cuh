@@ -75,7 +75,7 @@ struct Prof {
     u64 t;
     bool on;
     __device__ __forceinline__ void init(bool enable) {
-        on = enable && blockIdx.x == 0 && threadIdx.x == 0;
+        on = enable && threadIdx.x == 0;
         for (int i = 0; i < PROF_N; i++) acc[i] = 0;
         t = on ? globaltimer_ns() : 0;
     }
@@ -291,9 +291,10 @@ __device__ inline void compact_slots(const Common& a, u32 buf, u32 nb, const Ran
     __syncthreads();
 }
 
+// The join loop for CTA b of a.nCTA co-resident CTAs (b = 0 of 1 when one
+// CTA runs a whole join by itself).  smem: engine + model dynamic memory.
 template <class M>
-__global__ void __launch_bounds__(kThreads, 1) k_join(Common a, typename M::Args m) {
-    extern __shared__ __align__(16) unsigned char smem[];
+__device__ __forceinline__ void join_run(const Common& a, const typename M::Args& m, u32 b, unsigned char* smem) {
     u32* ordOut = reinterpret_cast<u32*>(smem);                        // kMaxCap
     BlockRec* tabRec = reinterpret_cast<BlockRec*>(ordOut + kMaxCap);  // 2*nCTA
     u32* ranks = reinterpret_cast<u32*>(tabRec + 2 * a.nCTA);          // Rmax
@@ -311,9 +312,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_join(Common a, typename M::Args
     __shared__ int s_flag;
 
     const Table T{tabRec, tabCnt, tabExact};
-    const u32 b = blockIdx.x, nCTA = a.nCTA;
+    const u32 nCTA = a.nCTA;
     Prof pf;
-    pf.init(a.prof != nullptr);
+    pf.init(a.prof != nullptr && b == 0);
     u32 buf = 0;
     Range rg = make_range(a.ntip, nCTA, b, a.align);
     u32 k = 0, p = 0;
@@ -558,6 +559,12 @@ out:
     }
     if (pf.on)
         for (int i = 0; i < PROF_N; i++) a.prof[i] = pf.acc[i];
+}
+
+template <class M>
+__global__ void __launch_bounds__(kThreads, 1) k_join(Common a, typename M::Args m) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    join_run<M>(a, m, blockIdx.x, smem);
 }
 
 // Host: bytes of engine shared memory before the model's part.

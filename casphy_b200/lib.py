@@ -47,6 +47,15 @@ class BloptStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
+class BootstrapStats(C.Structure):
+    _fields_ = [("nrep", C.c_uint32), ("nclade", C.c_uint32), ("prep_ms", C.c_double), ("join_ms", C.c_double),
+                ("transfer_ms", C.c_double), ("total_ms", C.c_double), ("kernel_launches", C.c_uint64),
+                ("join_phases", C.c_uint64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 MODEL_HKY85, MODEL_IRREVERSIBLE = 0, 1
 GRAD_ADJOINT, GRAD_CENTRAL_DIFF = 0, 1
 
@@ -88,6 +97,8 @@ def lib():
                                                 C.POINTER(C.c_double), vp]
         L.casphy_felsenstein_optimize.argtypes = [u32, u32, _u32p, _f64p, u32, _u32p, vp, C.POINTER(FelModel),
                                                   C.c_int, u32, C.c_double, C.POINTER(BloptStats)]
+        L.casphy_bootstrap_bit.argtypes = [u32, u32, _u32p, _u32p, u32, _u32p, _u32p, _f64p, C.c_int, C.c_double,
+                                           _u32p, vp, vp, vp, C.POINTER(BootstrapStats)]
         if hasattr(L, "casphy_join_bit"):
             L.casphy_join_bit.argtypes = [u32, u32, _u32p, _f64p, C.c_int, _u32p, _u32p, C.POINTER(JoinStats)]
             L.casphy_join_bit_dev.argtypes = [u32, u32, vp, _f64p, C.c_int, _u32p, vp, C.POINTER(JoinStats), vp]
@@ -260,3 +271,29 @@ def felsenstein_optimize(edge, brlen, codes, model="hky85", kappa=2.0, pi=(0.25,
                                            None if wk is None else wk.ctypes.data, C.byref(m), mode, max_iter,
                                            rel_tol, C.byref(st)), "casphy_felsenstein_optimize")
     return t, st.as_dict()
+
+
+def bootstrap_bit(words, full_edge, offsets, cells, weights, ancestral_type=1, threshold=0.05, matrices=True,
+                  raw_edges=False):
+    """Batched bootstrap: returns dict(support, ymin, ysize, raw_edges, stats)."""
+    words = _u32(words)
+    ntip, nbin = words.shape
+    edge = _u32(full_edge).reshape(-1, 2)
+    offsets, cells = _u32(offsets), _u32(cells)
+    nrep = len(offsets) - 1
+    weights = np.ascontiguousarray(weights, dtype=np.float64).reshape(nrep, nbin * 32)
+    nX = ntip - 2
+    support = np.zeros(max(nX, 1), np.uint32)
+    ymin = np.zeros((nrep, nX), np.uint32) if matrices else None
+    ysize = np.zeros((nrep, nX), np.uint32) if matrices else None
+    n = np.diff(offsets.astype(np.int64))
+    raw = np.zeros(int((4 * (n - 1)).sum()), np.uint32) if raw_edges else None
+    st = BootstrapStats()
+    ptr = lambda a: None if a is None else a.ctypes.data
+    _chk(lib().casphy_bootstrap_bit(ntip, nbin, words, edge, nrep, offsets, cells, weights.reshape(-1),
+                                    1 if ancestral_type else 0, float(threshold), support, ptr(ymin), ptr(ysize),
+                                    ptr(raw), C.byref(st)), "casphy_bootstrap_bit")
+    out = {"support": support[:nX], "ymin": ymin, "ysize": ysize, "stats": st.as_dict()}
+    if raw_edges:
+        out["raw_edges"] = np.split(raw, np.cumsum(4 * (n - 1))[:-1])
+    return out

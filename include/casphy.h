@@ -214,6 +214,40 @@ int casphy_felsenstein_optimize(uint32_t ntip, uint32_t nedge, const uint32_t *e
                                 uint32_t max_iter, double rel_tol, casphy_blopt_stats *stats);
 
 /*
+ * Batched bootstrap of the bit join with transfer support.  Replaces running
+ * joinEdgeBitReverse, the clade writer and TransferDisStream once per
+ * replicate (vignettes/CasPhy.Rmd:255-291, R/bootstrap_functions.R:190-219).
+ *   words        ntip x nbin u32, the full matrix (the .tbmat body)
+ *   full_edge    (2*ntip-2) x 2 u32, the .edge2 body of the full-data tree
+ *   replicate r  cells rep_cells[rep_offsets[r] .. rep_offsets[r+1]) (distinct
+ *                full-matrix rows, in the order they become the replicate's
+ *                tips 0..n_r-1) and integer site weights rep_weights[r*nbin*32
+ *                ..] (column multiplicities of the resample)
+ *   support      per clade of the full tree (its internal nodes except the
+ *                root, in increasing node id): the number of replicates with
+ *                ysize > 0 and ymin <= threshold * ysize
+ *   ymin, ysize  optional, nrep x nclade: TransferDisStream's _ymin.bin values
+ *                for the full-tree clades restricted to the replicate's cells
+ *                against the replicate tree's clades (ntip = n_r)
+ *   rep_raw_edges optional: per replicate, 2*(n_r-1) raw join edges (parent,
+ *                child) in join order over the replicate's tip ids
+ * Each replicate tree is the tree joinEdgeBitReverse builds from its rows and
+ * weights (the same engine as casphy_join_bit).
+ */
+typedef struct {
+    uint32_t nrep, nclade;
+    double prep_ms, join_ms, transfer_ms, total_ms;  /* device times */
+    uint64_t kernel_launches;
+    uint64_t join_phases;                            /* summed over replicates */
+} casphy_bootstrap_stats;
+
+int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t *words, const uint32_t *full_edge,
+                         uint32_t nrep, const uint32_t *rep_offsets, const uint32_t *rep_cells,
+                         const double *rep_weights, int ancestralType, double threshold,
+                         uint32_t *support, uint32_t *ymin, uint32_t *ysize, uint32_t *rep_raw_edges,
+                         casphy_bootstrap_stats *stats);
+
+/*
  * Zero-allocation variant of casphy_join_indel_dev.  It has no counterpart
  * in the reference; it exists for callers that must not allocate device
  * memory during the call -- e.g. a framework that has already reserved the
