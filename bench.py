@@ -204,6 +204,74 @@ def run_reference(args, world, rank):
     return 0
 
 
+def bootstrap_suite(L):
+    """Batched bootstrap (200 replicates of the 10,000-cell x 512-site binary
+    matrix, 2,000-10,000 cells each) against 200 plain runs one replicate at
+    a time (join -> clades -> TransferDisStream), both through the host API."""
+    from casphy_b200 import bootstrap as B
+    from casphy_b200 import synth
+    ncell, nsite, nrep = 10_000, 512, 200
+    words = synth.binary_workload(ncell, nsite, 16, 0.03, 0.05, seed=11)
+    full_edge, _, _ = L.join_bit(words, None, 1)
+    off, cells, w = B.make_replicates(ncell, nsite, nrep, 2000, 10_000, seed=12)
+    L.bootstrap_bit(words, full_edge, off, cells, w, threshold=0.05)  # warm-up
+    t0 = time.perf_counter()
+    got = L.bootstrap_bit(words, full_edge, off, cells, w, threshold=0.05)
+    batched_s = time.perf_counter() - t0
+    full_bits = B.clade_bits(full_edge, ncell, (ncell + 31) // 32)
+    same = True
+    ymin = np.zeros_like(got["ymin"])
+    ysize = np.zeros_like(got["ysize"])
+    t0 = time.perf_counter()
+    for r in range(nrep):
+        c = cells[off[r]:off[r + 1]]
+        ymin[r], ysize[r] = B.plain_replicate(L, words, full_bits, c, w[r])
+    plain_s = time.perf_counter() - t0
+    same = bool(np.array_equal(ymin, got["ymin"]) and np.array_equal(ysize, got["ysize"]))
+    sup_same = bool(np.array_equal(B.support_counts(ymin, ysize, 0.05), got["support"]))
+    return {"workload": f"{nrep} replicates of the {ncell} x {nsite} binary matrix (Yule depth 16, p_edit 0.03, "
+                        "5% missing), columns resampled with replacement, 2000-10000 cells each; transfer support "
+                        "of the full-data tree's clades at threshold 0.05",
+            "batched_s": batched_s, "batched_device_ms": got["stats"]["total_ms"],
+            "batched_phases": {k: got["stats"][k] for k in ("prep_ms", "join_ms", "transfer_ms")},
+            "plain_s": plain_s, "plain": "casphy_join_bit + clade bitsets + casphy_transfer_dis per replicate",
+            "speedup": plain_s / batched_s, "transfer_values_identical": same, "support_identical": sup_same}
+
+
+def blopt_suite(L):
+    """Adjoint L-BFGS branch lengths on the 20,000 x 2,000 HKY85 alignment,
+    and adjoint against per-edge central differences on a 128-tip subproblem
+    with the same sites (the central-difference run needs 2 evaluations per
+    edge per gradient and is not run at full size)."""
+    from casphy_b200 import synth
+    pi = [0.3, 0.2, 0.2, 0.3]
+    states, (par, ch, t_true) = synth.hky85_alignment(20_000, 2000, 4.0, pi, 0.01, 0.02, seed=13)
+    codes = synth.dna_nibbles(states)
+    edge = np.stack([par, ch], 1).astype(np.uint32)
+    t0 = np.full(len(t_true), 0.01)
+    L.felsenstein_optimize(edge, t0, codes, kappa=4.0, pi=pi, rel_tol=1e-9, max_iter=3)  # warm-up
+    _, full = L.felsenstein_optimize(edge, t0, codes, kappa=4.0, pi=pi, rel_tol=1e-9, max_iter=1000)
+    s_states, (sp, sc, st) = synth.hky85_alignment(128, 2000, 4.0, pi, 0.01, 0.02, seed=14)
+    s_codes = synth.dna_nibbles(s_states)
+    s_edge = np.stack([sp, sc], 1).astype(np.uint32)
+    s_t0 = np.full(len(st), 0.01)
+    _, adj = L.felsenstein_optimize(s_edge, s_t0, s_codes, kappa=4.0, pi=pi, rel_tol=1e-9, max_iter=1000)
+    _, fd = L.felsenstein_optimize(s_edge, s_t0, s_codes, kappa=4.0, pi=pi, rel_tol=1e-9, max_iter=1000,
+                                   gradient="central_diff")
+    rel = abs(fd["loglik_end"] - adj["loglik_end"]) / abs(adj["loglik_end"])
+    return {"workload": "HKY85 (kappa 4, pi .3/.2/.2/.3) 20000 tips x 2000 sites, Yule tree, Exp(mean 0.01) "
+                        "branches, 2% gaps; start at t = 0.01; FP32 partials, FP64 sums and L-BFGS step",
+            "adjoint_s": full["seconds"], "iterations": full["iterations"], "evaluations": full["evaluations"],
+            "ms_per_evaluation": full["seconds"] * 1e3 / max(full["evaluations"], 1),
+            "loglik_start": full["loglik_start"], "loglik_end": full["loglik_end"],
+            "fd_evaluations_per_gradient": 2 * len(t0),
+            "small_case": {"workload": "same model, 128 tips x 2000 sites", "adjoint_s": adj["seconds"],
+                           "adjoint_evaluations": adj["evaluations"], "adjoint_loglik": adj["loglik_end"],
+                           "central_diff_s": fd["seconds"], "central_diff_evaluations": fd["evaluations"],
+                           "central_diff_loglik": fd["loglik_end"], "speedup": fd["seconds"] / adj["seconds"],
+                           "central_diff_within_1e-6": rel <= 1e-6, "rel_loglik_gap": rel}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -212,6 +280,7 @@ def main():
     ap.add_argument("--impl", default="casphy", choices=["casphy", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-extras", action="store_true", help="skip the bootstrap and branch-length measurements")
     ap.add_argument("--cells", type=int, default=None,
                     help="profiling only: use the first N cells of the workload")
     args = ap.parse_args()
@@ -322,6 +391,9 @@ def main():
                     "h2d_bytes_per_step": int(codes.nbytes + wflat.nbytes + tip.nbytes),
                     "d2h_bytes_per_step": int(edge.nbytes + hstate_np.nbytes), "tree_s": e2e_s / e2e_steps},
             "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary()}
+    if rank == 0 and world == 1 and args.cells is None and not args.no_extras:
+        line["bootstrap"] = bootstrap_suite(L)
+        line["blopt"] = blopt_suite(L)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
