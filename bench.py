@@ -204,7 +204,7 @@ def run_reference(args, world, rank):
     return 0
 
 
-def bootstrap_suite(L):
+def bootstrap_suite(L, plain=True):
     """Batched bootstrap (200 replicates of the 10,000-cell x 512-site binary
     matrix, 2,000-10,000 cells each) against 200 plain runs one replicate at
     a time (join -> clades -> TransferDisStream), both through the host API."""
@@ -218,8 +218,9 @@ def bootstrap_suite(L):
     t0 = time.perf_counter()
     got = L.bootstrap_bit(words, full_edge, off, cells, w, threshold=0.05)
     batched_s = time.perf_counter() - t0
+    if not plain:
+        return {"batched_s": batched_s, "batched_device_ms": got["stats"]["total_ms"]}
     full_bits = B.clade_bits(full_edge, ncell, (ncell + 31) // 32)
-    same = True
     ymin = np.zeros_like(got["ymin"])
     ysize = np.zeros_like(got["ysize"])
     t0 = time.perf_counter()
@@ -281,6 +282,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-extras", action="store_true", help="skip the bootstrap and branch-length measurements")
+    ap.add_argument("--only", choices=["bootstrap", "blopt"], default=None,
+                    help="run one of the extra measurements alone (profiling)")
+    ap.add_argument("--no-plain", action="store_true", help="with --only bootstrap: skip the plain runs")
     ap.add_argument("--cells", type=int, default=None,
                     help="profiling only: use the first N cells of the workload")
     args = ap.parse_args()
@@ -298,6 +302,11 @@ def main():
 
     lib = L.lib()
     torch.cuda.set_device(local)
+    if args.only:
+        res = bootstrap_suite(L, plain=not args.no_plain) if args.only == "bootstrap" else blopt_suite(L)
+        if rank == 0:
+            print(json.dumps({args.only: res}), flush=True)
+        return 0
     codes, nstate, weight = gen_workload(args.cells)
     ntip, ncol = codes.shape
     d_codes = torch.from_numpy(codes.view(np.int32)).cuda()
