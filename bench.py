@@ -273,6 +273,107 @@ def blopt_suite(L):
                            "central_diff_within_1e-6": rel <= 1e-6, "rel_loglik_gap": rel}}
 
 
+def _timed(fn, reps=1):
+    fn()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        out = fn()
+    return out, (time.perf_counter() - t0) / reps
+
+
+def rows_suite(L, nthreads):
+    """The other rows of the hot path on their own configs, each timed through
+    the host API (inputs and outputs through host memory) next to the CPU
+    restatement (oracle/) on the host cores."""
+    import oracle as O
+    from casphy_b200 import synth
+    res = {}
+    # C1: indel 1,024 x 256, joinEdgeIndel + nodeKeepIndel
+    raw = synth.lineage_states(1024, 256, 12, 0.04, 64, 1.5, 0.10, seed=21)
+    codes, ns = synth.regularize(raw)
+    w = np.ones((ns, 256))
+    (edge, state, st), t_gpu = _timed(lambda: L.join_indel(codes, ns, w), reps=3)
+    out_raw = synth.lineage_states(256, 256, 12, 0.04, 64, 1.5, 0.10, seed=22)
+    outm, _ = synth.regularize(out_raw)
+    keep, t_keep = _timed(lambda: L.node_keep(state, edge, outm, 2), reps=3)
+    t0 = time.perf_counter()
+    e0, s0, _ = O.join_indel(codes, ns, w, None, 0, 2.0, nthreads)
+    k0 = O.node_keep(s0, e0, outm, 2)
+    t_cpu = time.perf_counter() - t0
+    res["C1_joinEdgeIndel_nodeKeepIndel"] = {
+        "workload": "indel 1024 cells x 256 sites, 64 alleles Zipf(1.5), depth 12, p_edit 0.04, 10% missing; "
+                    "nodeKeepIndel against 256 out-group cells, cutoff 2",
+        "gpu_s": t_gpu + t_keep, "join_device_ms": st["total_ms"], "cpu_s": t_cpu, "cpu_cores": nthreads,
+        "identical": bool(np.array_equal(edge, e0) and np.array_equal(state, s0) and np.array_equal(keep, k0))}
+    # C2: binary 10,000 x 512: joinEdgeBitReverse, radiusNeighbor r=4, TransferDisStream vs the true tree
+    words = synth.binary_workload(10_000, 512, 16, 0.03, 0.05, seed=23)
+    (bedge, bstate, bst), t_join = _timed(lambda: L.join_bit(words, None, 1))
+    bmat = np.ascontiguousarray(words.T)
+    wr = np.ones(512)
+    (cnt, idx), t_rad = _timed(lambda: L.radius_bit(bmat, wr, 4))
+    from casphy_b200 import bootstrap as B
+    truth = synth.lineage_clades(10_000, 16, seed=23)
+    est = B.clade_bits(bedge, 10_000, (10_000 + 31) // 32)
+    (ymin, ysize, xmin, xsize), t_td = _timed(lambda: L.transfer_dis(truth, est, 10_000))
+    sub = 3000
+    t0 = time.perf_counter()
+    O.join_bit(words[:sub], None, 1, nthreads)
+    t_cj = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    c0, i0 = O.radius_bit(np.ascontiguousarray(words[:sub].T), wr, 4, nthreads)
+    t_cr = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    O.transfer_dis(truth[:sub], est[:sub], 10_000, nthreads)
+    t_ct = time.perf_counter() - t0
+    res["C2_binary"] = {
+        "workload": "base-editor 10000 cells x 512 sites, depth 16, p_edit 0.03, 5% missing",
+        "joinEdgeBitReverse": {"gpu_s": t_join, "device_ms": bst["total_ms"], "pairs": bst["pair_scores"],
+                               "cpu_sample": f"first {sub} cells", "cpu_s_sample": t_cj},
+        "radiusNeighbor_r4": {"gpu_s": t_rad, "pairs": 10_000 * 10_000, "neighbours": int(cnt.sum()),
+                              "cpu_sample": f"first {sub} cells", "cpu_s_sample": t_cr,
+                              "sample_identical": None},
+        "TransferDisStream_vs_true_tree": {"gpu_s": t_td, "rows_y": int(truth.shape[0]), "rows_x": int(est.shape[0]),
+                                           "words": int(truth.shape[1]),
+                                           "mean_normalised_distance": float(np.mean(ymin / np.maximum(ysize, 1))),
+                                           "cpu_sample": f"first {sub} rows of each", "cpu_s_sample": t_ct},
+        "cpu_cores": nthreads}
+    # the GPU radius lists of the sample rows are those of the full run restricted to j < sub
+    g_c, g_i = L.radius_bit(np.ascontiguousarray(words[:sub].T), wr, 4)
+    res["C2_binary"]["radiusNeighbor_r4"]["sample_identical"] = bool(np.array_equal(g_c, c0) and
+                                                                     np.array_equal(g_i, i0))
+    # C3: DNA 20,000 x 2,000 HKY85 through fasta2bin coding, radiusNeighborDNA at Hamming 20
+    states, _ = synth.hky85_alignment(20_000, 2000, 4.0, [0.3, 0.2, 0.2, 0.3], 0.01, 0.02, seed=13)
+    raw, var = synth.dna_to_fasta2bin(states)
+    lvalid = int(var.sum())
+    (dc, di), t_dna = _timed(lambda: L.radius_dna(raw, lvalid - 20))
+    sub = 4000
+    t0 = time.perf_counter()
+    oc, oi = O.radius_dna(raw[:sub], lvalid - 20, nthreads)
+    t_cd = time.perf_counter() - t0
+    gc, gi = L.radius_dna(raw[:sub], lvalid - 20)
+    res["C3_radiusNeighborDNA"] = {
+        "workload": f"HKY85 20000 x 2000 (kappa 4, pi .3/.2/.2/.3, Exp(0.01) Yule), 2% gaps, fasta2bin coding, "
+                    f"{lvalid} variable columns; shared >= L_valid - 20",
+        "gpu_s": t_dna, "pairs": 20_000 * 20_000, "neighbours": int(dc.sum()),
+        "cpu_sample": f"first {sub} sequences", "cpu_s_sample": t_cd, "cpu_cores": nthreads,
+        "sample_identical": bool(np.array_equal(gc, oc) and np.array_equal(gi, oi))}
+    return res
+
+
+def blopt_c5(L, codes, nstate, edge):
+    """Irreversible edit-model branch lengths on the 200,000-cell join tree."""
+    e = np.asarray(edge, dtype=np.uint32).reshape(-1, 2)
+    t0 = np.full(len(e), 0.05)
+    _, st = L.felsenstein_optimize(e, t0, codes, model="irreversible", rate=1.0, nallele=int(nstate),
+                                   rel_tol=1e-9, max_iter=1000)
+    return {"workload": "irreversible edit model (rate 1, allele frequencies from the tips) on the 200000-cell "
+                        "join tree of the headline workload, 1024 sites; start at t = 0.05",
+            "adjoint_s": st["seconds"], "iterations": st["iterations"], "evaluations": st["evaluations"],
+            "ms_per_evaluation": st["seconds"] * 1e3 / max(st["evaluations"], 1),
+            "loglik_start": st["loglik_start"], "loglik_end": st["loglik_end"],
+            "levels_inside": st["levels_inside"], "levels_outside": st["levels_outside"]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -282,7 +383,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-extras", action="store_true", help="skip the bootstrap and branch-length measurements")
-    ap.add_argument("--only", choices=["bootstrap", "blopt"], default=None,
+    ap.add_argument("--only", choices=["bootstrap", "blopt", "rows"], default=None,
                     help="run one of the extra measurements alone (profiling)")
     ap.add_argument("--no-plain", action="store_true", help="with --only bootstrap: skip the plain runs")
     ap.add_argument("--cells", type=int, default=None,
@@ -303,7 +404,9 @@ def main():
     lib = L.lib()
     torch.cuda.set_device(local)
     if args.only:
-        res = bootstrap_suite(L, plain=not args.no_plain) if args.only == "bootstrap" else blopt_suite(L)
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        res = (bootstrap_suite(L, plain=not args.no_plain) if args.only == "bootstrap" else
+               blopt_suite(L) if args.only == "blopt" else rows_suite(L, os.cpu_count() or 1))
         if rank == 0:
             print(json.dumps({args.only: res}), flush=True)
         return 0
@@ -401,8 +504,11 @@ def main():
                     "d2h_bytes_per_step": int(edge.nbytes + hstate_np.nbytes), "tree_s": e2e_s / e2e_steps},
             "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary()}
     if rank == 0 and world == 1 and args.cells is None and not args.no_extras:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        line["blopt_c5"] = blopt_c5(L, codes, nstate, edge)
         line["bootstrap"] = bootstrap_suite(L)
         line["blopt"] = blopt_suite(L)
+        line["rows"] = rows_suite(L, os.cpu_count() or 1)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

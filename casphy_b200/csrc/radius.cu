@@ -30,14 +30,14 @@ enum { SC_UNIT = 0, SC_FLOAT = 1, SC_DNA = 2 };
 // rows are column-major: word k of row t at col[k * ld + t]
 template <int MODE>
 __global__ void __launch_bounds__(kThreads) k_mask(const u32* __restrict__ col, u32 nwords, u32 ld, u32 ntip,
-                                                   const float* __restrict__ wf, float radius, u32 uradius,
-                                                   u32 maskWords, u32* __restrict__ mask) {
-    extern __shared__ u32 qs[];  // kQ x nwords query words
-    const u32 q0 = blockIdx.y * kQ;
+                                                   u32 qBegin, u32 qEnd, const float* __restrict__ wf, float radius,
+                                                   u32 uradius, u32 maskWords, u32* __restrict__ mask) {
+    extern __shared__ u32 qs[];  // kQ x nwords query words (query rows qBegin..qEnd-1)
+    const u32 q0 = qBegin + blockIdx.y * kQ;
     const u32 t = blockIdx.x * kThreads + threadIdx.x;
     for (u32 i = threadIdx.x; i < kQ * nwords; i += kThreads) {
         const u32 q = i / nwords, k = i % nwords;
-        qs[q * nwords + k] = q0 + q < ntip ? col[(size_t)k * ld + q0 + q] : 0u;
+        qs[q * nwords + k] = q0 + q < qEnd ? col[(size_t)k * ld + q0 + q] : 0u;
     }
     __syncthreads();
     u32 acc[kQ];
@@ -83,7 +83,8 @@ __global__ void __launch_bounds__(kThreads) k_mask(const u32* __restrict__ col, 
         else hit = facc[q] >= radius;
         hit = hit && t < ntip;
         const u32 bal = __ballot_sync(0xFFFFFFFFu, hit);
-        if (lane == 0 && q0 + q < ntip && (t >> 5) < maskWords) mask[(size_t)(q0 + q) * maskWords + (t >> 5)] = bal;
+        if (lane == 0 && q0 + q < qEnd && (t >> 5) < maskWords)
+            mask[(size_t)(q0 + q - qBegin) * maskWords + (t >> 5)] = bal;
     }
 }
 
@@ -250,9 +251,15 @@ static int prep_dna(RadiusInput& in, u32 ntip, u32 nbinRaw, const u32* raw, u32 
     return CASPHY_OK;
 }
 
-static int radius_impl(RadiusInput& in, u32* counts, u32* idx, u64 cap, u64* total) {
-    if (!counts) return CASPHY_EINVAL;
-    const u32 ntip = in.ntip;
+// Lists of the query rows [row0, row1) (counts[0 .. row1-row0) and their
+// concatenated index lists); the whole matrix is [0, ntip).
+static int radius_impl(RadiusInput& in, u32 row0, u32 row1, u32* counts, u32* idx, u64 cap, u64* total) {
+    if (!counts || row0 > row1 || row1 > in.ntip) return CASPHY_EINVAL;
+    const u32 ntip = in.ntip, nq = row1 - row0;
+    if (nq == 0) {
+        if (total) *total = 0;
+        return CASPHY_OK;
+    }
     const u32 maskWords = (ntip + 31) / 32;
     const size_t smem = sizeof(u32) * kQ * in.nwords;
     if (smem > 200 * 1024) {
@@ -263,9 +270,9 @@ static int radius_impl(RadiusInput& in, u32* counts, u32* idx, u64 cap, u64* tot
     cudaStream_t st = 0;
     auto lay = [&](Carve& c) {
         struct B { u32* mask; u32* counts; u64* off; } b;
-        b.mask = c.take<u32>((size_t)ntip * maskWords);
-        b.counts = c.take<u32>(ntip);
-        b.off = c.take<u64>(ntip);
+        b.mask = c.take<u32>((size_t)nq * maskWords);
+        b.counts = c.take<u32>(nq);
+        b.off = c.take<u64>(nq);
         return b;
     };
     // sizes: rows + mask first; index space after counting
@@ -285,26 +292,26 @@ static int radius_impl(RadiusInput& in, u32* counts, u32* idx, u64 cap, u64* tot
     rc = upload_rows(in, c2, &dcol, &dwf, st);
     if (rc) return rc;
     auto L = lay(c2);
-    dim3 grid((ntip + kThreads - 1) / kThreads, (ntip + kQ - 1) / kQ);
+    dim3 grid((ntip + kThreads - 1) / kThreads, (nq + kQ - 1) / kQ);
     void* fn = in.mode == SC_UNIT ? (void*)k_mask<SC_UNIT> : in.mode == SC_DNA ? (void*)k_mask<SC_DNA>
                                                                                   : (void*)k_mask<SC_FLOAT>;
     CASPHY_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (in.mode == SC_UNIT)
-        k_mask<SC_UNIT><<<grid, kThreads, smem, st>>>(dcol, in.nwords, ntip, ntip, dwf, in.radius, in.uradius,
+        k_mask<SC_UNIT><<<grid, kThreads, smem, st>>>(dcol, in.nwords, ntip, ntip, row0, row1, dwf, in.radius, in.uradius,
                                                        maskWords, L.mask);
     else if (in.mode == SC_DNA)
-        k_mask<SC_DNA><<<grid, kThreads, smem, st>>>(dcol, in.nwords, ntip, ntip, dwf, in.radius, in.uradius,
+        k_mask<SC_DNA><<<grid, kThreads, smem, st>>>(dcol, in.nwords, ntip, ntip, row0, row1, dwf, in.radius, in.uradius,
                                                       maskWords, L.mask);
     else
-        k_mask<SC_FLOAT><<<grid, kThreads, smem, st>>>(dcol, in.nwords, ntip, ntip, dwf, in.radius, in.uradius,
+        k_mask<SC_FLOAT><<<grid, kThreads, smem, st>>>(dcol, in.nwords, ntip, ntip, row0, row1, dwf, in.radius, in.uradius,
                                                         maskWords, L.mask);
-    k_count<<<(ntip + 7) / 8, 256, 0, st>>>(L.mask, ntip, maskWords, L.counts);
+    k_count<<<(nq + 7) / 8, 256, 0, st>>>(L.mask, nq, maskWords, L.counts);
     CASPHY_CUDA_TRY(cudaGetLastError());
-    CASPHY_CUDA_TRY(cudaMemcpyAsync(counts, L.counts, sizeof(u32) * ntip, cudaMemcpyDeviceToHost, st));
+    CASPHY_CUDA_TRY(cudaMemcpyAsync(counts, L.counts, sizeof(u32) * nq, cudaMemcpyDeviceToHost, st));
     CASPHY_CUDA_TRY(cudaStreamSynchronize(st));
-    std::vector<u64> off(ntip);
+    std::vector<u64> off(nq);
     u64 tot = 0;
-    for (u32 i = 0; i < ntip; i++) {
+    for (u32 i = 0; i < nq; i++) {
         off[i] = tot;
         tot += counts[i];
     }
@@ -314,8 +321,8 @@ static int radius_impl(RadiusInput& in, u32* counts, u32* idx, u64 cap, u64* tot
     // the index lists get their own buffer: their size is only known now
     u32* didx = nullptr;
     CASPHY_CUDA_TRY(cudaMalloc(&didx, sizeof(u32) * (tot ? tot : 1)));
-    CASPHY_CUDA_TRY(cudaMemcpyAsync(L.off, off.data(), sizeof(u64) * ntip, cudaMemcpyHostToDevice, st));
-    k_expand<<<(ntip + 7) / 8, 256, 0, st>>>(L.mask, ntip, maskWords, L.off, didx);
+    CASPHY_CUDA_TRY(cudaMemcpyAsync(L.off, off.data(), sizeof(u64) * nq, cudaMemcpyHostToDevice, st));
+    k_expand<<<(nq + 7) / 8, 256, 0, st>>>(L.mask, nq, maskWords, L.off, didx);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess && tot) e = cudaMemcpyAsync(idx, didx, sizeof(u32) * tot, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -376,7 +383,18 @@ extern "C" int casphy_radius_bit(uint32_t nrow, uint32_t ntip, const uint32_t* b
     casphy::RadiusInput in;
     rc = casphy::prep_bit(in, nrow, ntip, bmat, weight, radius);
     if (rc) return rc;
-    return casphy::radius_impl(in, counts, idx, idx_cap, total);
+    return casphy::radius_impl(in, 0, ntip, counts, idx, idx_cap, total);
+}
+
+extern "C" int casphy_radius_bit_rows(uint32_t nrow, uint32_t ntip, const uint32_t* bmat, const double* weight,
+                                      int32_t radius, uint32_t row_begin, uint32_t row_end, uint32_t* counts,
+                                      uint32_t* idx, uint64_t idx_cap, uint64_t* total) {
+    int rc = casphy::require_device();
+    if (rc) return rc;
+    casphy::RadiusInput in;
+    rc = casphy::prep_bit(in, nrow, ntip, bmat, weight, radius);
+    if (rc) return rc;
+    return casphy::radius_impl(in, row_begin, row_end, counts, idx, idx_cap, total);
 }
 
 extern "C" int casphy_radius_dna(uint32_t ntip, uint32_t nbinRaw, const uint32_t* raw, uint32_t radius,
@@ -386,7 +404,18 @@ extern "C" int casphy_radius_dna(uint32_t ntip, uint32_t nbinRaw, const uint32_t
     casphy::RadiusInput in;
     rc = casphy::prep_dna(in, ntip, nbinRaw, raw, radius);
     if (rc) return rc;
-    return casphy::radius_impl(in, counts, idx, idx_cap, total);
+    return casphy::radius_impl(in, 0, ntip, counts, idx, idx_cap, total);
+}
+
+extern "C" int casphy_radius_dna_rows(uint32_t ntip, uint32_t nbinRaw, const uint32_t* raw, uint32_t radius,
+                                      uint32_t row_begin, uint32_t row_end, uint32_t* counts, uint32_t* idx,
+                                      uint64_t idx_cap, uint64_t* total) {
+    int rc = casphy::require_device();
+    if (rc) return rc;
+    casphy::RadiusInput in;
+    rc = casphy::prep_dna(in, ntip, nbinRaw, raw, radius);
+    if (rc) return rc;
+    return casphy::radius_impl(in, row_begin, row_end, counts, idx, idx_cap, total);
 }
 
 extern "C" int casphy_try_radius_bit(uint32_t nrow, uint32_t ntip, const uint32_t* bmat, const double* weight,

@@ -89,6 +89,10 @@ def lib():
         L.casphy_radius_bit.argtypes = [u32, u32, _u32p, _f64p, C.c_int32, _u32p, vp, C.c_uint64,
                                         C.POINTER(C.c_uint64)]
         L.casphy_radius_dna.argtypes = [u32, u32, _u32p, u32, _u32p, vp, C.c_uint64, C.POINTER(C.c_uint64)]
+        L.casphy_radius_bit_rows.argtypes = [u32, u32, _u32p, _f64p, C.c_int32, u32, u32, _u32p, vp, C.c_uint64,
+                                             C.POINTER(C.c_uint64)]
+        L.casphy_radius_dna_rows.argtypes = [u32, u32, _u32p, u32, u32, u32, _u32p, vp, C.c_uint64,
+                                             C.POINTER(C.c_uint64)]
         L.casphy_try_radius_bit.argtypes = [u32, u32, _u32p, _f64p, C.c_int32, u32, _u32p, _u32p]
         L.casphy_try_radius_dna.argtypes = [u32, u32, _u32p, u32, u32, _u32p, _u32p]
         L.casphy_transfer_dis.argtypes = [u32, u32, u32, u32, _u32p, _u32p, _u32p, _u32p, _u32p, _u32p]
@@ -158,12 +162,12 @@ def node_keep(node_state, edge, outmat, cutoff, bit=False):
 
 
 def _lists(call, ntip):
-    counts = np.zeros(ntip, dtype=np.uint32)
+    counts = np.zeros(max(ntip, 1), dtype=np.uint32)
     tot = C.c_uint64(0)
     _chk(call(counts, None, 0, C.byref(tot)), "casphy_radius")
     idx = np.zeros(max(tot.value, 1), dtype=np.uint32)
     _chk(call(counts, idx.ctypes.data_as(C.c_void_p), tot.value, C.byref(tot)), "casphy_radius")
-    return counts, idx[: tot.value]
+    return counts[:ntip], idx[: tot.value]
 
 
 def radius_bit(bmat, w, radius):
@@ -179,6 +183,23 @@ def radius_dna(raw, radius):
     raw = _u32(raw)
     ntip, nb = raw.shape
     return _lists(lambda c, i, cap, t: lib().casphy_radius_dna(ntip, nb, raw, int(radius), c, i, cap, t), ntip)
+
+
+def radius_bit_rows(bmat, w, radius, row_begin, row_end):
+    """radiusNeighbor lists of query rows [row_begin, row_end) only."""
+    bmat = _u32(bmat)
+    nrow, ntip = bmat.shape
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    return _lists(lambda c, i, cap, t: lib().casphy_radius_bit_rows(nrow, ntip, bmat, w, int(radius), row_begin,
+                                                                    row_end, c, i, cap, t), row_end - row_begin)
+
+
+def radius_dna_rows(raw, radius, row_begin, row_end):
+    """radiusNeighborDNA lists of query rows [row_begin, row_end) only."""
+    raw = _u32(raw)
+    ntip, nb = raw.shape
+    return _lists(lambda c, i, cap, t: lib().casphy_radius_dna_rows(ntip, nb, raw, int(radius), row_begin, row_end,
+                                                                    c, i, cap, t), row_end - row_begin)
 
 
 def try_radius_bit(bmat, w, radius, qidx):

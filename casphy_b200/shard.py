@@ -4,6 +4,8 @@ per GPU, torch.distributed for the exchange).
 * Bootstrap replicates are independent units: rank k runs replicates
   k, k + world, ...; the per-clade support counts are summed (all-reduce SUM)
   and the per-replicate TransferDisStream rows are gathered.
+* Radius search splits the query rows into contiguous blocks (each row's
+  list depends only on that row); counts and lists are all-gathered.
 * TransferDisStream splits its y rows (cu/TransferDisStream.cu runs y chunks
   on several GPUs the same way, :130-344): every rank takes a block of whole
   8-row groups, so the groups the x-side minimum is formed over stay aligned
@@ -114,3 +116,39 @@ def bootstrap_sharded(compute, words, full_edge, offsets, cells, weights, thresh
             ymin[r] = p[0, i]
             ysize[r] = p[1, i]
     return s.cpu().numpy().astype(np.uint32), ymin, ysize
+
+
+def radius_sharded(compute_rows, nrows, group=None, device=None):
+    """Radius lists over world ranks.  compute_rows(lo, hi) returns (counts,
+    idx) of query rows [lo, hi) (casphy_b200.lib.radius_bit_rows or
+    radius_dna_rows with the matrix bound); every rank returns the full
+    (counts, idx)."""
+    import torch
+    import torch.distributed as dist
+    world, rank = dist.get_world_size(group), dist.get_rank(group)
+    lo, hi = block(nrows, world, rank)
+    counts, idx = compute_rows(lo, hi) if hi > lo else (np.zeros(0, np.uint32), np.zeros(0, np.uint32))
+    n = torch.tensor([len(idx)], dtype=torch.int64)
+    if device is not None:
+        n = n.to(device)
+    sizes = [torch.zeros_like(n) for _ in range(world)]
+    dist.all_gather(sizes, n, group=group)
+    sizes = [int(x.item()) for x in sizes]
+    share = block(nrows, world, 0)[1]
+    c = np.zeros(share, np.int64)
+    c[:hi - lo] = counts
+    i = np.zeros(max(sizes) if sizes else 0, np.int64)
+    i[:len(idx)] = idx
+    tc, ti = torch.from_numpy(c), torch.from_numpy(i)
+    if device is not None:
+        tc, ti = tc.to(device), ti.to(device)
+    pc = [torch.zeros_like(tc) for _ in range(world)]
+    pi = [torch.zeros_like(ti) for _ in range(world)]
+    dist.all_gather(pc, tc, group=group)
+    dist.all_gather(pi, ti, group=group)
+    out_c, out_i = [], []
+    for k in range(world):
+        a, b = block(nrows, world, k)
+        out_c.append(pc[k].cpu().numpy()[:b - a])
+        out_i.append(pi[k].cpu().numpy()[:sizes[k]])
+    return np.concatenate(out_c).astype(np.uint32), np.concatenate(out_i).astype(np.uint32)

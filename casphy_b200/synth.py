@@ -224,3 +224,35 @@ def edit_alignment(ntip: int, nsite: int, rate: float, nallele: int, zipf_s: flo
     codes = (st[:ntip] + 1).astype(np.uint32)
     codes[rng.random(codes.shape) < p_missing] = 0
     return codes, (par, ch, bl)
+
+
+def lineage_clades(ncell: int, depth: int, seed: int):
+    """Clades of the true division tree behind ``lineage_states(ncell, ...,
+    depth, ..., seed)``: for every generation, the sets of sampled cells
+    sharing an ancestor there, without duplicates (unary lineages) and
+    without the trivial sets (one cell, all cells).  Rows are tip bitsets of
+    (ncell + 31) // 32 u32 words over the output row order."""
+    rng = np.random.default_rng(seed)
+    total = 1 << depth
+    leaves = np.sort(rng.choice(total, size=ncell, replace=False)).astype(np.int64)
+    perm = rng.permutation(ncell)
+    leaf_of_row = leaves[perm]
+    ncol = (ncell + 31) // 32
+    seen, rows = set(), []
+    word = np.arange(ncell) // 32
+    bit = (1 << (np.arange(ncell) % 32)).astype(np.uint32)
+    for g in range(1, depth + 1):
+        pref = leaf_of_row >> (depth - g)
+        order = np.argsort(pref, kind="stable")
+        bounds = np.flatnonzero(np.diff(pref[order])) + 1
+        for grp in np.split(order, bounds):
+            if len(grp) <= 1 or len(grp) >= ncell:
+                continue
+            key = grp.tobytes()
+            if key in seen:
+                continue
+            seen.add(key)
+            r = np.zeros(ncol, dtype=np.uint32)
+            np.bitwise_or.at(r, word[grp], bit[grp])
+            rows.append(r)
+    return np.array(rows, dtype=np.uint32).reshape(-1, ncol)

@@ -132,6 +132,15 @@ int casphy_radius_bit(uint32_t nrow, uint32_t ntip, const uint32_t *bmat, const 
  * .bin body (ntip x nbinRaw u32, four 8-bit codes per word). */
 int casphy_radius_dna(uint32_t ntip, uint32_t nbinRaw, const uint32_t *raw, uint32_t radius,
                       uint32_t *counts, uint32_t *idx, uint64_t idx_cap, uint64_t *total);
+/* The lists of query rows [row_begin, row_end) only (counts has row_end -
+ * row_begin entries, idx their concatenated lists): one GPU's share when the
+ * rows are split over several GPUs. */
+int casphy_radius_bit_rows(uint32_t nrow, uint32_t ntip, const uint32_t *bmat, const double *weight,
+                           int32_t radius, uint32_t row_begin, uint32_t row_end, uint32_t *counts,
+                           uint32_t *idx, uint64_t idx_cap, uint64_t *total);
+int casphy_radius_dna_rows(uint32_t ntip, uint32_t nbinRaw, const uint32_t *raw, uint32_t radius,
+                           uint32_t row_begin, uint32_t row_end, uint32_t *counts, uint32_t *idx,
+                           uint64_t idx_cap, uint64_t *total);
 /* tryRadius / tryRadiusDNA (cu/tryRadius.cu:52-189, cu/tryRadiusDNA.cu:76-178)
  * with the query rows given in qidx (the tools draw them with rand()). */
 int casphy_try_radius_bit(uint32_t nrow, uint32_t ntip, const uint32_t *bmat, const double *weight,

@@ -88,3 +88,20 @@ def test_transfer_dis_random(gpu_lib, ny, nx, ntip):
     want = O.transfer_dis(y, x, ntip)
     for g, w_ in zip(got, want):
         assert np.array_equal(g, w_)
+
+
+def test_radius_row_ranges_concatenate_to_full_lists(gpu_lib):
+    from casphy_b200 import synth
+    words = synth.binary_workload(700, 128, 10, 0.05, 0.05, seed=31)
+    bmat = np.ascontiguousarray(words.T)
+    w = np.ones(128)
+    fc, fi = gpu_lib.radius_bit(bmat, w, 3)
+    parts = [gpu_lib.radius_bit_rows(bmat, w, 3, lo, hi) for lo, hi in ((0, 33), (33, 400), (400, 700))]
+    assert np.array_equal(np.concatenate([p[0] for p in parts]), fc)
+    assert np.array_equal(np.concatenate([p[1] for p in parts]), fi)
+    raw, var = synth.dna_to_fasta2bin(synth.hky85_alignment(500, 300, 4.0, [.3, .2, .2, .3], 0.02, 0.02, seed=32)[0])
+    r = int(var.sum()) - 10
+    dc, di = gpu_lib.radius_dna(raw, r)
+    parts = [gpu_lib.radius_dna_rows(raw, r, lo, hi) for lo, hi in ((0, 250), (250, 251), (251, 500))]
+    assert np.array_equal(np.concatenate([p[0] for p in parts]), dc)
+    assert np.array_equal(np.concatenate([p[1] for p in parts]), di)

@@ -49,7 +49,15 @@ def _worker(rank, world, port, q):
         full_edge, _, _ = O.join_bit(words, None, 1)
         off, cells, w = B.make_replicates(160, 64, 5, 40, 160, seed=7)
         bs = shard.bootstrap_sharded(_oracle_bootstrap, words, full_edge, off, cells, w)
-        q.put((rank, td, bs))
+        bmat = np.ascontiguousarray(words.T)
+        fc, fi = O.radius_bit(bmat, np.ones(64), 3)
+        starts = np.concatenate([[0], np.cumsum(fc.astype(np.int64))])
+
+        def rows(lo, hi):  # one rank's share, cut from the oracle's full lists
+            return fc[lo:hi], fi[starts[lo]:starts[hi]]
+
+        rd = shard.radius_sharded(rows, len(fc))
+        q.put((rank, td, bs, rd, (fc, fi)))
     finally:
         dist.destroy_process_group()
 
@@ -76,7 +84,8 @@ def test_two_rank_sharding_matches_one_process():
     full_edge, _, _ = O.join_bit(words, None, 1)
     off, cells, w = B.make_replicates(160, 64, 5, 40, 160, seed=7)
     want_bs = _oracle_bootstrap(words, full_edge, off, cells, w)
-    for _, td, bs in res:
+    for _, td, bs, rd, full in res:
+        assert np.array_equal(rd[0], full[0]) and np.array_equal(rd[1], full[1])
         for a, b in zip(td, want_td):
             assert np.array_equal(a, b)
         assert np.array_equal(bs[0], want_bs["support"])
