@@ -134,7 +134,8 @@ def traffic_from_profile(kernel):
     try:
         with open(path) as f:
             d = json.load(f)
-        return d.get(kernel)
+        v = d.get(kernel)
+        return float(v) if v is not None else None
     except Exception:
         return None
 
