@@ -338,6 +338,15 @@ def rows_suite(L, nthreads):
                                            "mean_normalised_distance": float(np.mean(ymin / np.maximum(ysize, 1))),
                                            "cpu_sample": f"first {sub} rows of each", "cpu_s_sample": t_ct},
         "cpu_cores": nthreads}
+    # a20: parsimony change counts per edge (ancestralBitReverse) on the C2 join tree
+    (pstate, plen), t_par = _timed(lambda: L.ancestral_bit(words, bedge), reps=3)
+    t0 = time.perf_counter()
+    ostate, olen = O.ancestral_bit(words, bedge)
+    t_cpar = time.perf_counter() - t0
+    res["C2_binary"]["ancestralBitReverse"] = {"gpu_s": t_par, "cpu_s": t_cpar, "edges": int(len(plen)),
+                                               "total_changes": int(plen.sum()),
+                                               "identical": bool(np.array_equal(pstate, ostate) and
+                                                                 np.array_equal(plen, olen))}
     # the GPU radius lists of the sample rows are those of the full run restricted to j < sub
     g_c, g_i = L.radius_bit(np.ascontiguousarray(words[:sub].T), wr, 4)
     res["C2_binary"]["radiusNeighbor_r4"]["sample_identical"] = bool(np.array_equal(g_c, c0) and
@@ -362,8 +371,17 @@ def rows_suite(L, nthreads):
 
 
 def blopt_c5(L, codes, nstate, edge):
-    """Irreversible edit-model branch lengths on the 200,000-cell join tree."""
+    """Irreversible edit-model branch lengths on the 200,000-cell join tree, and
+    the reference's parsimony change counts (charAncestralEC) on the same tree."""
     e = np.asarray(edge, dtype=np.uint32).reshape(-1, 2)
+    raw = codes.astype(np.int32) - 1  # .tbmat coding back to -1 missing, 0 unedited, alleles
+    (_, plen), t_par = _timed(lambda: L.ancestral_char(raw, e))
+    import oracle as O
+    t0 = time.perf_counter()
+    _, olen = O.ancestral_char(raw, e)
+    t_cpar = time.perf_counter() - t0
+    par = {"gpu_s": t_par, "cpu_s": t_cpar, "edges": int(len(plen)), "total_changes": int(plen.sum()),
+           "identical": bool(np.array_equal(plen, olen))}
     t0 = np.full(len(e), 0.05)
     _, st = L.felsenstein_optimize(e, t0, codes, model="irreversible", rate=1.0, nallele=int(nstate),
                                    rel_tol=1e-9, max_iter=1000)
@@ -372,7 +390,8 @@ def blopt_c5(L, codes, nstate, edge):
             "adjoint_s": st["seconds"], "iterations": st["iterations"], "evaluations": st["evaluations"],
             "ms_per_evaluation": st["seconds"] * 1e3 / max(st["evaluations"], 1),
             "loglik_start": st["loglik_start"], "loglik_end": st["loglik_end"],
-            "levels_inside": st["levels_inside"], "levels_outside": st["levels_outside"]}
+            "levels_inside": st["levels_inside"], "levels_outside": st["levels_outside"],
+            "charAncestralEC": par}
 
 
 def main():

@@ -103,6 +103,9 @@ def lib():
                                                   C.c_int, u32, C.c_double, C.POINTER(BloptStats)]
         L.casphy_bootstrap_bit.argtypes = [u32, u32, _u32p, _u32p, u32, _u32p, _u32p, _f64p, C.c_int, C.c_double,
                                            _u32p, vp, vp, vp, C.POINTER(BootstrapStats)]
+        _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+        L.casphy_ancestral_bit.argtypes = [u32, u32, u32, _u32p, u32, _u32p, vp, _u32p]
+        L.casphy_ancestral_char.argtypes = [u32, u32, u32, _i32p, u32, _u32p, _u32p, C.c_float, C.c_float, vp, _u32p]
         if hasattr(L, "casphy_join_bit"):
             L.casphy_join_bit.argtypes = [u32, u32, _u32p, _f64p, C.c_int, _u32p, _u32p, C.POINTER(JoinStats)]
             L.casphy_join_bit_dev.argtypes = [u32, u32, vp, _f64p, C.c_int, _u32p, vp, C.POINTER(JoinStats), vp]
@@ -318,3 +321,30 @@ def bootstrap_bit(words, full_edge, offsets, cells, weights, ancestral_type=1, t
     if raw_edges:
         out["raw_edges"] = np.split(raw, np.cumsum(4 * (n - 1))[:-1])
     return out
+
+
+def ancestral_bit(mat, edge, nnode=None):
+    """ancestralBitReverse: (node states nnode x nbin, edge lengths)."""
+    mat = _u32(mat)
+    ntip, nbin = mat.shape
+    edge = _u32(edge).reshape(-1, 2)
+    nnode = int(edge.max()) + 1 - ntip if nnode is None else int(nnode)
+    state = np.zeros((nnode, nbin), np.uint32)
+    ln = np.zeros(len(edge), np.uint32)
+    _chk(lib().casphy_ancestral_bit(ntip, nnode, nbin, mat, len(edge), edge.reshape(-1), state.ctypes.data, ln),
+         "casphy_ancestral_bit")
+    return state, ln
+
+
+def ancestral_char(mat, edge, tip_size=None, min_size=0.0, min_ratio=0.0, nnode=None):
+    """charAncestralEC on int32 states (-1 unknown): (node states, edge lengths)."""
+    mat = np.ascontiguousarray(mat, dtype=np.int32)
+    ntip, nsite = mat.shape
+    edge = _u32(edge).reshape(-1, 2)
+    nnode = int(edge.max()) + 1 - ntip if nnode is None else int(nnode)
+    tips = _u32(np.ones(ntip) if tip_size is None else tip_size)
+    state = np.zeros((nnode, nsite), np.int32)
+    ln = np.zeros(len(edge), np.uint32)
+    _chk(lib().casphy_ancestral_char(ntip, nnode, nsite, mat, len(edge), edge.reshape(-1), tips, float(min_size),
+                                     float(min_ratio), state.ctypes.data, ln), "casphy_ancestral_char")
+    return state, ln

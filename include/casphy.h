@@ -223,6 +223,26 @@ int casphy_felsenstein_optimize(uint32_t ntip, uint32_t nedge, const uint32_t *e
                                 uint32_t max_iter, double rel_tol, casphy_blopt_stats *stats);
 
 /*
+ * Parsimony change counts per edge, the reference's branch lengths
+ * (collapse.infoless / cal.nevo, R/CasPhy_functions.R:804-845).
+ *   edge      nedge x 2 u32 (parent, child), 0-based: tips 0..ntip-1, internal
+ *             nodes ntip..ntip+nnode-1; rows in pre-order (a node's parent edge
+ *             before its own edges, as an ape cladewise edge matrix or .edge2)
+ *   edge_len  nedge u32: changes on each edge row
+ * casphy_ancestral_bit replaces ancestralBitReverse (src/functions.cpp:
+ * 3478-3542): mat is ntip x nbin u32 bit rows, the root must be node ntip,
+ * state_out (optional) nnode x nbin gets the resolved node states.
+ * casphy_ancestral_char replaces charAncestralEC (src/functions.cpp:
+ * 3085-3150): mat is ntip x nsite int32 (-1 unknown), tipSize[ntip] and the
+ * minSize / minRatio rule as there; state_out (optional) nnode x nsite.
+ */
+int casphy_ancestral_bit(uint32_t ntip, uint32_t nnode, uint32_t nbin, const uint32_t *mat,
+                         uint32_t nedge, const uint32_t *edge, uint32_t *state_out, uint32_t *edge_len);
+int casphy_ancestral_char(uint32_t ntip, uint32_t nnode, uint32_t nsite, const int32_t *mat,
+                          uint32_t nedge, const uint32_t *edge, const uint32_t *tipSize, float minSize,
+                          float minRatio, int32_t *state_out, uint32_t *edge_len);
+
+/*
  * Batched bootstrap of the bit join with transfer support.  Replaces running
  * joinEdgeBitReverse, the clade writer and TransferDisStream once per
  * replicate (vignettes/CasPhy.Rmd:255-291, R/bootstrap_functions.R:190-219).

@@ -753,3 +753,113 @@ int oracle_transfer_dis(uint32_t nrow_y, uint32_t nrow_x, uint32_t ncol, uint32_
     row_size(nrow_x, ncol, ntip, x, xsize);
     return ORACLE_OK;
 }
+
+/* ------------------------------------------------------------------------
+ * Parsimony change counts (the reference's branch-length surrogate).
+ * ancestralBitReverse, src/functions.cpp:3478-3542: a bottom-up pass over the
+ * edges in reverse order keeps per internal node a state (AND of the
+ * children), a bistate (AND of the children's bistates; tips 0) and a
+ * conflict mask (bits where a child differs from the AND so far and neither
+ * side is bistate); a child's conflict bits are folded into its state and
+ * bistate when its parent edge is reached.  The root then drops its
+ * conflict and bistate bits.  A pre-order pass resolves every internal
+ * child's bistate bits from its parent ((s & ~bs) | (parent & bs),
+ * calcDesStateBitReverse :3464-3476) and counts the differing bits per edge
+ * (countBitEvo :3005-3015).
+ */
+int oracle_ancestral_bit(uint32_t ntip, uint32_t nnode, uint32_t nbin, const uint32_t *mat,
+                         uint32_t nedge, const uint32_t *edge, uint32_t *state, uint32_t *bis,
+                         uint32_t *len) {
+    if (!mat || !edge || !state || !bis || !len || nnode == 0) return ORACLE_EINVAL;
+    u32 *conf = (u32 *)calloc((size_t)nnode * nbin, sizeof(u32));
+    if (!conf) return ORACLE_ENOMEM;
+    for (size_t i = 0; i < (size_t)nnode * nbin; i++) { state[i] = 0xFFFFFFFFu; bis[i] = 0xFFFFFFFFu; }
+    for (long i = (long)nedge - 1; i >= 0; i--) {
+        const u32 a = edge[2 * i], d = edge[2 * i + 1];
+        if (a < ntip || a >= ntip + nnode || d >= ntip + nnode) { free(conf); return ORACLE_EINVAL; }
+        u32 *sa = state + (size_t)(a - ntip) * nbin, *ba = bis + (size_t)(a - ntip) * nbin;
+        u32 *ca = conf + (size_t)(a - ntip) * nbin;
+        for (u32 j = 0; j < nbin; j++) {
+            u32 s2, bs2;
+            if (d < ntip) {
+                s2 = mat[(size_t)d * nbin + j];
+                bs2 = 0;
+            } else {
+                u32 *sd = state + (size_t)(d - ntip) * nbin, *bd = bis + (size_t)(d - ntip) * nbin;
+                const u32 cd = conf[(size_t)(d - ntip) * nbin + j];
+                sd[j] |= cd;
+                bd[j] |= cd;
+                s2 = sd[j];
+                bs2 = bd[j];
+            }
+            const u32 s1 = sa[j], bs1 = ba[j];
+            sa[j] = s1 & s2;
+            ba[j] &= bs2;
+            ca[j] |= (s1 ^ s2) & ~(bs1 | bs2);
+        }
+    }
+    for (u32 j = 0; j < nbin; j++) state[j] &= ~(conf[j] | bis[j]);
+    for (u32 i = 0; i < nedge; i++) {
+        const u32 a = edge[2 * i], d = edge[2 * i + 1];
+        const u32 *sa = state + (size_t)(a - ntip) * nbin;
+        u32 cnt = 0;
+        if (d < ntip) {
+            for (u32 j = 0; j < nbin; j++) cnt += (u32)__builtin_popcount(sa[j] ^ mat[(size_t)d * nbin + j]);
+        } else {
+            u32 *sd = state + (size_t)(d - ntip) * nbin;
+            const u32 *bd = bis + (size_t)(d - ntip) * nbin;
+            for (u32 j = 0; j < nbin; j++) {
+                sd[j] = (sd[j] & ~bd[j]) | (sa[j] & bd[j]);
+                cnt += (u32)__builtin_popcount(sa[j] ^ sd[j]);
+            }
+        }
+        len[i] = cnt;
+    }
+    free(conf);
+    return ORACLE_OK;
+}
+
+/* charAncestralEC, src/functions.cpp:3085-3150: node sizes and the largest
+ * child size bottom-up; then, over the edges in reverse order, a child that
+ * passes the size rule (minRatio * size >= largest sibling size, or size >=
+ * minSize) sets each unknown (-1) site of its parent to its own value, and a
+ * known site that disagrees with a known child value becomes 0.  Edge
+ * lengths count the sites where both ends are known and differ
+ * (countCharEvo :3074-3082). */
+int oracle_ancestral_char(uint32_t ntip, uint32_t nnode, uint32_t nsite, const int32_t *mat,
+                          uint32_t nedge, const uint32_t *edge, const uint32_t *tipSize,
+                          float minSize, float minRatio, int32_t *state, uint32_t *len) {
+    if (!mat || !edge || !state || !len || !tipSize || nnode == 0) return ORACLE_EINVAL;
+    int32_t *nsz = (int32_t *)calloc(nnode, sizeof(int32_t)), *mx = (int32_t *)calloc(nnode, sizeof(int32_t));
+    if (!nsz || !mx) { free(nsz); free(mx); return ORACLE_ENOMEM; }
+    for (long i = (long)nedge - 1; i >= 0; i--) {
+        const u32 a = edge[2 * i], d = edge[2 * i + 1];
+        if (a < ntip || a >= ntip + nnode || d >= ntip + nnode) { free(nsz); free(mx); return ORACLE_EINVAL; }
+        const int32_t sd = d < ntip ? (int32_t)tipSize[d] : nsz[d - ntip];
+        nsz[a - ntip] += sd;
+        if (mx[a - ntip] < sd) mx[a - ntip] = sd;
+    }
+    for (size_t i = 0; i < (size_t)nnode * nsite; i++) state[i] = -1;
+    for (long i = (long)nedge - 1; i >= 0; i--) {
+        const u32 a = edge[2 * i], d = edge[2 * i + 1];
+        const int32_t sd = d < ntip ? (int32_t)tipSize[d] : nsz[d - ntip];
+        if (!(minRatio * (float)sd >= (float)mx[a - ntip] || (float)sd >= minSize)) continue;
+        int32_t *pa = state + (size_t)(a - ntip) * nsite;
+        const int32_t *pd = d < ntip ? mat + (size_t)d * nsite : state + (size_t)(d - ntip) * nsite;
+        for (u32 j = 0; j < nsite; j++) {
+            if (pa[j] == -1) pa[j] = pd[j];
+            else if (pa[j] != pd[j] && pd[j] != -1) pa[j] = 0;
+        }
+    }
+    for (u32 i = 0; i < nedge; i++) {
+        const u32 a = edge[2 * i], d = edge[2 * i + 1];
+        const int32_t *pa = state + (size_t)(a - ntip) * nsite;
+        const int32_t *pd = d < ntip ? mat + (size_t)d * nsite : state + (size_t)(d - ntip) * nsite;
+        u32 cnt = 0;
+        for (u32 j = 0; j < nsite; j++) cnt += pa[j] >= 0 && pd[j] >= 0 && pa[j] != pd[j];
+        len[i] = cnt;
+    }
+    free(nsz);
+    free(mx);
+    return ORACLE_OK;
+}

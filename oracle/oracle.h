@@ -89,6 +89,20 @@ int oracle_transfer_dis(uint32_t nrow_y, uint32_t nrow_x, uint32_t ncol, uint32_
                         uint32_t *ysize, uint32_t *xmin, uint32_t *xsize,
                         int nthreads);
 
+/* Parsimony change counts per edge.  edge: nedge x 2 (parent, child), 0-based,
+ * tips 0..ntip-1, internal nodes ntip..ntip+nnode-1, rows in pre-order
+ * (parents before children, as an ape edge matrix).
+ * ancestralBitReverse (src/functions.cpp:3478-3542): mat ntip x nbin words;
+ *   state_out, bistate_out nnode x nbin; len_out[nedge].
+ * charAncestralEC (src/functions.cpp:3085-3150): mat ntip x nsite int32
+ *   (-1 unknown); state_out nnode x nsite; len_out[nedge]. */
+int oracle_ancestral_bit(uint32_t ntip, uint32_t nnode, uint32_t nbin, const uint32_t *mat,
+                         uint32_t nedge, const uint32_t *edge, uint32_t *state_out,
+                         uint32_t *bistate_out, uint32_t *len_out);
+int oracle_ancestral_char(uint32_t ntip, uint32_t nnode, uint32_t nsite, const int32_t *mat,
+                          uint32_t nedge, const uint32_t *edge, const uint32_t *tipSize,
+                          float minSize, float minRatio, int32_t *state_out, uint32_t *len_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -159,3 +159,38 @@ def transfer_dis(y, x, ntip, nthreads=0):
     _chk(lib().oracle_transfer_dis(ny, nx, ncol, ntip, y, x, ymin, ysize, xmin, xsize,
                                    nthreads or os.cpu_count()), "transfer_dis")
     return ymin, ysize, xmin, xsize
+
+
+def ancestral_bit(mat, edge, nnode=None):
+    mat = _u32(mat)
+    ntip, nbin = mat.shape
+    edge = _u32(edge).reshape(-1, 2)
+    nnode = int(edge.max()) + 1 - ntip if nnode is None else int(nnode)
+    state = np.zeros((nnode, nbin), np.uint32)
+    bis = np.zeros((nnode, nbin), np.uint32)
+    ln = np.zeros(len(edge), np.uint32)
+    L = lib()
+    _chk(L.oracle_ancestral_bit(C.c_uint32(ntip), C.c_uint32(nnode), C.c_uint32(nbin),
+                                mat.ctypes.data_as(C.c_void_p), C.c_uint32(len(edge)),
+                                np.ascontiguousarray(edge.reshape(-1)).ctypes.data_as(C.c_void_p),
+                                state.ctypes.data_as(C.c_void_p), bis.ctypes.data_as(C.c_void_p),
+                                ln.ctypes.data_as(C.c_void_p)), "ancestral_bit")
+    return state, ln
+
+
+def ancestral_char(mat, edge, tip_size=None, min_size=0.0, min_ratio=0.0, nnode=None):
+    mat = np.ascontiguousarray(mat, dtype=np.int32)
+    ntip, nsite = mat.shape
+    edge = _u32(edge).reshape(-1, 2)
+    nnode = int(edge.max()) + 1 - ntip if nnode is None else int(nnode)
+    tips = _u32(np.ones(ntip) if tip_size is None else tip_size)
+    state = np.zeros((nnode, nsite), np.int32)
+    ln = np.zeros(len(edge), np.uint32)
+    L = lib()
+    _chk(L.oracle_ancestral_char(C.c_uint32(ntip), C.c_uint32(nnode), C.c_uint32(nsite),
+                                 mat.ctypes.data_as(C.c_void_p), C.c_uint32(len(edge)),
+                                 np.ascontiguousarray(edge.reshape(-1)).ctypes.data_as(C.c_void_p),
+                                 tips.ctypes.data_as(C.c_void_p), C.c_float(min_size),
+                                 C.c_float(min_ratio), state.ctypes.data_as(C.c_void_p),
+                                 ln.ctypes.data_as(C.c_void_p)), "ancestral_char")
+    return state, ln
