@@ -261,12 +261,26 @@ def blopt_suite(L):
     _, fd = L.felsenstein_optimize(s_edge, s_t0, s_codes, kappa=4.0, pi=pi, rel_tol=1e-9, max_iter=1000,
                                    gradient="central_diff")
     rel = abs(fd["loglik_end"] - adj["loglik_end"]) / abs(adj["loglik_end"])
+    # algorithmic bytes of one evaluation with gradient, per site: inside
+    # writes a 20 B partial per internal node and reads each child once (20 B
+    # internal, 4 B tip code); outside reads U (16 B), the two children again
+    # and writes U (16 B) for each internal child
+    ntip = codes.shape[0]
+    nint, nsite = ntip - 1, codes.shape[1]
+    per_site = 20 * nint + 2 * (20 * (nint - 1) + 4 * ntip) + 16 * (nint - 1) + 16 * (nint - 1)
+    alg = float(per_site) * nsite
+    hbm, how = peaks()
+    achieved = alg * full["evaluations"] / full["eval_seconds"] / 1e9 if full["eval_seconds"] else 0.0
     return {"workload": "HKY85 (kappa 4, pi .3/.2/.2/.3) 20000 tips x 2000 sites, Yule tree, Exp(mean 0.01) "
                         "branches, 2% gaps; start at t = 0.01; FP32 partials, FP64 sums and L-BFGS step",
             "adjoint_s": full["seconds"], "iterations": full["iterations"], "evaluations": full["evaluations"],
+            "eval_graph_s": full["eval_seconds"],
             "ms_per_evaluation": full["seconds"] * 1e3 / max(full["evaluations"], 1),
             "loglik_start": full["loglik_start"], "loglik_end": full["loglik_end"],
             "fd_evaluations_per_gradient": 2 * len(t0),
+            "roofline": {"kernels": "k_inside_hky + k_outside_hky (evaluation graph)", "bound": "hbm",
+                         "alg_bytes_per_evaluation": alg, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "peak_source": f"{how} hbm_gbs"},
             "small_case": {"workload": "same model, 128 tips x 2000 sites", "adjoint_s": adj["seconds"],
                            "adjoint_evaluations": adj["evaluations"], "adjoint_loglik": adj["loglik_end"],
                            "central_diff_s": fd["seconds"], "central_diff_evaluations": fd["evaluations"],
@@ -388,6 +402,7 @@ def blopt_c5(L, codes, nstate, edge):
     return {"workload": "irreversible edit model (rate 1, allele frequencies from the tips) on the 200000-cell "
                         "join tree of the headline workload, 1024 sites; start at t = 0.05",
             "adjoint_s": st["seconds"], "iterations": st["iterations"], "evaluations": st["evaluations"],
+            "eval_graph_s": st["eval_seconds"],
             "ms_per_evaluation": st["seconds"] * 1e3 / max(st["evaluations"], 1),
             "loglik_start": st["loglik_start"], "loglik_end": st["loglik_end"],
             "levels_inside": st["levels_inside"], "levels_outside": st["levels_outside"],

@@ -51,7 +51,7 @@
 namespace casphy {
 namespace fel {
 
-constexpr u32 kSites = 128;  // sites per block (one thread per site)
+constexpr u32 kSites = 256;  // sites per block (one thread per site)
 constexpr int kWild = 0x7FFF, kNoneA = 0x7FFE;
 constexpr u32 kLbThreads = 512;
 constexpr u32 kMaxHist = 16;
@@ -64,7 +64,21 @@ struct Tree {
     const u32* edgeB;
     const u32* inOrder;   // internal nodes by height
     const u32* outOrder;  // internal nodes by depth
+    const uint4* inInfo;  // per position of inOrder: {node, kidA, kidB, edgeA}
+    const u32* inEdgeB;   // per position of inOrder: edgeB
+    const uint4* outInfo; // per position of outOrder
+    const u32* outEdgeB;
 };
+
+// 2^-e with e the exponent of m (m > 0, normal, not near the top of the
+// range): returned in sc, exactly; false sends the caller to ilogbf/ldexpf.
+__device__ __forceinline__ bool pow2_of(float m, int& e, float& sc) {
+    const int ex = (__float_as_int(m) >> 23) & 0xFF;
+    if (ex < 1 || ex > 253) return false;
+    e = ex - 127;
+    sc = __int_as_float((254 - ex) << 23);
+    return true;
+}
 
 // One chunk of sites [s0, s0 + w); partial buffers have row stride W.
 struct Chunk {
@@ -146,7 +160,16 @@ __device__ __forceinline__ float dot4(float4 a, float4 b) { return a.x * b.x + a
 __device__ __forceinline__ int renorm4(float4& v) {
     const float m = fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w));
     if (!(m > 0.f)) return 0;
-    const int e = ilogbf(m);
+    int e;
+    float sc;
+    if (pow2_of(m, e, sc)) {
+        v.x *= sc;
+        v.y *= sc;
+        v.z *= sc;
+        v.w *= sc;
+        return e;
+    }
+    e = ilogbf(m);
     v.x = ldexpf(v.x, -e);
     v.y = ldexpf(v.y, -e);
     v.z = ldexpf(v.z, -e);
@@ -176,12 +199,13 @@ __device__ __forceinline__ float4 child_hky(const Tree& T, const HkyBuf& B, cons
 __global__ void __launch_bounds__(kSites) k_inside_hky(Tree T, HkyBuf B, Chunk C, u32 off) {
     const u32 s = blockIdx.x * kSites + threadIdx.x;
     if (s >= C.w) return;
-    const u32 v = T.inOrder[off + blockIdx.y], vi = v - T.ntip;
+    const uint4 nf = T.inInfo[off + blockIdx.y];
+    const u32 vi = nf.x - T.ntip, eB = T.inEdgeB[off + blockIdx.y];
     int ea, eb;
-    const float4 la = child_hky(T, B, C, T.kidA[vi], s, &ea);
-    const float4 lb = child_hky(T, B, C, T.kidB[vi], s, &eb);
-    const float4 ma = pmatvec(B.P + 16 * T.edgeA[vi], la);
-    const float4 mb = pmatvec(B.P + 16 * T.edgeB[vi], lb);
+    const float4 la = child_hky(T, B, C, nf.y, s, &ea);
+    const float4 lb = child_hky(T, B, C, nf.z, s, &eb);
+    const float4 ma = pmatvec(B.P + 16 * nf.w, la);
+    const float4 mb = pmatvec(B.P + 16 * eB, lb);
     float4 l = make_float4(ma.x * mb.x, ma.y * mb.y, ma.z * mb.z, ma.w * mb.w);
     const int e = renorm4(l);
     B.L[(size_t)vi * C.W + s] = l;
@@ -208,15 +232,16 @@ __global__ void __launch_bounds__(kSites) k_outside_hky(u32 root, Tree T, HkyBuf
                                                         const double* __restrict__ w, double* gpart) {
     __shared__ double red[kSites / 32];
     const u32 s = blockIdx.x * kSites + threadIdx.x;
-    const u32 v = T.outOrder[off + blockIdx.y], vi = v - T.ntip;
+    const uint4 nf = T.outInfo[off + blockIdx.y];
+    const u32 v = nf.x, vi = v - T.ntip;
     const bool ok = s < C.w;
     const u32 ss = ok ? s : 0;
     float4 u;
     if (v == root) u = make_float4((float)m.pi[0], (float)m.pi[1], (float)m.pi[2], (float)m.pi[3]);
     else u = B.U[(size_t)vi * C.W + ss];
     int e;
-    const u32 ca = T.kidA[vi], cb = T.kidB[vi];
-    const u32 eA = T.edgeA[vi], eB = T.edgeB[vi];
+    const u32 ca = nf.y, cb = nf.z;
+    const u32 eA = nf.w, eB = T.outEdgeB[off + blockIdx.y];
     const float4 la = child_hky(T, B, C, ca, ss, &e);
     const float4 lb = child_hky(T, B, C, cb, ss, &e);
     const float4 ma = pmatvec(B.P + 16 * eA, la), mb = pmatvec(B.P + 16 * eB, lb);
@@ -286,10 +311,11 @@ __global__ void __launch_bounds__(kSites) k_inside_irr(Tree T, IrrBuf B, Chunk C
     const u32 s = blockIdx.x * kSites + threadIdx.x;
     if (s >= C.w) return;
     const u32 gs = C.s0 + s;
-    const u32 v = T.inOrder[off + blockIdx.y], vi = v - T.ntip;
-    const float4 la = child_irr(T, B, C, T.kidA[vi], s);
-    const float4 lb = child_irr(T, B, C, T.kidB[vi], s);
-    const float2 pa = B.p[T.edgeA[vi]], pb = B.p[T.edgeB[vi]];
+    const uint4 nf = T.inInfo[off + blockIdx.y];
+    const u32 vi = nf.x - T.ntip;
+    const float4 la = child_irr(T, B, C, nf.y, s);
+    const float4 lb = child_irr(T, B, C, nf.z, s);
+    const float2 pa = B.p[nf.w], pb = B.p[T.inEdgeB[off + blockIdx.y]];
     const float m0a = la.x + pa.y * (qsum(B, gs, la) - la.x);
     const float m0b = lb.x + pb.y * (qsum(B, gs, lb) - lb.x);
     const int aa = __float_as_int(la.z), ab = __float_as_int(lb.z);
@@ -304,9 +330,15 @@ __global__ void __launch_bounds__(kSites) k_inside_irr(Tree T, IrrBuf B, Chunk C
     int e = 0;
     const float mx = fmaxf(l0, lA);
     if (mx > 0.f) {
-        e = ilogbf(mx);
-        l0 = ldexpf(l0, -e);
-        lA = ldexpf(lA, -e);
+        float sc;
+        if (pow2_of(mx, e, sc)) {
+            l0 *= sc;
+            lA *= sc;
+        } else {
+            e = ilogbf(mx);
+            l0 = ldexpf(l0, -e);
+            lA = ldexpf(lA, -e);
+        }
     }
     e += __float_as_int(la.w) + __float_as_int(lb.w);
     B.L[(size_t)vi * C.W + s] = make_float4(l0, lA, __int_as_float(a), __int_as_float(e));
@@ -329,7 +361,8 @@ __global__ void __launch_bounds__(kSites) k_outside_irr(u32 root, Tree T, IrrBuf
                                                         const double* __restrict__ w, double* gpart) {
     __shared__ double red[kSites / 32];
     const u32 s = blockIdx.x * kSites + threadIdx.x;
-    const u32 v = T.outOrder[off + blockIdx.y], vi = v - T.ntip;
+    const uint4 nf = T.outInfo[off + blockIdx.y];
+    const u32 v = nf.x, vi = v - T.ntip;
     const bool ok = s < C.w;
     const u32 ss = ok ? s : 0, gs = C.s0 + ss;
     float U0 = 1.f, X = 0.f, Y = 0.f;
@@ -341,8 +374,8 @@ __global__ void __launch_bounds__(kSites) k_outside_irr(u32 root, Tree T, IrrBuf
         Y = u.z;
         aY = __float_as_int(u.w);
     }
-    const u32 kids[2] = {T.kidA[vi], T.kidB[vi]};
-    const u32 eds[2] = {T.edgeA[vi], T.edgeB[vi]};
+    const u32 kids[2] = {nf.y, nf.z};
+    const u32 eds[2] = {nf.w, T.outEdgeB[off + blockIdx.y]};
     float4 l[2];
     float m0[2], qs[2];
     float2 pp[2];
@@ -383,10 +416,18 @@ __global__ void __launch_bounds__(kSites) k_outside_irr(u32 root, Tree T, IrrBuf
             float u0 = R0 * pp[c].x, x = pp[c].y * R0 + RX, y = RY;
             const float mx = fmaxf(u0, fmaxf(x, y));
             if (mx > 0.f) {
-                const int ee = ilogbf(mx);
-                u0 = ldexpf(u0, -ee);
-                x = ldexpf(x, -ee);
-                y = ldexpf(y, -ee);
+                int ee;
+                float sc;
+                if (pow2_of(mx, ee, sc)) {
+                    u0 *= sc;
+                    x *= sc;
+                    y *= sc;
+                } else {
+                    ee = ilogbf(mx);
+                    u0 = ldexpf(u0, -ee);
+                    x = ldexpf(x, -ee);
+                    y = ldexpf(y, -ee);
+                }
             }
             B.U[(size_t)(kids[c] - T.ntip) * C.W + s] = make_float4(u0, x, y, __int_as_float(aR));
         }
@@ -757,6 +798,8 @@ struct FelProblem {
         if (gLL) cudaGraphExecDestroy(gLL);
         if (e0) cudaEventDestroy(e0);
         if (e1) cudaEventDestroy(e1);
+        if (g0) cudaEventDestroy(g0);
+        if (g1) cudaEventDestroy(g1);
         if (st) cudaStreamDestroy(st);
     }
 
@@ -819,11 +862,17 @@ struct FelProblem {
 
     // log L (and d log L / d t in `grad`) at the branch lengths in `t`
     int eval(bool withGrad, double* llOut) {
+        CASPHY_CUDA_TRY(cudaEventRecord(g0, st));
         CASPHY_CUDA_TRY(cudaGraphLaunch(withGrad ? gFull : gLL, st));
+        CASPHY_CUDA_TRY(cudaEventRecord(g1, st));
         CASPHY_CUDA_TRY(cudaMemcpyAsync(llOut, ll, sizeof(double), cudaMemcpyDeviceToHost, st));
         CASPHY_CUDA_TRY(cudaStreamSynchronize(st));
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, g0, g1) == cudaSuccess) graphMs += ms;
         return CASPHY_OK;
     }
+    cudaEvent_t g0 = nullptr, g1 = nullptr;
+    double graphMs = 0;
 };
 
 static int setup_problem(FelProblem& F, DeviceScope& ds, u32 ntip, u32 nedge, const u32* edge, const double* brlen,
@@ -897,7 +946,8 @@ static int setup_problem(FelProblem& F, DeviceScope& ds, u32 ntip, u32 nedge, co
     const u32 nCTA = (u32)std::max(1, nsm), Mr = hist + 1;
     if (hist >= kMaxHist) return CASPHY_EINVAL;
     struct Bufs {
-        u32 *kidA, *kidB, *edgeA, *edgeB, *inO, *outO, *codes, *flags;
+        u32 *kidA, *kidB, *edgeA, *edgeB, *inO, *outO, *codes, *flags, *inEB, *outEB;
+        uint4 *inInfo, *outInfo;
         double *t, *w, *grad, *gpart, *part, *ll;
         double *x, *g, *d, *xn, *S, *Y, *rho, *gam, *sc, *lpart;
         float *P, *dP, *q;
@@ -915,6 +965,10 @@ static int setup_problem(FelProblem& F, DeviceScope& ds, u32 ntip, u32 nedge, co
         b.edgeB = c.take<u32>(nint);
         b.inO = c.take<u32>(nint);
         b.outO = c.take<u32>(nint);
+        b.inInfo = c.take<uint4>(nint);
+        b.outInfo = c.take<uint4>(nint);
+        b.inEB = c.take<u32>(nint);
+        b.outEB = c.take<u32>(nint);
         b.codes = c.take<u32>((size_t)ntip * nsite);
         b.flags = c.take<u32>(16 * nCTA);
         b.err = c.take<int>(1);
@@ -954,6 +1008,8 @@ static int setup_problem(FelProblem& F, DeviceScope& ds, u32 ntip, u32 nedge, co
     CASPHY_CUDA_TRY(cudaStreamCreateWithFlags(&F.st, cudaStreamNonBlocking));
     CASPHY_CUDA_TRY(cudaEventCreate(&F.e0));
     CASPHY_CUDA_TRY(cudaEventCreate(&F.e1));
+    CASPHY_CUDA_TRY(cudaEventCreate(&F.g0));
+    CASPHY_CUDA_TRY(cudaEventCreate(&F.g1));
     cudaStream_t st = F.st;
     auto up = [&](void* d, const void* h, size_t n) { return cudaMemcpyAsync(d, h, n, cudaMemcpyHostToDevice, st); };
     CASPHY_CUDA_TRY(up(L.kidA, F.th.kidA.data(), 4ull * nint));
@@ -962,6 +1018,21 @@ static int setup_problem(FelProblem& F, DeviceScope& ds, u32 ntip, u32 nedge, co
     CASPHY_CUDA_TRY(up(L.edgeB, F.th.edgeB.data(), 4ull * nint));
     CASPHY_CUDA_TRY(up(L.inO, F.th.inOrder.data(), 4ull * F.th.inOrder.size()));
     CASPHY_CUDA_TRY(up(L.outO, F.th.outOrder.data(), 4ull * F.th.outOrder.size()));
+    // node, children and edges per level position, so a block finds its node's
+    // whole neighbourhood with one dependent load
+    std::vector<uint4> inInfo(nint), outInfo(nint);
+    std::vector<u32> inEB(nint), outEB(nint);
+    for (u32 i = 0; i < nint; i++) {
+        const u32 a = F.th.inOrder[i] - ntip, b = F.th.outOrder[i] - ntip;
+        inInfo[i] = make_uint4(F.th.inOrder[i], F.th.kidA[a], F.th.kidB[a], F.th.edgeA[a]);
+        inEB[i] = F.th.edgeB[a];
+        outInfo[i] = make_uint4(F.th.outOrder[i], F.th.kidA[b], F.th.kidB[b], F.th.edgeA[b]);
+        outEB[i] = F.th.edgeB[b];
+    }
+    CASPHY_CUDA_TRY(up(L.inInfo, inInfo.data(), sizeof(uint4) * nint));
+    CASPHY_CUDA_TRY(up(L.outInfo, outInfo.data(), sizeof(uint4) * nint));
+    CASPHY_CUDA_TRY(up(L.inEB, inEB.data(), 4ull * nint));
+    CASPHY_CUDA_TRY(up(L.outEB, outEB.data(), 4ull * nint));
     CASPHY_CUDA_TRY(up(L.codes, codes, 4ull * ntip * nsite));
     CASPHY_CUDA_TRY(up(L.t, brlen, 8ull * nedge));
     std::vector<double> wv(nsite, 1.0);
@@ -990,7 +1061,7 @@ static int setup_problem(FelProblem& F, DeviceScope& ds, u32 ntip, u32 nedge, co
         }
         CASPHY_CUDA_TRY(up(L.q, q.data(), 4 * q.size()));
     }
-    F.T = Tree{ntip, L.kidA, L.kidB, L.edgeA, L.edgeB, L.inO, L.outO};
+    F.T = Tree{ntip, L.kidA, L.kidB, L.edgeA, L.edgeB, L.inO, L.outO, L.inInfo, L.inEB, L.outInfo, L.outEB};
     F.t = L.t;
     F.w = L.w;
     F.grad = L.grad;
@@ -1017,9 +1088,12 @@ static int lb_coop(FelProblem& F, const void* fn, void** args) {
     return CASPHY_OK;
 }
 
-static int lb_check_err(FelProblem& F) {
+// Reads `n` doubles from the device scalars at `src` together with the grid
+// barrier's error flag, with one synchronisation.
+static int lb_read(FelProblem& F, const double* src, double* dst, size_t n) {
     int err = 0;
     CASPHY_CUDA_TRY(cudaMemcpyAsync(&err, F.lb.err, sizeof(int), cudaMemcpyDeviceToHost, F.st));
+    CASPHY_CUDA_TRY(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyDeviceToHost, F.st));
     CASPHY_CUDA_TRY(cudaStreamSynchronize(F.st));
     if (err) {
         casphy_set_last_error_msg("felsenstein: a grid barrier of the L-BFGS step timed out");
@@ -1105,16 +1179,15 @@ extern "C" int casphy_felsenstein_optimize(uint32_t ntip, uint32_t nedge, const 
     k_lb_grad0<<<nb, 256, 0, F.st>>>(a);
     st.loglik_start = ll;
     double f = -ll;
-    u32 first = 0, count = 0;
+    u32 first = 0, count = 0, quiet = 0;
+    const u32 kQuiet = 5;
     for (u32 it = 0; it < max_iter; it++) {
         u32 cnt = count;
         double sc[2] = {0, 0};
         for (int attempt = 0; attempt < 2; attempt++) {
             void* args[] = {&a, &first, &cnt};
             if ((rc = lb_coop(F, (const void*)k_lb_dir, args))) return rc;
-            if ((rc = lb_check_err(F))) return rc;
-            CASPHY_CUDA_TRY(cudaMemcpyAsync(sc, a.sc + SC_GD, sizeof(sc), cudaMemcpyDeviceToHost, F.st));
-            CASPHY_CUDA_TRY(cudaStreamSynchronize(F.st));
+            if ((rc = lb_read(F, a.sc + SC_GD, sc, 2))) return rc;
             if (sc[0] < 0 || cnt == 0) break;
             cnt = 0;  // not a descent direction: restart from steepest descent
         }
@@ -1145,10 +1218,8 @@ extern "C" int casphy_felsenstein_optimize(uint32_t ntip, uint32_t nedge, const 
         u32 slot = (first + count) % a.Mr;
         void* args[] = {&a, &slot};
         if ((rc = lb_coop(F, (const void*)k_lb_accept, args))) return rc;
-        if ((rc = lb_check_err(F))) return rc;
         double sy = 0;
-        CASPHY_CUDA_TRY(cudaMemcpyAsync(&sy, a.sc + SC_SY, sizeof(double), cudaMemcpyDeviceToHost, F.st));
-        CASPHY_CUDA_TRY(cudaStreamSynchronize(F.st));
+        if ((rc = lb_read(F, a.sc + SC_SY, &sy, 1))) return rc;
         st.iterations++;
         if (sy > 1e-12) {
             if (count < M) count++;
@@ -1159,7 +1230,10 @@ extern "C" int casphy_felsenstein_optimize(uint32_t ntip, uint32_t nedge, const 
             std::fprintf(stderr, "blopt it %u f %.10f df %.3e gd %.3e step %.3e hist %u sy %.3e\n", it, fn, fn - f, gd,
                          step, count, sy);
         f = fn;
-        if (rel <= rel_tol) break;
+        // converged when log L has changed by at most rel_tol (relative) in
+        // each of the last kQuiet steps: one short step alone does not stop
+        quiet = rel <= rel_tol ? quiet + 1 : 0;
+        if (quiet >= kQuiet) break;
     }
     CASPHY_CUDA_TRY(cudaEventRecord(F.e1, F.st));
     CASPHY_CUDA_TRY(cudaEventSynchronize(F.e1));
@@ -1175,6 +1249,7 @@ extern "C" int casphy_felsenstein_optimize(uint32_t ntip, uint32_t nedge, const 
     st.levels_inside = (u32)F.th.inOff.size() - 1;
     st.levels_outside = (u32)F.th.outOff.size() - 1;
     st.launches_per_eval = adj ? F.launchesFull : F.launchesLL;
+    st.eval_seconds = F.graphMs / 1e3;
     if (stats) *stats = st;
     return CASPHY_OK;
 }

@@ -41,7 +41,7 @@ class BloptStats(C.Structure):
     _fields_ = [("iterations", C.c_uint32), ("evaluations", C.c_uint32), ("site_chunks", C.c_uint32),
                 ("levels_inside", C.c_uint32), ("levels_outside", C.c_uint32), ("reserved", C.c_uint32),
                 ("loglik_start", C.c_double), ("loglik_end", C.c_double), ("seconds", C.c_double),
-                ("launches_per_eval", C.c_uint64)]
+                ("launches_per_eval", C.c_uint64), ("eval_seconds", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

@@ -206,6 +206,7 @@ typedef struct {
     double loglik_start, loglik_end;
     double seconds;             /* device time of the whole optimisation */
     uint64_t launches_per_eval; /* kernels in one evaluation graph */
+    double eval_seconds;        /* device time inside the evaluation graphs */
 } casphy_blopt_stats;
 
 /* log L (FP32 partials with per-site power-of-two scaling, FP64 site sums) and,
@@ -215,7 +216,8 @@ int casphy_felsenstein_loglik(uint32_t ntip, uint32_t nedge, const uint32_t *edg
                               const double *site_weights, const casphy_felsenstein_model *model,
                               double *loglik, double *grad);
 /* L-BFGS over log branch lengths (FP64 step on the device) until the relative
- * change of log L in one step is <= rel_tol or max_iter steps; brlen is
+ * change of log L is <= rel_tol in 5 consecutive steps, no descent step is
+ * found, or max_iter steps; brlen is
  * updated in place (clamped to [1e-8, 10]). */
 int casphy_felsenstein_optimize(uint32_t ntip, uint32_t nedge, const uint32_t *edge, double *brlen,
                                 uint32_t nsite, const uint32_t *tip_codes, const double *site_weights,
