@@ -381,6 +381,16 @@ def rows_suite(L, nthreads):
         "gpu_s": t_dna, "pairs": 20_000 * 20_000, "neighbours": int(dc.sum()),
         "cpu_sample": f"first {sub} sequences", "cpu_s_sample": t_cd, "cpu_cores": nthreads,
         "sample_identical": bool(np.array_equal(gc, oc) and np.array_equal(gi, oi))}
+    # tipMerge on 140,000 tips' clustered neighbour lists (avg 18 per row)
+    counts, nidx = synth.neighbour_lists(140_000, 4)
+    mem, t_tm = _timed(lambda: L.tip_merge(counts, nidx, 0.4))
+    t0 = time.perf_counter()
+    omem = O.tip_merge(counts, nidx, 0.4)
+    t_ctm = time.perf_counter() - t0
+    res["tipMerge"] = {"workload": "140000 tips, clustered symmetric neighbour lists (synth.neighbour_lists, "
+                                   "seed 4, mean 18 per row), pShared 0.4",
+                       "gpu_s": t_tm, "cpu_s": t_ctm, "categories": int(mem.max()) + 1,
+                       "identical": bool(np.array_equal(mem, omem))}
     return res
 
 

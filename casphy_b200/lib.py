@@ -106,6 +106,7 @@ def lib():
         _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
         L.casphy_ancestral_bit.argtypes = [u32, u32, u32, _u32p, u32, _u32p, vp, _u32p]
         L.casphy_ancestral_char.argtypes = [u32, u32, u32, _i32p, u32, _u32p, _u32p, C.c_float, C.c_float, vp, _u32p]
+        L.casphy_tip_merge.argtypes = [u32, _u32p, vp, C.c_double, _i32p]
         if hasattr(L, "casphy_join_bit"):
             L.casphy_join_bit.argtypes = [u32, u32, _u32p, _f64p, C.c_int, _u32p, _u32p, C.POINTER(JoinStats)]
             L.casphy_join_bit_dev.argtypes = [u32, u32, vp, _f64p, C.c_int, _u32p, vp, C.POINTER(JoinStats), vp]
@@ -348,3 +349,13 @@ def ancestral_char(mat, edge, tip_size=None, min_size=0.0, min_ratio=0.0, nnode=
     _chk(lib().casphy_ancestral_char(ntip, nnode, nsite, mat, len(edge), edge.reshape(-1), tips, float(min_size),
                                      float(min_ratio), state.ctypes.data, ln), "casphy_ancestral_char")
     return state, ln
+
+
+def tip_merge(counts, idx, pshared):
+    """tipMerge: .member categories from radius lists (counts, concatenated idx)."""
+    counts = _u32(counts)
+    idx = _u32(idx)
+    member = np.zeros(max(len(counts), 1), np.int32)
+    _chk(lib().casphy_tip_merge(len(counts), counts, idx.ctypes.data if idx.size else None, float(pshared), member),
+         "casphy_tip_merge")
+    return member[: len(counts)]

@@ -256,3 +256,38 @@ def lineage_clades(ncell: int, depth: int, seed: int):
             np.bitwise_or.at(r, word[grp], bit[grp])
             rows.append(r)
     return np.array(rows, dtype=np.uint32).reshape(-1, ncol)
+
+
+def neighbour_lists(ntip, seed):
+    """Symmetric, ascending neighbour lists: tips in random clusters of 3-40,
+    pairs inside a cluster linked with probability 0.6, each tip linked to one
+    random tip elsewhere, and half the tips listing themselves (a radius list
+    holds its own row when the row's self score reaches the radius).
+    Returns (counts u32[ntip], concatenated idx u32)."""
+    rng = np.random.default_rng(seed)
+    perm = rng.permutation(ntip)
+    a, b = [], []
+    pos = 0
+    while pos < ntip:
+        size = int(rng.integers(3, 41))
+        members = perm[pos:pos + size]
+        pos += size
+        m = len(members)
+        if m > 1:
+            iu, ju = np.triu_indices(m, 1)
+            keep = rng.random(len(iu)) < 0.6
+            a.append(members[iu[keep]])
+            b.append(members[ju[keep]])
+    x = rng.integers(0, ntip, ntip)
+    a.append(np.arange(ntip))
+    b.append(x)
+    a, b = np.concatenate(a), np.concatenate(b)
+    ok = a != b
+    a, b = a[ok], b[ok]
+    selfs = np.flatnonzero(rng.random(ntip) < 0.5)
+    rows = np.concatenate([a, b, selfs])
+    cols = np.concatenate([b, a, selfs])
+    key = np.unique(rows.astype(np.int64) * ntip + cols)
+    rows, cols = key // ntip, key % ntip
+    counts = np.bincount(rows, minlength=ntip).astype(np.uint32)
+    return counts, cols.astype(np.uint32)

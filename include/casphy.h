@@ -225,6 +225,17 @@ int casphy_felsenstein_optimize(uint32_t ntip, uint32_t nedge, const uint32_t *e
                                 uint32_t max_iter, double rel_tol, casphy_blopt_stats *stats);
 
 /*
+ * tipMerge (cu/tipMerge.cu:130-461): categories of tips whose neighbour lists
+ * overlap.  counts[ntip] and idx (the concatenated ascending lists) are the
+ * .nNeighbor body and the .idx file of radiusNeighbor(DNA); member[ntip]
+ * receives the .member values.  A list longer than 1048576 entries gives
+ * CASPHY_ERANGE with the reference's message in casphy_last_error() (the
+ * reference then writes no .member file).
+ */
+int casphy_tip_merge(uint32_t ntip, const uint32_t *counts, const uint32_t *idx, double pShared,
+                     int32_t *member);
+
+/*
  * Parsimony change counts per edge, the reference's branch lengths
  * (collapse.infoless / cal.nevo, R/CasPhy_functions.R:804-845).
  *   edge      nedge x 2 u32 (parent, child), 0-based: tips 0..ntip-1, internal

@@ -863,3 +863,103 @@ int oracle_ancestral_char(uint32_t ntip, uint32_t nnode, uint32_t nsite, const i
     free(mx);
     return ORACLE_OK;
 }
+
+/* ------------------------------------------------------------------------
+ * tipMerge (cu/tipMerge.cu:130-461).  Rows are visited in chunks of 131072
+ * candidate columns (CACHEMAX): for chunk [c0, c1) every row j < c1, in
+ * increasing order, takes the neighbours k of its list with max(c0, j+1) <=
+ * k < c1, keeps those that pass the reference's filter (:366-370: the root
+ * of j's category against transitionRoot(transition, k), k used as a
+ * category index), counts |N(j) n N(k)| for each (sharedIdxKernel :26-128,
+ * an intersection of the two ascending lists) and then, in list order,
+ * merges categories when the count exceeds pShared times either list's
+ * length (:403-425).  Untouched rows get new categories in row order
+ * (:446-456). */
+static int tm_root(const int *transition, int idx) {
+    if (idx == -1) return -1;
+    int r = idx;
+    while (transition[r] != r && transition[r] != -1) r = transition[r];
+    return r;
+}
+
+static u32 tm_shared(const u32 *a, u32 na, const u32 *b, u32 nb) {
+    u32 i = 0, j = 0, n = 0;
+    while (i < na && j < nb) {
+        if (a[i] < b[j]) i++;
+        else if (a[i] > b[j]) j++;
+        else { n++; i++; j++; }
+    }
+    return n;
+}
+
+int oracle_tip_merge(uint32_t ntip, const uint32_t *counts, const uint32_t *idx, double pShared,
+                     int32_t *member) {
+    if (!counts || !member || ntip == 0) return ORACLE_EINVAL;
+    const u32 kCache = 1024u * 128u, kMaxNeighbor = 1024u * 1024u;
+    u64 *off = (u64 *)malloc(sizeof(u64) * (ntip + 1));
+    u32 *so = (u32 *)malloc(sizeof(u32) * ntip);
+    int *tr = (int *)malloc(sizeof(int) * ntip);
+    u32 *run = (u32 *)malloc(sizeof(u32) * (ntip ? ntip : 1));
+    u32 *sh = (u32 *)malloc(sizeof(u32) * (ntip ? ntip : 1));
+    if (!off || !so || !tr || !run || !sh) { free(off); free(so); free(tr); free(run); free(sh); return ORACLE_ENOMEM; }
+    off[0] = 0;
+    int st = ORACLE_OK;
+    for (u32 i = 0; i < ntip; i++) {
+        if (counts[i] > kMaxNeighbor) { st = ORACLE_ERANGE; goto done; }
+        off[i + 1] = off[i] + counts[i];
+    }
+    for (u32 i = 0; i < ntip; i++) {
+        u32 j = 0;
+        while (j < counts[i] && idx[off[i] + j] <= i) j++;
+        so[i] = j;
+        member[i] = -1;
+        tr[i] = -1;
+    }
+    int ncat = 0;
+    for (u32 c0 = 0; c0 < ntip; c0 += kCache) {
+        const u32 c1 = c0 + kCache < ntip ? c0 + kCache : ntip;
+        for (u32 j = 0; j < c1; j++) {
+            int root1 = member[j];
+            if (root1 != -1) root1 = tm_root(tr, root1);
+            u32 nrun = 0;
+            const u32 *lj = idx + off[j];
+            for (u32 k = so[j]; k < counts[j]; k++) {
+                const u32 t = lj[k];
+                if (t >= c1) { so[j] = k; break; }
+                if (t >= c0 && (root1 == -1 || root1 != tm_root(tr, (int)t))) run[nrun++] = t;
+            }
+            if (!nrun) continue;
+            for (u32 k = 0; k < nrun; k++) sh[k] = tm_shared(lj, counts[j], idx + off[run[k]], counts[run[k]]);
+            for (u32 k = 0; k < nrun; k++) {
+                const u32 t = run[k];
+                if ((double)sh[k] > counts[j] * pShared || (double)sh[k] > counts[t] * pShared) {
+                    const int root2 = tm_root(tr, member[t]);
+                    if (root1 == -1) {
+                        if (root2 == -1) {
+                            root1 = ncat;
+                            tr[ncat] = ncat;
+                            member[j] = ncat;
+                            member[t] = ncat;
+                            ncat++;
+                        } else {
+                            root1 = root2;
+                            member[j] = root2;
+                        }
+                    } else {
+                        if (root2 == -1) {
+                            member[t] = root1;
+                        } else {
+                            tr[root1] = root2;
+                            member[j] = root2;
+                            root1 = root2;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    for (u32 i = 0; i < ntip; i++) member[i] = member[i] == -1 ? ncat++ : tm_root(tr, member[i]);
+done:
+    free(off); free(so); free(tr); free(run); free(sh);
+    return st;
+}

@@ -103,6 +103,13 @@ int oracle_ancestral_char(uint32_t ntip, uint32_t nnode, uint32_t nsite, const i
                           uint32_t nedge, const uint32_t *edge, const uint32_t *tipSize,
                           float minSize, float minRatio, int32_t *state_out, uint32_t *len_out);
 
+/* tipMerge (cu/tipMerge.cu:130-461): counts[ntip] and the concatenated
+ * ascending neighbour lists idx (the .nNeighbor body and .idx); member_out
+ * gets the .member values.  Returns ORACLE_ERANGE when a list is longer than
+ * 1048576 (the reference prints a message and writes nothing). */
+int oracle_tip_merge(uint32_t ntip, const uint32_t *counts, const uint32_t *idx, double pShared,
+                     int32_t *member_out);
+
 #ifdef __cplusplus
 }
 #endif

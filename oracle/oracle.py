@@ -194,3 +194,13 @@ def ancestral_char(mat, edge, tip_size=None, min_size=0.0, min_ratio=0.0, nnode=
                                  C.c_float(min_ratio), state.ctypes.data_as(C.c_void_p),
                                  ln.ctypes.data_as(C.c_void_p)), "ancestral_char")
     return state, ln
+
+
+def tip_merge(counts, idx, pshared):
+    counts = _u32(counts)
+    idx = _u32(idx)
+    member = np.zeros(max(len(counts), 1), np.int32)
+    _chk(lib().oracle_tip_merge(C.c_uint32(len(counts)), counts.ctypes.data_as(C.c_void_p),
+                                idx.ctypes.data_as(C.c_void_p), C.c_double(pshared),
+                                member.ctypes.data_as(C.c_void_p)), "tip_merge")
+    return member[: len(counts)]
