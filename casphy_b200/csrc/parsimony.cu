@@ -1,7 +1,9 @@
-// Parsimony change counts per edge on B200: the reference's branch-length
-// surrogate (ancestralBitReverse and charAncestralEC, src/functions.cpp:
-// 3478-3542 and 3085-3150, called by collapse.infoless / cal.nevo,
-// R/CasPhy_functions.R:804-845).
+// Tree passes of the reference's CPU helpers on B200: parsimony change counts
+// per edge, the reference's branch-length surrogate (ancestralBitReverse and
+// charAncestralEC, src/functions.cpp:3478-3542 and 3085-3150, called by
+// collapse.infoless / cal.nevo, R/CasPhy_functions.R:804-845), and the clade
+// rows of nodeDesBig (src/functions.cpp:1277-1366), the TransferDisStream
+// input that phy2clade writes (R/bootstrap_functions.R:1-32).
 //
 // Both are a bottom-up pass followed by a per-edge count.  The reference runs
 // the bottom-up pass over the edge rows in reverse order, so for every
@@ -133,6 +135,22 @@ __global__ void k_len_char(u32 ntip, u32 nedge, u32 nsite, const u32* __restrict
         for (u32 k = 0; k < blockDim.x / 32; k++) t += red[k];
         len[e] = t;
     }
+}
+
+// clade rows, one height level: thread per (node, word); a node's row is the
+// OR of its tip children's bits and its internal children's rows; rows live
+// at their output positions (rowOf), the root in the extra last row
+__global__ void k_clade(Tree T, u32 off, u32 cnt, u32 nbin, const u32* __restrict__ rowOf, u32* rows) {
+    const u64 id = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= (u64)cnt * nbin) return;
+    const u32 v = T.order[off + (u32)(id / nbin)], i = v - T.ntip, w = (u32)(id % nbin);
+    u32 acc = 0;
+    for (u32 k = T.kidOff[i]; k < T.kidOff[i + 1]; k++) {
+        const u32 d = T.kid[k];
+        if (d < T.ntip) acc |= (d >> 5) == w ? 1u << (d & 31) : 0u;
+        else acc |= rows[(size_t)rowOf[d - T.ntip] * nbin + w];
+    }
+    rows[(size_t)rowOf[i] * nbin + w] = acc;
 }
 
 }  // namespace pars
@@ -383,6 +401,68 @@ extern "C" int casphy_ancestral_char(uint32_t ntip, uint32_t nnode, uint32_t nsi
     CASPHY_CUDA_TRY(cudaMemcpyAsync(edge_len, L.len, 4ull * nedge, cudaMemcpyDeviceToHost, st));
     if (state_out)
         CASPHY_CUDA_TRY(cudaMemcpyAsync(state_out, L.state, 4ull * nnode * nsite, cudaMemcpyDeviceToHost, st));
+    CASPHY_CUDA_TRY(cudaStreamSynchronize(st));
+    return CASPHY_OK;
+}
+
+extern "C" int casphy_node_des(uint32_t ntip, uint32_t nnode, uint32_t nedge, const uint32_t* edge,
+                               uint32_t* rows_out, int32_t* sizes_out) {
+    using namespace casphy;
+    int rc = require_device();
+    if (rc) return rc;
+    if (!rows_out || !sizes_out || ntip == 0) return CASPHY_EINVAL;
+    HostTree H;
+    if ((rc = build(ntip, nnode, nedge, edge, H))) return rc;
+    const u32 nbin = ((ntip - 1) >> 5) + 1, kCache = 8192;
+    // output row of every internal child (reverse edge order), sizes, and the
+    // reference's open-row limit (nodeDesBig keeps 8192 cache rows)
+    std::vector<u32> rowOf(nnode, nnode - 1);
+    std::vector<int> size(nnode, 0);
+    std::vector<unsigned char> open(nnode, 0);
+    u32 nUse = 0, r = 0;
+    for (u32 e = nedge; e-- > 0;) {
+        const u32 a = edge[2 * e] - ntip, d = edge[2 * e + 1];
+        if (!open[a]) {
+            if (nUse == kCache) {
+                casphy_set_last_error_msg("Run out of cache!");
+                return CASPHY_ERANGE;
+            }
+            open[a] = 1;
+            nUse++;
+        }
+        if (d < ntip) {
+            size[a]++;
+        } else {
+            size[a] += size[d - ntip];
+            rowOf[d - ntip] = r++;
+            open[d - ntip] = 0;
+            nUse--;
+        }
+    }
+    for (u32 i = 1; i < nnode; i++) sizes_out[nnode - 1 - i] = size[i];
+    DeviceScope ds;
+    cudaStream_t st = 0;
+    struct B {
+        u32 *rows, *rowOf;
+    };
+    auto lay = [&](Carve& c) {
+        B b;
+        b.rows = c.take<u32>((size_t)nnode * nbin);
+        b.rowOf = c.take<u32>(nnode);
+        return b;
+    };
+    B L;
+    DevTree D;
+    if ((rc = reserve_and_upload(ds, H, lay, L, D, st))) return rc;
+    CASPHY_CUDA_TRY(cudaMemcpyAsync(L.rowOf, rowOf.data(), 4ull * nnode, cudaMemcpyHostToDevice, st));
+    Tree Tu{ntip, D.kidOff, D.kid, D.kidEdge, D.up};
+    for (size_t lv = 0; lv + 1 < H.upOff.size(); lv++) {
+        const u32 cnt = H.upOff[lv + 1] - H.upOff[lv];
+        k_clade<<<blocks((u64)cnt * nbin, 256), 256, 0, st>>>(Tu, H.upOff[lv], cnt, nbin, L.rowOf, L.rows);
+    }
+    CASPHY_CUDA_TRY(cudaGetLastError());
+    if (nnode > 1)
+        CASPHY_CUDA_TRY(cudaMemcpyAsync(rows_out, L.rows, 4ull * (nnode - 1) * nbin, cudaMemcpyDeviceToHost, st));
     CASPHY_CUDA_TRY(cudaStreamSynchronize(st));
     return CASPHY_OK;
 }

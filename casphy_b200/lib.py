@@ -106,6 +106,7 @@ def lib():
         _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
         L.casphy_ancestral_bit.argtypes = [u32, u32, u32, _u32p, u32, _u32p, vp, _u32p]
         L.casphy_ancestral_char.argtypes = [u32, u32, u32, _i32p, u32, _u32p, _u32p, C.c_float, C.c_float, vp, _u32p]
+        L.casphy_node_des.argtypes = [u32, u32, u32, _u32p, _u32p, _i32p]
         L.casphy_tip_merge.argtypes = [u32, _u32p, vp, C.c_double, _i32p]
         if hasattr(L, "casphy_join_bit"):
             L.casphy_join_bit.argtypes = [u32, u32, _u32p, _f64p, C.c_int, _u32p, _u32p, C.POINTER(JoinStats)]
@@ -359,3 +360,14 @@ def tip_merge(counts, idx, pshared):
     _chk(lib().casphy_tip_merge(len(counts), counts, idx.ctypes.data if idx.size else None, float(pshared), member),
          "casphy_tip_merge")
     return member[: len(counts)]
+
+
+def node_des(edge, ntip, nnode=None):
+    """nodeDesBig: (clade rows (nnode-1) x nbin in file order, sizes as returned)."""
+    edge = _u32(edge).reshape(-1, 2)
+    nnode = int(edge.max()) + 1 - ntip if nnode is None else int(nnode)
+    nbin = (ntip - 1) // 32 + 1
+    rows = np.zeros((max(nnode - 1, 1), nbin), np.uint32)
+    sizes = np.zeros(max(nnode - 1, 1), np.int32)
+    _chk(lib().casphy_node_des(ntip, nnode, len(edge), edge.reshape(-1), rows, sizes), "casphy_node_des")
+    return rows[: nnode - 1], sizes[: nnode - 1]

@@ -225,6 +225,18 @@ int casphy_felsenstein_optimize(uint32_t ntip, uint32_t nedge, const uint32_t *e
                                 uint32_t max_iter, double rel_tol, casphy_blopt_stats *stats);
 
 /*
+ * nodeDesBig (src/functions.cpp:1277-1366): the clade matrix phy2clade
+ * writes for TransferDisStream (R/bootstrap_functions.R:1-32).  edge as for
+ * the parsimony entry points; rows_out gets (nnode-1) x nbin u32 rows, nbin =
+ * (ntip-1)/32+1: the tip bitset of every internal child, in reverse edge
+ * order (the file body after its {nnode-1, nbin} header); sizes_out[nnode-1]
+ * gets the sizes nodeDesBig returns (internal nodes 1..nnode-1, last first).
+ * CASPHY_ERANGE where the reference runs out of its 8192 open rows.
+ */
+int casphy_node_des(uint32_t ntip, uint32_t nnode, uint32_t nedge, const uint32_t *edge,
+                    uint32_t *rows_out, int32_t *sizes_out);
+
+/*
  * tipMerge (cu/tipMerge.cu:130-461): categories of tips whose neighbour lists
  * overlap.  counts[ntip] and idx (the concatenated ascending lists) are the
  * .nNeighbor body and the .idx file of radiusNeighbor(DNA); member[ntip]

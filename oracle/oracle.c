@@ -963,3 +963,48 @@ done:
     free(off); free(so); free(tr); free(run); free(sh);
     return st;
 }
+
+/* ------------------------------------------------------------------------
+ * nodeDesBig (src/functions.cpp:1277-1366): over the edges in reverse order,
+ * a tip child sets its bit in the parent's row and adds 1 to its size; an
+ * internal child adds its size and ORs its row into the parent's, and its
+ * own row is written out then.  The reference keeps the open rows in 8192
+ * cache slots and stops with "Run out of cache!" when more are open.  The
+ * returned sizes are those of internal nodes 1..nnode-1, last node first. */
+int oracle_node_des(uint32_t ntip, uint32_t nnode, uint32_t nedge, const uint32_t *edge,
+                    uint32_t *rows_out, int32_t *sizes_out) {
+    if (!edge || !rows_out || !sizes_out || nnode == 0 || ntip == 0) return ORACLE_EINVAL;
+    const u32 nbin = ((ntip - 1) >> 5) + 1, kCache = 8192;
+    u32 *bits = (u32 *)calloc((size_t)nnode * nbin, sizeof(u32));
+    int32_t *size = (int32_t *)calloc(nnode, sizeof(int32_t));
+    char *open = (char *)calloc(nnode, 1);
+    if (!bits || !size || !open) { free(bits); free(size); free(open); return ORACLE_ENOMEM; }
+    int st = ORACLE_OK;
+    u32 nUse = 0, r = 0;
+    for (long i = (long)nedge - 1; i >= 0; i--) {
+        const u32 a = edge[2 * i], d = edge[2 * i + 1];
+        if (a < ntip || a >= ntip + nnode || d >= ntip + nnode) { st = ORACLE_EINVAL; break; }
+        const u32 ai = a - ntip;
+        if (!open[ai]) {
+            if (nUse == kCache) { st = ORACLE_ERANGE; break; }
+            open[ai] = 1;
+            nUse++;
+        }
+        if (d < ntip) {
+            size[ai]++;
+            bits[(size_t)ai * nbin + (d >> 5)] |= 1u << (d & 31);
+        } else {
+            const u32 di = d - ntip;
+            size[ai] += size[di];
+            for (u32 x = 0; x < nbin; x++) bits[(size_t)ai * nbin + x] |= bits[(size_t)di * nbin + x];
+            memcpy(rows_out + (size_t)r * nbin, bits + (size_t)di * nbin, sizeof(u32) * nbin);
+            r++;
+            open[di] = 0;
+            nUse--;
+        }
+    }
+    if (st == ORACLE_OK)
+        for (u32 i = 1; i < nnode; i++) sizes_out[nnode - 1 - i] = size[i];
+    free(bits); free(size); free(open);
+    return st;
+}

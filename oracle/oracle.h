@@ -103,6 +103,13 @@ int oracle_ancestral_char(uint32_t ntip, uint32_t nnode, uint32_t nsite, const i
                           uint32_t nedge, const uint32_t *edge, const uint32_t *tipSize,
                           float minSize, float minRatio, int32_t *state_out, uint32_t *len_out);
 
+/* nodeDesBig (src/functions.cpp:1277-1366): rows_out gets, for the internal
+ * children in reverse edge order, their tip bitsets ((nnode-1) x nbin u32,
+ * nbin = (ntip-1)/32+1: the file body); sizes_out[nnode-1] the returned
+ * sizes.  ORACLE_ERANGE where the reference runs out of its 8192 cache rows. */
+int oracle_node_des(uint32_t ntip, uint32_t nnode, uint32_t nedge, const uint32_t *edge,
+                    uint32_t *rows_out, int32_t *sizes_out);
+
 /* tipMerge (cu/tipMerge.cu:130-461): counts[ntip] and the concatenated
  * ascending neighbour lists idx (the .nNeighbor body and .idx); member_out
  * gets the .member values.  Returns ORACLE_ERANGE when a list is longer than

@@ -204,3 +204,15 @@ def tip_merge(counts, idx, pshared):
                                 idx.ctypes.data_as(C.c_void_p), C.c_double(pshared),
                                 member.ctypes.data_as(C.c_void_p)), "tip_merge")
     return member[: len(counts)]
+
+
+def node_des(edge, ntip, nnode=None):
+    edge = _u32(edge).reshape(-1, 2)
+    nnode = int(edge.max()) + 1 - ntip if nnode is None else int(nnode)
+    nbin = (ntip - 1) // 32 + 1
+    rows = np.zeros((max(nnode - 1, 1), nbin), np.uint32)
+    sizes = np.zeros(max(nnode - 1, 1), np.int32)
+    _chk(lib().oracle_node_des(C.c_uint32(ntip), C.c_uint32(nnode), C.c_uint32(len(edge)),
+                               np.ascontiguousarray(edge.reshape(-1)).ctypes.data_as(C.c_void_p),
+                               rows.ctypes.data_as(C.c_void_p), sizes.ctypes.data_as(C.c_void_p)), "node_des")
+    return rows[: nnode - 1], sizes[: nnode - 1]

@@ -1,6 +1,6 @@
-// C wrapper around the reference's parsimony functions (ancestralBitReverse,
-// charAncestralEC), which the ref build recipe pastes in front of this file
-// from src/functions.cpp.  Test infrastructure only: it produces the golden
+// C wrapper around the reference's CPU functions (ancestralBitReverse,
+// charAncestralEC, nodeDesBig), which the ref build recipe pastes in front of
+// this file from src/functions.cpp.  Test infrastructure only: it produces the golden
 // outputs the oracle restatement and the GPU path are checked against.
 #include <cstdint>
 #include <cstring>
@@ -38,4 +38,18 @@ extern "C" int ref_ancestral_char(uint32_t ntip, uint32_t nnode, uint32_t nsite,
     for (auto& x : out.vecs)
         if (x.first == "edgeLen") std::memcpy(len, x.second.v.data(), sizeof(uint32_t) * nedge);
     return 0;
+}
+
+// nodeDesBig writes the clade rows to a file (header {nnode-1, nbin} when
+// header is true) and returns the internal node sizes.
+extern "C" int ref_node_des_big(uint32_t ntip, uint32_t nnode, uint32_t nedge, const uint32_t* edge,
+                                const char* path, int header, int32_t* sizes_out) {
+    Rcpp::IntegerMatrix e((int)nedge, 2);
+    for (uint32_t i = 0; i < nedge; i++) {
+        e(i, 0) = (int)edge[2 * i] + 1;
+        e(i, 1) = (int)edge[2 * i + 1] + 1;
+    }
+    Rcpp::IntegerVector out = nodeDesBig(e, (int)nnode, (int)ntip, std::string(path), 8192, header != 0);
+    for (int i = 0; i < out.size(); i++) sizes_out[i] = out(i);
+    return out.size();
 }

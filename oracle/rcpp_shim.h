@@ -3,8 +3,14 @@
 // pin (test infrastructure, see oracle/Makefile target ref).  Matrices are
 // column-major like R's; only the members those functions use exist.
 #pragma once
+#include <cstdio>
+#include <cstdlib>
 #include <string>
 #include <vector>
+
+// R's transient allocator and printf (the test process frees at exit)
+inline char* R_alloc(size_t n, int size) { return static_cast<char*>(std::calloc(n ? n : 1, (size_t)size)); }
+#define Rprintf std::printf
 
 namespace Rcpp {
 
@@ -16,6 +22,13 @@ struct IntegerVector {
     int& operator[](int i) { return v[(size_t)i]; }
     int size() const { return (int)v.size(); }
     void fill(int x) { for (auto& e : v) e = x; }
+};
+
+struct LogicalVector {
+    std::vector<int> v;
+    LogicalVector(int n = 0) : v((size_t)n, 0) {}
+    int& operator()(int i) { return v[(size_t)i]; }
+    void fill(bool x) { for (auto& e : v) e = x ? 1 : 0; }
 };
 
 struct MatrixColumn {

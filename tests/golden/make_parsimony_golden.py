@@ -1,6 +1,7 @@
 """Golden fixtures for the parsimony edge lengths (ancestralBitReverse,
-charAncestralEC of src/functions.cpp), produced by the reference's own
-functions compiled into oracle/_ref/libparsimony_ref.so (make -C oracle ref).
+charAncestralEC of src/functions.cpp) and the clade rows of nodeDesBig,
+produced by the reference's own functions compiled into
+oracle/_ref/libparsimony_ref.so (make -C oracle ref).
 
     python tests/golden/make_parsimony_golden.py   # writes parsimony_reference.npz
 
@@ -87,6 +88,20 @@ def main():
     lib.ref_ancestral_bit.argtypes = [C.c_uint32] * 3 + [u32p, C.c_uint32, u32p, u32p, u32p]
     lib.ref_ancestral_char.argtypes = [C.c_uint32] * 3 + [i32p, C.c_uint32, u32p, u32p, C.c_float, C.c_float,
                                                            i32p, u32p]
+    lib.ref_node_des_big.argtypes = [C.c_uint32] * 3 + [u32p, C.c_char_p, C.c_int, i32p]
+
+    def node_des(edge, ntip, nnode, name):
+        import tempfile
+        sizes = np.zeros(max(nnode - 1, 1), np.int32)
+        with tempfile.TemporaryDirectory() as d:
+            path = os.path.join(d, "clades.bin")
+            lib.ref_node_des_big(ntip, nnode, len(edge), np.ascontiguousarray(edge.reshape(-1)), path.encode(), 1,
+                                 sizes)
+            raw = np.fromfile(path, dtype=np.uint32)
+        res[f"nd/{name}/edge"] = edge
+        res[f"nd/{name}/ntip"] = np.array([ntip, nnode], np.uint32)
+        res[f"nd/{name}/file"] = raw
+        res[f"nd/{name}/sizes"] = sizes[: nnode - 1]
     rng = np.random.default_rng(2024)
     res = {}
     # bit matrices
@@ -107,6 +122,7 @@ def main():
         res[f"pb/{name}/nnode"] = np.array([nnode], np.uint32)
         res[f"pb/{name}/state"] = state.reshape(nnode, nbin)
         res[f"pb/{name}/len"] = ln
+        node_des(edge, ntip, nnode, name)
     # indel matrices (raw states: -1 missing, 0 unedited, alleles >= 1)
     for name, ntip, nsite, kind, ms, mr, uneven in (("c60y", 60, 40, "yule", 0.0, 0.0, False),
                                                    ("c500m", 500, 128, "multi", 0.0, 0.0, False),
@@ -132,6 +148,9 @@ def main():
         res[f"pc/{name}/rule"] = np.array([ms, mr], np.float32)
         res[f"pc/{name}/state"] = state.reshape(nnode, nsite)
         res[f"pc/{name}/len"] = ln
+    for name, ntip in (("y3000", 3000), ("y33", 33)):
+        edge, nnode = trees(ntip, rng, "yule")
+        node_des(edge, ntip, nnode, name)
     path = os.path.join(HERE, "parsimony_reference.npz")
     np.savez_compressed(path, **res)
     print(f"wrote {path} ({len(res)} arrays)")

@@ -16,7 +16,8 @@ def _cases():
     out = {}
     for k in z.files:
         kind, name, field = k.split("/")
-        out.setdefault((kind, name), {})[field] = z[k]
+        if kind in ("pb", "pc"):
+            out.setdefault((kind, name), {})[field] = z[k]
     return sorted(out.items())
 
 
@@ -64,3 +65,42 @@ def test_gpu_rejects_unordered_edges(gpu_lib):
     edge, _, _ = gpu_lib.join_bit(words, None, 1)
     with pytest.raises(gpu_lib.CasphyError):
         gpu_lib.ancestral_bit(words, edge[::-1])
+
+
+def _nd_cases():
+    z = np.load(os.path.join(HERE, "golden", "parsimony_reference.npz"))
+    names = sorted(set(k.split("/")[1] for k in z.files if k.startswith("nd/")))
+    out = []
+    for n in names:
+        ntip, nnode = (int(x) for x in z[f"nd/{n}/ntip"])
+        raw = z[f"nd/{n}/file"]
+        out.append((n, z[f"nd/{n}/edge"], ntip, nnode, raw[:2], raw[2:].reshape(-1, raw[1]), z[f"nd/{n}/sizes"]))
+    return out
+
+
+@pytest.mark.parametrize("name,edge,ntip,nnode,hdr,rows,sizes", _nd_cases(), ids=[c[0] for c in _nd_cases()])
+def test_node_des_oracle_matches_reference(name, edge, ntip, nnode, hdr, rows, sizes):
+    r, s = O.node_des(edge, ntip, nnode)
+    assert tuple(hdr) == (nnode - 1, (ntip - 1) // 32 + 1)
+    assert np.array_equal(r, rows) and np.array_equal(s, sizes)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,edge,ntip,nnode,hdr,rows,sizes", _nd_cases(), ids=[c[0] for c in _nd_cases()])
+def test_node_des_gpu_matches_reference(gpu_lib, name, edge, ntip, nnode, hdr, rows, sizes):
+    r, s = gpu_lib.node_des(edge, ntip, nnode)
+    assert np.array_equal(r, rows) and np.array_equal(s, sizes)
+
+
+@pytest.mark.gpu
+def test_node_des_gpu_on_a_large_join_tree(gpu_lib):
+    from casphy_b200 import bootstrap as B
+    from casphy_b200 import synth
+    words = synth.binary_workload(30_000, 256, 16, 0.03, 0.05, seed=44)
+    edge, _, _ = gpu_lib.join_bit(words, None, 1)
+    r, s = gpu_lib.node_des(edge, 30_000)
+    ro, so = O.node_des(edge, 30_000)
+    assert np.array_equal(r, ro) and np.array_equal(s, so)
+    # the same set of clades as the package's clade bitsets (all internal nodes but the root)
+    cb = B.clade_bits(edge, 30_000, (30_000 + 31) // 32)
+    assert np.array_equal(np.unique(r, axis=0), np.unique(cb, axis=0))
