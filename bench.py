@@ -381,6 +381,32 @@ def rows_suite(L, nthreads):
         "gpu_s": t_dna, "pairs": 20_000 * 20_000, "neighbours": int(dc.sum()),
         "cpu_sample": f"first {sub} sequences", "cpu_s_sample": t_cd, "cpu_cores": nthreads,
         "sample_identical": bool(np.array_equal(gc, oc) and np.array_equal(gi, oi))}
+    # fasta2bin on the C3 alignment written as FASTA, beside the reference's
+    # own fasta2bin (host code, built from cu/fasta2bin.cu into oracle/_ref)
+    import subprocess
+    import tempfile
+    letters = np.frombuffer(b"ACGT-", dtype=np.uint8)
+    with tempfile.TemporaryDirectory() as d:
+        src = os.path.join(d, "c3.fasta")
+        with open(src, "wb") as f:
+            for i in range(states.shape[0]):
+                f.write(b">s%d\n" % i)
+                f.write(letters[states[i]].tobytes())
+                f.write(b"\n")
+        ours = os.path.join(ROOT, "casphy_b200", "bin", "fasta2bin")
+        ref = os.path.join(ROOT, "oracle", "_ref", "fasta2bin")
+        t0 = time.perf_counter()
+        subprocess.run([ours, src, os.path.join(d, "a")], check=True, stdout=subprocess.DEVNULL)
+        t_f = time.perf_counter() - t0
+        f2b = {"workload": "the C3 alignment (20000 x 2000, 2% gaps) as a FASTA file", "casphy_s": t_f}
+        if os.path.exists(ref):
+            t0 = time.perf_counter()
+            subprocess.run([ref, src, os.path.join(d, "b")], check=True, stdout=subprocess.DEVNULL)
+            f2b["reference_s"] = time.perf_counter() - t0
+            same = all(open(os.path.join(d, "a" + x), "rb").read() == open(os.path.join(d, "b" + x), "rb").read()
+                       for x in (".bin", "_names.txt", "_positions.txt"))
+            f2b["identical_files"] = bool(same)
+        res["C3_fasta2bin"] = f2b
     # tipMerge on 140,000 tips' clustered neighbour lists (avg 18 per row)
     counts, nidx = synth.neighbour_lists(140_000, 4)
     mem, t_tm = _timed(lambda: L.tip_merge(counts, nidx, 0.4))

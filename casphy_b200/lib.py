@@ -106,6 +106,7 @@ def lib():
         _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
         L.casphy_ancestral_bit.argtypes = [u32, u32, u32, _u32p, u32, _u32p, vp, _u32p]
         L.casphy_ancestral_char.argtypes = [u32, u32, u32, _i32p, u32, _u32p, _u32p, C.c_float, C.c_float, vp, _u32p]
+        L.casphy_fasta_encode.argtypes = [u32, u32, C.c_char_p, vp, C.POINTER(u32), vp, C.c_uint64]
         L.casphy_node_des.argtypes = [u32, u32, u32, _u32p, _u32p, _i32p]
         L.casphy_tip_merge.argtypes = [u32, _u32p, vp, C.c_double, _i32p]
         if hasattr(L, "casphy_join_bit"):
@@ -371,3 +372,18 @@ def node_des(edge, ntip, nnode=None):
     sizes = np.zeros(max(nnode - 1, 1), np.int32)
     _chk(lib().casphy_node_des(ntip, nnode, len(edge), edge.reshape(-1), rows, sizes), "casphy_node_des")
     return rows[: nnode - 1], sizes[: nnode - 1]
+
+
+def fasta_encode(seqs):
+    """fasta2bin's column classification and encoding of equal-length
+    sequences (bytes or str): (variable flags u8[len], .bin body u32 rows)."""
+    rows = [x.encode() if isinstance(x, str) else bytes(x) for x in seqs]
+    nseq, length = len(rows), len(rows[0])
+    buf = b"".join(rows)
+    var = np.zeros(length, np.uint8)
+    nkeep = C.c_uint32(0)
+    out = np.zeros(max(nseq * ((length + 3) // 4), 1), np.uint32)
+    _chk(lib().casphy_fasta_encode(nseq, length, buf, var.ctypes.data, C.byref(nkeep), out.ctypes.data, out.size),
+         "casphy_fasta_encode")
+    nw = (nkeep.value + 3) // 4
+    return var, out[: nseq * nw].reshape(nseq, nw)

@@ -225,6 +225,18 @@ int casphy_felsenstein_optimize(uint32_t ntip, uint32_t nedge, const uint32_t *e
                                 uint32_t max_iter, double rel_tol, casphy_blopt_stats *stats);
 
 /*
+ * fasta2bin's column classification and encoding (cu/fasta2bin.cu:47-206):
+ * seqs is the aligned sequences, nseq rows of len characters.  variable[len]
+ * gets 1 for a variable column (some base count, ambiguity codes counting for
+ * each of their bases, strictly between 0 and nseq); *nkeep_out the number
+ * kept; bin_out (when non-NULL and bin_cap >= nseq*ceil(nkeep/4)) the .bin
+ * body: per sequence the kept columns' 8-bit codes, four per u32, low byte
+ * first.  Parsing the FASTA text stays with the caller (the fasta2bin drop-in).
+ */
+int casphy_fasta_encode(uint32_t nseq, uint32_t len, const char *seqs, uint8_t *variable,
+                        uint32_t *nkeep_out, uint32_t *bin_out, uint64_t bin_cap);
+
+/*
  * nodeDesBig (src/functions.cpp:1277-1366): the clade matrix phy2clade
  * writes for TransferDisStream (R/bootstrap_functions.R:1-32).  edge as for
  * the parsimony entry points; rows_out gets (nnode-1) x nbin u32 rows, nbin =
