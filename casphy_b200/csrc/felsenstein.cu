@@ -15,7 +15,8 @@
 // d log L / d t_c, then passes U_c = R P_c down.  Both ratios are invariant
 // to the scale of R, so outside vectors are renormalised freely.  Site terms
 // are reduced per block and written to a per-(edge, site block) array that a
-// last kernel sums in a fixed order, so log L and the gradient are bitwise
+// last kernel sums in a fixed order (site terms in binary32 within a block,
+// the blocks in binary64), so log L and the gradient are bitwise
 // reproducible.  Sites are processed in chunks whose partials fit a
 // device-memory budget (sites are independent, so nothing is recomputed).
 // All launches of one evaluation are captured once per problem into a CUDA
@@ -94,6 +95,25 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
     if (threadIdx.x == 0)
         for (u32 i = 0; i < blockDim.x / 32; i++) t += red[i];
     return t;  // valid in thread 0
+}
+
+// Block sums of two binary32 values (thread 0 gets them); one CTA barrier
+// pair for both children's site terms.
+__device__ __forceinline__ float2 block_sum2f(float a, float b, float2* red) {
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xFFFFFFFFu, a, o);
+        b += __shfl_xor_sync(0xFFFFFFFFu, b, o);
+    }
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = make_float2(a, b);
+    __syncthreads();
+    float2 t = make_float2(0.f, 0.f);
+    if (threadIdx.x == 0)
+        for (u32 i = 0; i < blockDim.x / 32; i++) {
+            t.x += red[i].x;
+            t.y += red[i].y;
+        }
+    return t;
 }
 
 // ---------------------------------------------------------------- HKY85 ---
@@ -228,9 +248,9 @@ __global__ void __launch_bounds__(kSites) k_loglik_hky(u32 root, Tree T, HkyBuf 
     if (threadIdx.x == 0) part[C.blk0 + blockIdx.x] = v;
 }
 
-__global__ void __launch_bounds__(kSites) k_outside_hky(u32 root, Tree T, HkyBuf B, Chunk C, u32 off, Hky m,
+__global__ void __launch_bounds__(kSites, 5) k_outside_hky(u32 root, Tree T, HkyBuf B, Chunk C, u32 off, Hky m,
                                                         const double* __restrict__ w, double* gpart) {
-    __shared__ double red[kSites / 32];
+    __shared__ float2 red[kSites / 32];
     const u32 s = blockIdx.x * kSites + threadIdx.x;
     const uint4 nf = T.outInfo[off + blockIdx.y];
     const u32 v = nf.x, vi = v - T.ntip;
@@ -245,7 +265,8 @@ __global__ void __launch_bounds__(kSites) k_outside_hky(u32 root, Tree T, HkyBuf
     const float4 la = child_hky(T, B, C, ca, ss, &e);
     const float4 lb = child_hky(T, B, C, cb, ss, &e);
     const float4 ma = pmatvec(B.P + 16 * eA, la), mb = pmatvec(B.P + 16 * eB, lb);
-    const double ws = ok ? w[C.s0 + s] : 0.0;
+    const float ws = ok ? (float)w[C.s0 + s] : 0.f;
+    float gs[2];
 #pragma unroll
     for (int side = 0; side < 2; side++) {
         const u32 c = side ? cb : ca;
@@ -255,15 +276,18 @@ __global__ void __launch_bounds__(kSites) k_outside_hky(u32 root, Tree T, HkyBuf
         const float4 mc = side ? mb : ma;
         const float4 r = make_float4(u.x * msib.x, u.y * msib.y, u.z * msib.z, u.w * msib.w);
         const float4 dm = matvec(B.dP + 16 * ec, lc);
-        double g = 0.0;
-        if (ok) g = ws * ((double)dot4(r, dm) / (double)dot4(r, mc));
-        g = block_sum(g, red);
-        if (threadIdx.x == 0) gpart[(size_t)ec * C.nblkTot + C.blk0 + blockIdx.x] = g;
+        gs[side] = ok ? ws * (dot4(r, dm) / dot4(r, mc)) : 0.f;
         if (ok && c >= T.ntip) {
             float4 uc = pvecmat(r, B.P + 16 * ec);
             renorm4(uc);
             B.U[(size_t)(c - T.ntip) * C.W + s] = uc;
         }
+    }
+    // site terms in binary32 within the block; blocks are added in binary64
+    const float2 g = block_sum2f(gs[0], gs[1], red);
+    if (threadIdx.x == 0) {
+        gpart[(size_t)eA * C.nblkTot + C.blk0 + blockIdx.x] = g.x;
+        gpart[(size_t)eB * C.nblkTot + C.blk0 + blockIdx.x] = g.y;
     }
 }
 
@@ -359,7 +383,7 @@ __global__ void __launch_bounds__(kSites) k_loglik_irr(u32 root, Tree T, IrrBuf 
 
 __global__ void __launch_bounds__(kSites) k_outside_irr(u32 root, Tree T, IrrBuf B, Chunk C, u32 off,
                                                         const double* __restrict__ w, double* gpart) {
-    __shared__ double red[kSites / 32];
+    __shared__ float2 red[kSites / 32];
     const u32 s = blockIdx.x * kSites + threadIdx.x;
     const uint4 nf = T.outInfo[off + blockIdx.y];
     const u32 v = nf.x, vi = v - T.ntip;
@@ -386,7 +410,8 @@ __global__ void __launch_bounds__(kSites) k_outside_irr(u32 root, Tree T, IrrBuf
         qs[i] = qsum(B, gs, l[i]);
         m0[i] = l[i].x + pp[i].y * (qs[i] - l[i].x);
     }
-    const double ws = ok ? w[gs] : 0.0;
+    const float ws = ok ? (float)w[gs] : 0.f;
+    float gsum[2];
 #pragma unroll
     for (int c = 0; c < 2; c++) {
         const int sb = 1 - c;
@@ -408,10 +433,7 @@ __global__ void __launch_bounds__(kSites) k_outside_irr(u32 root, Tree T, IrrBuf
         float den = R0 * m0[c];
         if (ac == kWild) den += l[c].y * (RX + (aR != kNoneA ? RY : 0.f));
         else if (ac != kNoneA) den += l[c].y * (RX * qof(B, gs, ac) + (aR == ac ? RY : 0.f));
-        double g = 0.0;
-        if (ok) g = ws * ((double)(R0 * dm0) / (double)den);
-        g = block_sum(g, red);
-        if (threadIdx.x == 0) gpart[(size_t)eds[c] * C.nblkTot + C.blk0 + blockIdx.x] = g;
+        gsum[c] = ok ? ws * ((R0 * dm0) / den) : 0.f;
         if (ok && kids[c] >= T.ntip) {
             float u0 = R0 * pp[c].x, x = pp[c].y * R0 + RX, y = RY;
             const float mx = fmaxf(u0, fmaxf(x, y));
@@ -431,6 +453,12 @@ __global__ void __launch_bounds__(kSites) k_outside_irr(u32 root, Tree T, IrrBuf
             }
             B.U[(size_t)(kids[c] - T.ntip) * C.W + s] = make_float4(u0, x, y, __int_as_float(aR));
         }
+    }
+    // site terms in binary32 within the block; blocks are added in binary64
+    const float2 g = block_sum2f(gsum[0], gsum[1], red);
+    if (threadIdx.x == 0) {
+        gpart[(size_t)eds[0] * C.nblkTot + C.blk0 + blockIdx.x] = g.x;
+        gpart[(size_t)eds[1] * C.nblkTot + C.blk0 + blockIdx.x] = g.y;
     }
 }
 
