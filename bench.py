@@ -38,7 +38,8 @@ METRIC = "pair-scores/s & tree s @200k cells; BL-opt & bootstrap speedup vs plai
 UNIT = "pair-scores/s"
 WORKLOAD = dict(ncell=200_000, nsite=1024, depth=20, p_edit=0.02, nallele=256, zipf_s=1.3,
                 p_missing=0.15, seed=5)
-CPU_SAMPLE_CELLS = 5000
+CPU_SAMPLE_CELLS = 5000      # oracle port (multi-threaded restatement of cu/joinEdgeIndel.cu)
+TWIN_SAMPLE_CELLS = 1024     # the reference's own CPU join (greedyJoinEdge2), about 10 s a tree
 
 
 def workload_name():
@@ -149,6 +150,25 @@ def cpu_port_run(codes, nstate, weight, nthreads):
     return float(st[1]), dt
 
 
+def cpu_twin_run(codes, nstate, weight):
+    """The reference's CPU path for this job: greedyJoinEdge2 (src/functions
+    .cpp:1880-2017, what phy.join runs when no CUDA path is given), compiled
+    from the reference's source into oracle/_ref/libcputwin_ref.so.  It is
+    single-threaded.  Its pair-scores: N(N-1)/2 at the start plus, after each
+    join, one per remaining live node, (N-1)^2 in all."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import cputwin as T
+    n = codes.shape[0]
+    t0 = time.perf_counter()
+    T.greedy_join_edge2(codes, nstate, weight, want_edge=False)
+    dt = time.perf_counter() - t0
+    return float((n - 1) ** 2), dt
+
+
+def cpu_twin_available():
+    return os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libcputwin_ref.so"))
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -179,27 +199,40 @@ def barrier(world):
 
 
 def run_reference(args, world, rank):
+    """The reference's CPU path on a bounded sample of the workload per step:
+    greedyJoinEdge2 compiled from the reference's source when it was built
+    here, else the oracle port."""
     if rank != 0:
         return 0
-    nthreads = os.cpu_count() or 1
-    codes, nstate, weight = gen_workload(CPU_SAMPLE_CELLS)
+    twin = cpu_twin_available()
+    if twin:
+        ncell, cores, kind = TWIN_SAMPLE_CELLS, 1, "reference"
+        run = cpu_twin_run
+        what = ("greedyJoinEdge2 (src/functions.cpp:1880-2017) compiled from the reference's source behind an "
+                "Rcpp stand-in header, single-threaded as in R; pair-scores counted as its own (N-1)^2")
+    else:
+        ncell, cores, kind = CPU_SAMPLE_CELLS, os.cpu_count() or 1, "port"
+        run = lambda c, n, w: cpu_port_run(c, n, w, cores)  # noqa: E731
+        what = "greedy join restated from cu/joinEdgeIndel.cu (oracle port)"
+    codes, nstate, weight = gen_workload(ncell)
     times, pairs = [], 0.0
     if args.warmup > 0:
-        cpu_port_run(codes[:500], nstate, weight, nthreads)
+        wc, wn, ww = gen_workload(256)
+        run(wc, wn, ww)
     for _ in range(args.steps):
-        p, dt = cpu_port_run(codes, nstate, weight, nthreads)
+        p, dt = run(codes, nstate, weight)
         times.append(dt)
         pairs = p
     tot = sum(times)
     value = pairs * args.steps / tot
-    sample = (f"first {CPU_SAMPLE_CELLS} cells of the {WORKLOAD['ncell']}-cell workload per step "
-              f"({pairs:.0f} pair-scores, greedy join restated from cu/joinEdgeIndel.cu, {nthreads} threads)")
+    sample = (f"first {ncell} cells of the {WORKLOAD['ncell']}-cell workload per step "
+              f"({pairs:.0f} pair-scores, {tot / args.steps:.2f} s a tree; {what}; {cores} thread(s))")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
-            "config": {"workload": workload_name(), "cells_per_step": CPU_SAMPLE_CELLS},
+            "config": {"workload": workload_name(), "cells_per_step": ncell},
             "impl": "reference",
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -301,7 +334,16 @@ def rows_suite(L, nthreads):
     the host API (inputs and outputs through host memory) next to the CPU
     restatement (oracle/) on the host cores."""
     import oracle as O
+    from casphy_b200 import bootstrap as B
     from casphy_b200 import synth
+    twin = cpu_twin_available()
+    if twin:
+        import cputwin as T
+
+    def same_clades(e_a, e_b, ntip):
+        nw = (ntip + 31) // 32
+        return (set(map(bytes, B.clade_bits(e_a, ntip, nw))) == set(map(bytes, B.clade_bits(e_b, ntip, nw))))
+
     res = {}
     # C1: indel 1,024 x 256, joinEdgeIndel + nodeKeepIndel
     raw = synth.lineage_states(1024, 256, 12, 0.04, 64, 1.5, 0.10, seed=21)
@@ -320,13 +362,18 @@ def rows_suite(L, nthreads):
                     "nodeKeepIndel against 256 out-group cells, cutoff 2",
         "gpu_s": t_gpu + t_keep, "join_device_ms": st["total_ms"], "cpu_s": t_cpu, "cpu_cores": nthreads,
         "identical": bool(np.array_equal(edge, e0) and np.array_equal(state, s0) and np.array_equal(keep, k0))}
+    if twin:
+        t0 = time.perf_counter()
+        te = T.greedy_join_edge2(codes, ns, w)
+        res["C1_joinEdgeIndel_nodeKeepIndel"]["reference_cpu"] = {
+            "function": "greedyJoinEdge2 (src/functions.cpp:1880-2017), 1 thread", "join_s": time.perf_counter() - t0,
+            "same_tree": bool(same_clades(np.stack([te[0, :-1], te[1, :-1]], 1), edge, 1024))}
     # C2: binary 10,000 x 512: joinEdgeBitReverse, radiusNeighbor r=4, TransferDisStream vs the true tree
     words = synth.binary_workload(10_000, 512, 16, 0.03, 0.05, seed=23)
     (bedge, bstate, bst), t_join = _timed(lambda: L.join_bit(words, None, 1))
     bmat = np.ascontiguousarray(words.T)
     wr = np.ones(512)
     (cnt, idx), t_rad = _timed(lambda: L.radius_bit(bmat, wr, 4))
-    from casphy_b200 import bootstrap as B
     truth = synth.lineage_clades(10_000, 16, seed=23)
     est = B.clade_bits(bedge, 10_000, (10_000 + 31) // 32)
     (ymin, ysize, xmin, xsize), t_td = _timed(lambda: L.transfer_dis(truth, est, 10_000))
@@ -365,6 +412,22 @@ def rows_suite(L, nthreads):
     g_c, g_i = L.radius_bit(np.ascontiguousarray(words[:sub].T), wr, 4)
     res["C2_binary"]["radiusNeighbor_r4"]["sample_identical"] = bool(np.array_equal(g_c, c0) and
                                                                      np.array_equal(g_i, i0))
+    if twin:
+        tsub = 2000
+        t0 = time.perf_counter()
+        tj = T.greedy_join_edge_bit(words[:tsub], ancestral_type=1)
+        t_tj = time.perf_counter() - t0
+        gj, _, _ = L.join_bit(words[:tsub], None, 1)
+        t0 = time.perf_counter()
+        tc, _ = T.radius_weighted_rows(words[:sub], 4, 0, sub, nthreads)
+        t_tr = time.perf_counter() - t0
+        res["C2_binary"]["reference_cpu"] = {
+            "joinEdgeBitReverse": {"function": "greedyJoinEdgeBitReverse (src/functions.cpp:3316-3461), 1 thread",
+                                   "sample": f"first {tsub} cells", "s_sample": t_tj,
+                                   "same_tree_as_gpu": bool(same_clades(tj.T, gj, tsub))},
+            "radiusNeighbor_r4": {"function": f"radiusWeightedParallel (src/functions.cpp:1825-1857) per row, "
+                                              f"{nthreads} threads", "sample": f"first {sub} cells",
+                                  "s_sample": t_tr, "same_counts_as_gpu": bool(np.array_equal(tc, g_c))}}
     # C3: DNA 20,000 x 2,000 HKY85 through fasta2bin coding, radiusNeighborDNA at Hamming 20
     states, _ = synth.hky85_alignment(20_000, 2000, 4.0, [0.3, 0.2, 0.2, 0.3], 0.01, 0.02, seed=13)
     raw, var = synth.dna_to_fasta2bin(states)
@@ -381,6 +444,13 @@ def rows_suite(L, nthreads):
         "gpu_s": t_dna, "pairs": 20_000 * 20_000, "neighbours": int(dc.sum()),
         "cpu_sample": f"first {sub} sequences", "cpu_s_sample": t_cd, "cpu_cores": nthreads,
         "sample_identical": bool(np.array_equal(gc, oc) and np.array_equal(gi, oi))}
+    if twin:
+        t0 = time.perf_counter()
+        tc, _ = T.radius_weighted_dna_rows(raw[:sub], lvalid - 20, 0, sub, nthreads)
+        res["C3_radiusNeighborDNA"]["reference_cpu"] = {
+            "function": f"radiusWeightedDNAParallel (src/functions.cpp:4021-4036) per row, {nthreads} threads",
+            "sample": f"first {sub} sequences", "s_sample": time.perf_counter() - t0,
+            "same_counts_as_gpu": bool(np.array_equal(tc, gc))}
     # fasta2bin on the C3 alignment written as FASTA, beside the reference's
     # own fasta2bin (host code, built from cu/fasta2bin.cu into oracle/_ref)
     import subprocess
@@ -543,12 +613,22 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         nthreads = os.cpu_count() or 1
-        # the sample is re-regularised exactly as R would for those cells
+        # samples are re-regularised exactly as R would for those cells
         sub_codes, sub_ns, sub_w = gen_workload(CPU_SAMPLE_CELLS)
         p, dt = cpu_port_run(sub_codes, sub_ns, sub_w, nthreads)
-        cpu = {"value": p / dt, "unit": UNIT, "cores": nthreads, "kind": "port",
-               "sample": (f"first {CPU_SAMPLE_CELLS} cells of this workload ({p:.0f} pair-scores in {dt:.1f} s), "
-                          "greedy join restated from cu/joinEdgeIndel.cu")}
+        port = {"value": p / dt, "unit": UNIT, "cores": nthreads, "kind": "port",
+                "sample": (f"first {CPU_SAMPLE_CELLS} cells of this workload ({p:.0f} pair-scores in {dt:.1f} s), "
+                           "greedy join restated from cu/joinEdgeIndel.cu")}
+        if cpu_twin_available():
+            tc, tn, tw = gen_workload(TWIN_SAMPLE_CELLS)
+            p2, dt2 = cpu_twin_run(tc, tn, tw)
+            cpu = {"value": p2 / dt2, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": (f"first {TWIN_SAMPLE_CELLS} cells of this workload ({p2:.0f} pair-scores in "
+                              f"{dt2:.1f} s): greedyJoinEdge2 (src/functions.cpp:1880-2017), the reference's CPU "
+                              "join, compiled from its source; single-threaded as in R"),
+                   "port": port}
+        else:
+            cpu = port
 
     hbm, how = peaks()
     jl = float(np.mean(join_ms))

@@ -8,16 +8,16 @@
 extern "C" int ref_ancestral_bit(uint32_t ntip, uint32_t nnode, uint32_t nbin, const uint32_t* mat, uint32_t nedge,
                                  const uint32_t* edge, uint32_t* state, uint32_t* len) {
     Rcpp::IntegerMatrix m((int)nbin, (int)ntip), e((int)nedge, 2);
-    std::memcpy(m.v.data(), mat, sizeof(uint32_t) * (size_t)ntip * nbin);
+    std::memcpy(m.data(), mat, sizeof(uint32_t) * (size_t)ntip * nbin);
     for (uint32_t i = 0; i < nedge; i++) {
         e(i, 0) = (int)edge[2 * i] + 1;
         e(i, 1) = (int)edge[2 * i + 1] + 1;
     }
     Rcpp::List out = ancestralBitReverse(m, e, (int)ntip, (int)nnode);
     for (auto& x : out.mats)
-        if (x.first == "nodeState") std::memcpy(state, x.second.v.data(), sizeof(uint32_t) * (size_t)nnode * nbin);
+        if (x.first == "nodeState") std::memcpy(state, x.second.data(), sizeof(uint32_t) * (size_t)nnode * nbin);
     for (auto& x : out.vecs)
-        if (x.first == "edgeLen") std::memcpy(len, x.second.v.data(), sizeof(uint32_t) * nedge);
+        if (x.first == "edgeLen") std::memcpy(len, x.second.data(), sizeof(uint32_t) * nedge);
     return 0;
 }
 
@@ -25,7 +25,7 @@ extern "C" int ref_ancestral_char(uint32_t ntip, uint32_t nnode, uint32_t nsite,
                                   const uint32_t* edge, const uint32_t* tipSize, float minSize, float minRatio,
                                   int32_t* state, uint32_t* len) {
     Rcpp::IntegerMatrix m((int)nsite, (int)ntip), e((int)nedge, 2);
-    std::memcpy(m.v.data(), mat, sizeof(int32_t) * (size_t)ntip * nsite);
+    std::memcpy(m.data(), mat, sizeof(int32_t) * (size_t)ntip * nsite);
     for (uint32_t i = 0; i < nedge; i++) {
         e(i, 0) = (int)edge[2 * i] + 1;
         e(i, 1) = (int)edge[2 * i + 1] + 1;
@@ -34,9 +34,9 @@ extern "C" int ref_ancestral_char(uint32_t ntip, uint32_t nnode, uint32_t nsite,
     for (uint32_t i = 0; i < ntip; i++) ts(i) = (int)tipSize[i];
     Rcpp::List out = charAncestralEC(m, e, ts, (int)nnode, minSize, minRatio);
     for (auto& x : out.mats)
-        if (x.first == "nodeState") std::memcpy(state, x.second.v.data(), sizeof(int32_t) * (size_t)nnode * nsite);
+        if (x.first == "nodeState") std::memcpy(state, x.second.data(), sizeof(int32_t) * (size_t)nnode * nsite);
     for (auto& x : out.vecs)
-        if (x.first == "edgeLen") std::memcpy(len, x.second.v.data(), sizeof(uint32_t) * nedge);
+        if (x.first == "edgeLen") std::memcpy(len, x.second.data(), sizeof(uint32_t) * nedge);
     return 0;
 }
 
@@ -51,5 +51,6 @@ extern "C" int ref_node_des_big(uint32_t ntip, uint32_t nnode, uint32_t nedge, c
     }
     Rcpp::IntegerVector out = nodeDesBig(e, (int)nnode, (int)ntip, std::string(path), 8192, header != 0);
     for (int i = 0; i < out.size(); i++) sizes_out[i] = out(i);
+    r_alloc_release();
     return out.size();
 }

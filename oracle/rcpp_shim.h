@@ -1,34 +1,62 @@
-// Minimal stand-ins for the Rcpp types used by the reference's parsimony
-// functions, so that those functions compile as plain C++ for the oracle
-// pin (test infrastructure, see oracle/Makefile target ref).  Matrices are
-// column-major like R's; only the members those functions use exist.
+// Minimal stand-ins for the Rcpp types used by the reference's CPU functions
+// (src/functions.cpp), so that those functions compile as plain C++ for the
+// oracle pin and the timed CPU baseline (test infrastructure, see the
+// oracle/Makefile target ref).  Only the members those functions use exist.
+//
+// The copy rules follow Rcpp's: a vector or matrix is a handle, so copying
+// one (passing it by value, assigning it) shares its storage; converting a
+// matrix column to a vector makes a new vector; assigning a vector or another
+// column to a matrix column copies the elements.  Matrices are column-major
+// like R's.  Element access is unchecked (Rcpp's operator() on vectors checks
+// bounds), so the functions run at least as fast here as under R.
 #pragma once
 #include <cstdio>
 #include <cstdlib>
+#include <memory>
 #include <string>
 #include <vector>
 
-// R's transient allocator and printf (the test process frees at exit)
-inline char* R_alloc(size_t n, int size) { return static_cast<char*>(std::calloc(n ? n : 1, (size_t)size)); }
+// R's transient allocator: memory lives until the wrapper that called the
+// function releases it, as R releases it when the .Call returns.
+inline std::vector<void*>& r_alloc_list() {
+    thread_local std::vector<void*> l;
+    return l;
+}
+inline char* R_alloc(size_t n, int size) {
+    void* p = std::calloc(n ? n : 1, (size_t)size);
+    r_alloc_list().push_back(p);
+    return static_cast<char*>(p);
+}
+inline void r_alloc_release() {
+    for (void* p : r_alloc_list()) std::free(p);
+    r_alloc_list().clear();
+}
 #define Rprintf std::printf
 
 namespace Rcpp {
 
-struct IntegerVector {
-    std::vector<int> v;
-    IntegerVector(int n = 0) : v((size_t)n, 0) {}
-    int& operator()(int i) { return v[(size_t)i]; }
-    int operator()(int i) const { return v[(size_t)i]; }
-    int& operator[](int i) { return v[(size_t)i]; }
-    int size() const { return (int)v.size(); }
-    void fill(int x) { for (auto& e : v) e = x; }
+template <class T>
+struct Vec {
+    std::shared_ptr<std::vector<T>> s;
+    Vec(int n = 0) : s(std::make_shared<std::vector<T>>((size_t)n, T())) {}
+    T& operator()(int i) const { return (*s)[(size_t)i]; }
+    T& operator[](size_t i) const { return (*s)[i]; }
+    int size() const { return (int)s->size(); }
+    void fill(T x) const { for (auto& e : *s) e = x; }
+    T* data() const { return s->data(); }
 };
 
-struct LogicalVector {
-    std::vector<int> v;
-    LogicalVector(int n = 0) : v((size_t)n, 0) {}
-    int& operator()(int i) { return v[(size_t)i]; }
-    void fill(bool x) { for (auto& e : v) e = x ? 1 : 0; }
+struct IntegerVector : Vec<int> {
+    using Vec<int>::Vec;
+};
+
+struct NumericVector : Vec<double> {
+    using Vec<double>::Vec;
+};
+
+struct LogicalVector : Vec<int> {
+    using Vec<int>::Vec;
+    void fill(bool x) const { Vec<int>::fill(x ? 1 : 0); }
 };
 
 struct MatrixColumn {
@@ -36,24 +64,41 @@ struct MatrixColumn {
     int n;
     operator IntegerVector() const {
         IntegerVector r(n);
-        for (int i = 0; i < n; i++) r.v[(size_t)i] = p[i];
+        for (int i = 0; i < n; i++) r[(size_t)i] = p[i];
         return r;
     }
     MatrixColumn& operator=(const IntegerVector& x) {
-        for (int i = 0; i < n; i++) p[i] = x.v[(size_t)i];
+        for (int i = 0; i < n; i++) p[i] = x[(size_t)i];
         return *this;
     }
+    MatrixColumn& operator=(const MatrixColumn& x) {
+        if (p != x.p)
+            for (int i = 0; i < n; i++) p[i] = x.p[i];
+        return *this;
+    }
+    MatrixColumn(int* p_, int n_) : p(p_), n(n_) {}
+    MatrixColumn(const MatrixColumn&) = default;
 };
 
-struct IntegerMatrix {
+template <class T>
+struct Mat {
     int nr = 0, nc = 0;
-    std::vector<int> v;
-    IntegerMatrix(int r = 0, int c = 0) : nr(r), nc(c), v((size_t)r * c, 0) {}
-    int& operator()(int i, int j) { return v[(size_t)i + (size_t)j * nr]; }
+    std::shared_ptr<std::vector<T>> s;
+    Mat(int r = 0, int c = 0) : nr(r), nc(c), s(std::make_shared<std::vector<T>>((size_t)r * c, T())) {}
+    T& operator()(int i, int j) const { return (*s)[(size_t)i + (size_t)j * nr]; }
     int nrow() const { return nr; }
     int ncol() const { return nc; }
-    void fill(int x) { for (auto& e : v) e = x; }
-    MatrixColumn column(int j) { return MatrixColumn{v.data() + (size_t)j * nr, nr}; }
+    void fill(T x) const { for (auto& e : *s) e = x; }
+    T* data() const { return s->data(); }
+};
+
+struct IntegerMatrix : Mat<int> {
+    using Mat<int>::Mat;
+    MatrixColumn column(int j) const { return MatrixColumn(s->data() + (size_t)j * nr, nr); }
+};
+
+struct NumericMatrix : Mat<double> {
+    using Mat<double>::Mat;
 };
 
 template <class T>
