@@ -318,7 +318,13 @@ def blopt_suite(L):
                            "adjoint_evaluations": adj["evaluations"], "adjoint_loglik": adj["loglik_end"],
                            "central_diff_s": fd["seconds"], "central_diff_evaluations": fd["evaluations"],
                            "central_diff_loglik": fd["loglik_end"], "speedup": fd["seconds"] / adj["seconds"],
-                           "central_diff_within_1e-6": rel <= 1e-6, "rel_loglik_gap": rel}}
+                           "target": "log L within 1e-6 (relative) of the FP64 optimum; the adjoint result is "
+                                     "checked against it in FP64 by tests/test_felsenstein_gpu.py",
+                           "central_diff_gap_to_adjoint": (adj["loglik_end"] - fd["loglik_end"]) / abs(adj["loglik_end"]),
+                           "central_diff_reached_target": rel <= 1e-6,
+                           "speedup_kind": ("time to the target" if rel <= 1e-6 else
+                                            "lower bound: the central-difference run stops short of the target "
+                                            "(binary32 differences), so its whole run time is counted")}}
 
 
 def _timed(fn, reps=1):

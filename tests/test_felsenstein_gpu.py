@@ -156,3 +156,37 @@ def test_resample_columns_matches_gather(gpu_lib):
     exp[:, :41] = b[:, idx]
     assert np.array_equal(out.view(np.uint8).reshape(37, -1)[:, :41], exp[:, :41])
     assert np.all(out.view(np.uint8).reshape(37, -1)[:, 41:] == 0)
+
+
+def _fp64_optimum_from(f_and_g, t_start):
+    from scipy.optimize import minimize
+
+    def fun(x):
+        ll, g = f_and_g(np.exp(x))
+        return -ll, -g * np.exp(x)
+
+    r = minimize(fun, np.log(np.maximum(t_start, 1e-8)), jac=True, method="L-BFGS-B",
+                 bounds=[(np.log(1e-8), np.log(10.0))] * len(t_start),
+                 options=dict(maxiter=2000, ftol=1e-15, gtol=1e-10))
+    return -r.fun
+
+
+def test_benchmark_small_case_reaches_fp64_optimum(gpu_lib):
+    """The 128-tip x 2,000-site HKY85 case the adjoint is timed against central
+    differences on: the adjoint result, evaluated in FP64, is within 1e-6
+    (relative) of the FP64 optimum; the central-difference result is not
+    better.  The FP64 optimum is refined by L-BFGS-B from the better of the
+    two results."""
+    codes, par, ch, _ = _hky_case(128, 2000, 14, mean_bl=0.01)
+    e = _edge(par, ch)
+    t0 = np.full(2 * 128 - 2, 0.01)
+    kw = dict(kappa=4.0, pi=PI, rel_tol=1e-9, max_iter=1000)
+    ta, sa = gpu_lib.felsenstein_optimize(e, t0, codes, **kw)
+    tf, sf = gpu_lib.felsenstein_optimize(e, t0, codes, gradient="central_diff", **kw)
+    f = lambda t, grad=False: F.loglik_hky85(128, par, ch, t, codes, None, 4.0, PI, grad=grad)  # noqa: E731
+    la, lf = f(ta), f(tf)
+    best = _fp64_optimum_from(lambda t: f(t, True), ta if la >= lf else tf)
+    best = max(best, la, lf)
+    assert abs(la - best) <= 1e-6 * abs(best)
+    assert lf <= la + 1e-7 * abs(la)
+    assert abs(sa["loglik_end"] - la) <= LL_RTOL * abs(la)
