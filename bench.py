@@ -405,6 +405,27 @@ def rows_suite(L, nthreads):
                                            "mean_normalised_distance": float(np.mean(ymin / np.maximum(ysize, 1))),
                                            "cpu_sample": f"first {sub} rows of each", "cpu_s_sample": t_ct},
         "cpu_cores": nthreads}
+    # cal.abs: transfer support of the C2 join tree's clades over join trees of
+    # column-resampled copies of the matrix (approximateCompare2_AVX2 per tree)
+    nq = 100
+    rng = np.random.default_rng(29)
+    bits = np.unpackbits(words.view(np.uint8), axis=1, bitorder="little")[:, :512]
+    qtrees = []
+    for _ in range(nq):
+        wb = np.ascontiguousarray(np.packbits(bits[:, rng.integers(0, 512, 512)], axis=1, bitorder="little"))
+        qe, _, _ = L.join_bit(wb.view(np.uint32), None, 1)
+        qtrees.append(qe)
+    (sup, nsz), t_ca = _timed(lambda: L.cal_abs(bedge, 10_000, qtrees, threshold=0.05), reps=3)
+    res["C2_binary"]["cal_abs"] = {"query_trees": nq, "gpu_s": t_ca, "mean_support": float(sup[1:].mean())}
+    if twin:
+        rows1, _ = O.node_des(bedge, 10_000)
+        t0 = time.perf_counter()
+        tdis, bad = T.approx_compare_many(rows1, 10_000, bedge, qtrees, nthreads, threshold=float(np.float32(0.1)))
+        t_tc = time.perf_counter() - t0
+        want = ((tdis.T / nsz[:, None].astype(np.float64)) <= 0.05).sum(axis=1) / nq
+        res["C2_binary"]["cal_abs"]["reference_cpu"] = {
+            "function": f"approximateCompare2_AVX2 (src/functions.cpp:5450-5600) per tree, {nthreads} threads",
+            "s": t_tc, "same_support_as_gpu": bool(bad == 0 and np.array_equal(want, sup))}
     # a20: parsimony change counts per edge (ancestralBitReverse) on the C2 join tree
     (pstate, plen), t_par = _timed(lambda: L.ancestral_bit(words, bedge), reps=3)
     t0 = time.perf_counter()

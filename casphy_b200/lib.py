@@ -109,6 +109,8 @@ def lib():
         L.casphy_fasta_encode.argtypes = [u32, u32, C.c_char_p, vp, C.POINTER(u32), vp, C.c_uint64]
         L.casphy_node_des.argtypes = [u32, u32, u32, _u32p, _u32p, _i32p]
         L.casphy_tip_merge.argtypes = [u32, _u32p, vp, C.c_double, _i32p]
+        L.casphy_approx_compare.argtypes = [u32, u32, _u32p, u32, _u32p, u32, vp, vp, u32, f32, vp, vp, _i32p]
+        L.casphy_cal_abs.argtypes = [u32, u32, _u32p, u32, vp, vp, C.c_double, vp, _i32p]
         if hasattr(L, "casphy_join_bit"):
             L.casphy_join_bit.argtypes = [u32, u32, _u32p, _f64p, C.c_int, _u32p, _u32p, C.POINTER(JoinStats)]
             L.casphy_join_bit_dev.argtypes = [u32, u32, vp, _f64p, C.c_int, _u32p, vp, C.POINTER(JoinStats), vp]
@@ -372,6 +374,50 @@ def node_des(edge, ntip, nnode=None):
     sizes = np.zeros(max(nnode - 1, 1), np.int32)
     _chk(lib().casphy_node_des(ntip, nnode, len(edge), edge.reshape(-1), rows, sizes), "casphy_node_des")
     return rows[: nnode - 1], sizes[: nnode - 1]
+
+
+def _query_trees(edges2):
+    es = [_u32(np.asarray(e)).reshape(-1, 2) for e in edges2]
+    off = np.zeros(len(es) + 1, np.uint64)
+    off[1:] = np.cumsum([len(e) for e in es])
+    flat = np.ascontiguousarray(np.concatenate(es) if es else np.zeros((1, 2), np.uint32), dtype=np.uint32)
+    return es, off, flat
+
+
+def approx_compare(clade_rows, ntip, edge1, edges2, cache_size=8192, threshold=0.1):
+    """approximateCompare2_AVX2 of each query tree (0-based cladewise edges)
+    against the reference tree (edge1, clade rows from node_des).  Returns
+    (ref2qry list of nnode1 x 2, qry2ref list of nnode2 x 3, status array)."""
+    clade = _u32(clade_rows)
+    nnode1 = clade.shape[0] + 1
+    e1 = _u32(edge1).reshape(-1, 2)
+    es, off, flat = _query_trees(edges2)
+    nt = len(es)
+    nn2 = [len(e) - ntip + 1 for e in es]
+    r = np.zeros((max(nt, 1), nnode1, 2), np.int32)
+    q = np.zeros((max(sum(nn2), 1), 3), np.int32)
+    status = np.zeros(max(nt, 1), np.int32)
+    _chk(lib().casphy_approx_compare(ntip, nnode1, clade.reshape(-1), len(e1), e1.reshape(-1), nt, off.ctypes.data,
+                                     flat.ctypes.data, int(cache_size), float(threshold), r.ctypes.data,
+                                     q.ctypes.data, status), "casphy_approx_compare")
+    qs, o = [], 0
+    for n in nn2:
+        qs.append(q[o:o + n].copy())
+        o += n
+    return [r[t].copy() for t in range(nt)], qs, status[:nt].copy()
+
+
+def cal_abs(edge1, ntip, edges2, threshold=0.05):
+    """cal.abs: (support, node_size) of every internal node of the reference
+    tree (0-based cladewise edges) over the query trees."""
+    e1 = _u32(edge1).reshape(-1, 2)
+    nnode1 = len(e1) - ntip + 1
+    es, off, flat = _query_trees(edges2)
+    sup = np.zeros(nnode1, np.float64)
+    size = np.zeros(nnode1, np.int32)
+    _chk(lib().casphy_cal_abs(ntip, len(e1), e1.reshape(-1), len(es), off.ctypes.data, flat.ctypes.data,
+                              float(threshold), sup.ctypes.data, size), "casphy_cal_abs")
+    return sup, size
 
 
 def fasta_encode(seqs):

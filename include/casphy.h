@@ -249,6 +249,37 @@ int casphy_node_des(uint32_t ntip, uint32_t nnode, uint32_t nedge, const uint32_
                     uint32_t *rows_out, int32_t *sizes_out);
 
 /*
+ * approximateCompare2_AVX2 (src/functions.cpp:5450-5600) for many query
+ * trees at once, as clade.support / cal.abs apply it over bootstrap trees
+ * (R/bootstrap_functions.R:34-57, :190-202).  Reference tree: edge1 (0-based
+ * (parent, child) pairs, tips 0..ntip-1, root ntip, nnode1 internal nodes)
+ * and its clade rows as casphy_node_des writes them ((nnode1-1) x nbin).
+ * Query tree t: edges2 + 2*edge_off[t], edge_off[t+1]-edge_off[t] edges in
+ * cladewise order over the same tips, nnode2_t = nedges - ntip + 1 internal
+ * nodes.  Outputs, the function's two matrices row by row: ref2qry[ntree *
+ * nnode1 * 2] (1-based query node, XOR distance) and qry2ref[sum nnode2_t *
+ * 3] (1-based reference node, distance, clade size), trees in order.
+ * status[t] = CASPHY_ERANGE where the function runs out of its cache_size
+ * open rows (it returns 0 to R then; that tree's rows are zero).
+ */
+int casphy_approx_compare(uint32_t ntip, uint32_t nnode1, const uint32_t *clade_rows, uint32_t nedge1,
+                          const uint32_t *edge1, uint32_t ntree, const uint64_t *edge_off, const uint32_t *edges2,
+                          uint32_t cache_size, float threshold, int32_t *ref2qry, int32_t *qry2ref,
+                          int32_t *status);
+
+/*
+ * cal.abs (R/bootstrap_functions.R:190-219): transfer support of every
+ * internal node of the reference tree (edge1, cladewise) over ntree query
+ * trees (as above): the fraction of trees whose approximateCompare2_AVX2
+ * distance (run at threshold + 0.05) over the node's size is at most
+ * threshold.  support[nnode1] and node_size[nnode1] are the two columns of
+ * its result (node order, root first).  CASPHY_ERANGE with "Run out of
+ * cache!" where nodeDesBig or the comparison runs out of its 8192 rows.
+ */
+int casphy_cal_abs(uint32_t ntip, uint32_t nedge1, const uint32_t *edge1, uint32_t ntree, const uint64_t *edge_off,
+                   const uint32_t *edges2, double threshold, double *support, int32_t *node_size);
+
+/*
  * tipMerge (cu/tipMerge.cu:130-461): categories of tips whose neighbour lists
  * overlap.  counts[ntip] and idx (the concatenated ascending lists) are the
  * .nNeighbor body and the .idx file of radiusNeighbor(DNA); member[ntip]

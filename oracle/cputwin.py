@@ -106,3 +106,57 @@ def radius_weighted_dna_rows(ints, radius, row0, row1, nthreads, weight=None):
     if rc:
         raise RuntimeError(f"ref_radius_weighted_dna_rows returned {rc}")
     return out[:, 0].copy(), out[:, 1:].copy()
+
+
+def _lib_ac():
+    L = lib()
+    if not getattr(L, "_ac", False):
+        P, u32, i32 = C.c_void_p, C.c_uint32, C.c_int
+        L.ref_approx_compare.argtypes = [u32, u32, u32, P, u32, P, u32, P, u32, i32, C.c_float, P, P]
+        L.ref_approx_compare.restype = i32
+        L.ref_approx_compare_many.argtypes = [u32, u32, u32, P, u32, P, u32, P, P, P, P, P, i32, C.c_float, i32,
+                                              P, P]
+        L.ref_approx_compare_many.restype = i32
+        L._ac = True
+    return L
+
+
+def approx_compare(clade_rows, ntip, edge1, edge2, nnode2=None, cache_size=8192, threshold=0.1):
+    """approximateCompare2_AVX2 of one query tree.  clade_rows: the reference
+    tree's nodeDesBig rows ((nnode1 - 1) x nbin, file order); edge1, edge2:
+    0-based (parent, child) pairs in cladewise order (tips 0.., root ntip).
+    Returns (ref2qry nnode1 x 2, qry2ref nnode2 x 3), 1-based nodes as R sees
+    them; raises when the function runs out of cache."""
+    clade = np.ascontiguousarray(clade_rows, dtype=np.int32)
+    nnode1 = clade.shape[0] + 1
+    nbin = clade.shape[1]
+    e1 = np.ascontiguousarray(np.asarray(edge1).reshape(-1, 2) + 1, dtype=np.int32)
+    e2 = np.ascontiguousarray(np.asarray(edge2).reshape(-1, 2) + 1, dtype=np.int32)
+    nnode2 = int(e2.max()) - ntip if nnode2 is None else int(nnode2)
+    r = np.zeros((2, nnode1), np.int32)
+    q = np.zeros((3, nnode2), np.int32)
+    rc = _lib_ac().ref_approx_compare(ntip, nnode1, nbin, _p(clade), len(e1), _p(e1), len(e2), _p(e2), nnode2,
+                                      int(cache_size), float(threshold), _p(r), _p(q))
+    if rc:
+        raise RuntimeError("approximateCompare2_AVX2 ran out of cache")
+    return r.T.copy(), q.T.copy()
+
+
+def approx_compare_many(clade_rows, ntip, edge1, edges2, nthreads, cache_size=8192, threshold=0.1):
+    """approx_compare over a list of query trees, trees spread over threads.
+    Returns (ref2qry distances ntree x nnode1, number of trees out of cache)."""
+    clade = np.ascontiguousarray(clade_rows, dtype=np.int32)
+    nnode1 = clade.shape[0] + 1
+    nbin = clade.shape[1]
+    e1 = np.ascontiguousarray(np.asarray(edge1).reshape(-1, 2) + 1, dtype=np.int32)
+    es = [np.asarray(e).reshape(-1, 2) for e in edges2]
+    ne = np.array([len(e) for e in es], np.uint32)
+    nn = np.array([int(e.max()) + 1 - ntip for e in es], np.uint32)
+    off = np.zeros(len(es), np.uint64)
+    off[1:] = np.cumsum(ne[:-1].astype(np.uint64))
+    allE = np.ascontiguousarray(np.concatenate(es) + 1, dtype=np.int32)
+    r = np.zeros((len(es), 2, nnode1), np.int32)
+    bad = _lib_ac().ref_approx_compare_many(ntip, nnode1, nbin, _p(clade), len(e1), _p(e1), len(es), _p(off),
+                                            _p(ne), _p(allE), _p(nn), None, int(cache_size), float(threshold),
+                                            int(nthreads), _p(r), None)
+    return r[:, 1, :].copy(), int(bad)

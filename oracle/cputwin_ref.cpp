@@ -95,3 +95,71 @@ extern "C" int ref_radius_weighted_dna_rows(uint32_t nseq, uint32_t nint, const 
     }
     return 0;
 }
+
+// approximateCompare2_AVX2 (src/functions.cpp:5450-5600) for one query tree.
+// clade: the reference tree's clade matrix as nodeDesBig writes it without
+// header (nbin x (nnode1 - 1) column-major, column k = node ntip+nnode1-1-k,
+// 0-based).  edge1, edge2: 1-based (parent, child) pairs in ape's cladewise
+// order.  ref2qry: nnode1 x 2 column-major (node, distance); qry2ref:
+// nnode2 x 3 column-major (node, distance, size).  Returns 1 when the
+// function ran out of cache (it returns 0 to R then), else 0.
+static int approx_compare_one(uint32_t ntip, uint32_t nnode1, uint32_t nbin, int32_t* clade, const Rcpp::IntegerMatrix& e1,
+                              uint32_t nedge2, const int32_t* edge2, uint32_t nnode2, int cacheSize, float threshold,
+                              int32_t* ref2qry, int32_t* qry2ref) {
+    BigMatrix bm;
+    bm.nr = nbin;
+    bm.nc = nnode1 - 1;
+    bm.d = clade;
+    Rcpp::IntegerMatrix e2((int)nedge2, 2);
+    for (uint32_t i = 0; i < nedge2; i++) {
+        e2(i, 0) = edge2[2 * i];
+        e2(i, 1) = edge2[2 * i + 1];
+    }
+    Rcpp::List out = approximateCompare2_AVX2(static_cast<SEXP>(&bm), (int)ntip, e1, e2, (int)nnode2, cacheSize,
+                                              threshold);
+    if (out.null) return 1;
+    for (auto& x : out.mats) {
+        if (x.first == "ref2qry" && ref2qry) std::memcpy(ref2qry, x.second.data(), sizeof(int32_t) * 2 * (size_t)nnode1);
+        if (x.first == "qry2ref" && qry2ref) std::memcpy(qry2ref, x.second.data(), sizeof(int32_t) * 3 * (size_t)nnode2);
+    }
+    return 0;
+}
+
+static Rcpp::IntegerMatrix edge_matrix(uint32_t nedge, const int32_t* edge) {
+    Rcpp::IntegerMatrix e((int)nedge, 2);
+    for (uint32_t i = 0; i < nedge; i++) {
+        e(i, 0) = edge[2 * i];
+        e(i, 1) = edge[2 * i + 1];
+    }
+    return e;
+}
+
+extern "C" int ref_approx_compare(uint32_t ntip, uint32_t nnode1, uint32_t nbin, int32_t* clade, uint32_t nedge1,
+                                  const int32_t* edge1, uint32_t nedge2, const int32_t* edge2, uint32_t nnode2,
+                                  int cacheSize, float threshold, int32_t* ref2qry, int32_t* qry2ref) {
+    return approx_compare_one(ntip, nnode1, nbin, clade, edge_matrix(nedge1, edge1), nedge2, edge2, nnode2,
+                              cacheSize, threshold, ref2qry, qry2ref);
+}
+
+// The query trees of cal.abs / clade.support (R/bootstrap_functions.R:34-57,
+// :190-202), spread over nthreads threads as parLapply spreads them over a
+// fork cluster.  Tree t: edges2 + 2 off2[t], nedge2[t] edges, nnode2[t]
+// internal nodes; outputs at ref2qry + 2 nnode1 t and qry2ref + 3 qoff[t].
+// Returns the number of trees that ran out of cache.
+extern "C" int ref_approx_compare_many(uint32_t ntip, uint32_t nnode1, uint32_t nbin, int32_t* clade,
+                                       uint32_t nedge1, const int32_t* edge1, uint32_t ntree, const uint64_t* off2,
+                                       const uint32_t* nedge2, const int32_t* edges2, const uint32_t* nnode2,
+                                       const uint64_t* qoff, int cacheSize, float threshold, int nthreads,
+                                       int32_t* ref2qry, int32_t* qry2ref) {
+    int bad = 0;
+#pragma omp parallel num_threads(nthreads) reduction(+ : bad)
+    {
+        const Rcpp::IntegerMatrix e1 = edge_matrix(nedge1, edge1);
+#pragma omp for schedule(dynamic, 1)
+        for (long t = 0; t < (long)ntree; t++)
+            bad += approx_compare_one(ntip, nnode1, nbin, clade, e1, nedge2[t], edges2 + 2 * off2[t], nnode2[t],
+                                      cacheSize, threshold, ref2qry + 2 * (size_t)nnode1 * t,
+                                      qry2ref ? qry2ref + 3 * qoff[t] : nullptr);
+    }
+    return bad;
+}

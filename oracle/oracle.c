@@ -1008,3 +1008,125 @@ int oracle_node_des(uint32_t ntip, uint32_t nnode, uint32_t nedge, const uint32_
     free(bits); free(size); free(open);
     return st;
 }
+
+/* ------------------------------------------------------------------------
+ * approximateCompare2_AVX2 (src/functions.cpp:5450-5600).  The query tree's
+ * edges are visited in reverse order.  A tip child sets its bit in the
+ * parent's open row and its stop node becomes its parent in the reference
+ * tree.  An internal child d ORs its row into the parent's, then from the
+ * stop node of each of its children (in edge order) walks up the reference
+ * tree while the node is not the root and the previous comparison left at
+ * most size(d) * threshold tips outside d (binary32 product): at each node it
+ * takes the XOR distance to d and the count of the node's tips missing
+ * from d, lowers the node's best distance (ties go to the later d) and d's
+ * best distance (ties go to the later node, which also becomes d's stop
+ * node).  d's stop node starts as its first child's.  The reference keeps
+ * the open rows in cacheSize slots and stops when more are needed. */
+int oracle_approx_compare(uint32_t ntip, uint32_t nnode1, uint32_t nbin, const uint32_t *clade, uint32_t nedge1,
+                          const uint32_t *edge1, uint32_t nedge2, const uint32_t *edge2, uint32_t nnode2,
+                          uint32_t cacheSize, float threshold, int32_t *ref2qry, int32_t *qry2ref) {
+    if (!clade || !edge1 || !edge2 || !ref2qry || !qry2ref || ntip == 0 || nnode1 == 0 || nnode2 == 0 ||
+        nbin != ((ntip - 1) >> 5) + 1)
+        return ORACLE_EINVAL;
+    const u32 n1 = ntip + nnode1, n2 = ntip + nnode2;
+    int32_t *par1 = (int32_t *)malloc(sizeof(int32_t) * n1);
+    u32 *stop = (u32 *)malloc(sizeof(u32) * n2);
+    int32_t *size2 = (int32_t *)calloc(n2, sizeof(int32_t));
+    u32 *bits = (u32 *)calloc((size_t)nnode2 * nbin, sizeof(u32));
+    char *open = (char *)calloc(nnode2, 1);
+    u32 *kidOff = (u32 *)calloc(nnode2 + 1, sizeof(u32));
+    u32 *kids = (u32 *)malloc(sizeof(u32) * (nedge2 ? nedge2 : 1));
+    u32 *fill = (u32 *)calloc(nnode2, sizeof(u32));
+    int32_t *d1 = (int32_t *)malloc(sizeof(int32_t) * nnode1), *m1 = (int32_t *)calloc(nnode1, sizeof(int32_t));
+    int32_t *d2 = (int32_t *)malloc(sizeof(int32_t) * nnode2), *m2 = (int32_t *)calloc(nnode2, sizeof(int32_t));
+    int st = ORACLE_OK;
+    if (!par1 || !stop || !size2 || !bits || !open || !kidOff || !kids || !fill || !d1 || !m1 || !d2 || !m2) {
+        st = ORACLE_ENOMEM;
+        goto done;
+    }
+    for (u32 v = 0; v < n1; v++) par1[v] = -1;
+    for (u32 i = 0; i < nedge1; i++) {
+        if (edge1[2 * i] >= n1 || edge1[2 * i + 1] >= n1) { st = ORACLE_EINVAL; goto done; }
+        par1[edge1[2 * i + 1]] = (int32_t)edge1[2 * i];
+    }
+    for (u32 i = 0; i < nedge2; i++) {
+        const u32 a = edge2[2 * i], d = edge2[2 * i + 1];
+        if (a < ntip || a >= n2 || d >= n2) { st = ORACLE_EINVAL; goto done; }
+        kidOff[a - ntip + 1]++;
+    }
+    for (u32 i = 0; i < nnode2; i++) kidOff[i + 1] += kidOff[i];
+    for (u32 i = 0; i < nedge2; i++) {
+        const u32 ai = edge2[2 * i] - ntip;
+        kids[kidOff[ai] + fill[ai]++] = edge2[2 * i + 1];
+    }
+    for (u32 v = 0; v < n2; v++) stop[v] = ntip;
+    for (u32 i = 0; i < nnode1; i++) d1[i] = (int32_t)(2 * ntip);
+    for (u32 i = 0; i < nnode2; i++) d2[i] = (int32_t)(2 * ntip);
+    u32 nUse = 0;
+    for (long i = (long)nedge2 - 1; i >= 0; i--) {
+        const u32 a = edge2[2 * i], d = edge2[2 * i + 1], ai = a - ntip;
+        if (!open[ai]) {
+            if (nUse == cacheSize) { st = ORACLE_ERANGE; goto done; }
+            open[ai] = 1;
+            nUse++;
+        }
+        u32 *ra = bits + (size_t)ai * nbin;
+        if (d < ntip) {
+            size2[d] = 1;
+            size2[a]++;
+            ra[d >> 5] |= 1u << (d & 31);
+            stop[d] = (u32)par1[d];
+            continue;
+        }
+        const u32 di = d - ntip;
+        const u32 *rd = bits + (size_t)di * nbin;
+        size2[a] += size2[d];
+        for (u32 x = 0; x < nbin; x++) ra[x] |= rd[x];
+        const u32 k0 = kidOff[di], k1 = kidOff[di + 1];
+        stop[d] = stop[kids[k0]];
+        int32_t best = (int32_t)(2 * ntip);
+        const float lim = (float)size2[d] * threshold;
+        for (u32 k = k0; k < k1; k++) {
+            u32 cur = stop[kids[k]];
+            int32_t nLarger = 0;
+            while (cur > ntip && (float)nLarger <= lim) {
+                const u32 t = nnode1 - 1 - (cur - ntip);
+                const u32 *rc = clade + (size_t)t * nbin;
+                int32_t xr = 0;
+                nLarger = 0;
+                for (u32 x = 0; x < nbin; x++) {
+                    xr += __builtin_popcount(rc[x] ^ rd[x]);
+                    nLarger += __builtin_popcount(rc[x] & ~rd[x]);
+                }
+                if (d1[t] >= xr) { d1[t] = xr; m1[t] = (int32_t)d + 1; }
+                if (best >= xr) {
+                    best = xr;
+                    stop[d] = cur;
+                    d2[di] = xr;
+                    m2[di] = (int32_t)cur + 1;
+                }
+                cur = (u32)par1[cur];
+            }
+        }
+        memset(bits + (size_t)di * nbin, 0, sizeof(u32) * nbin);
+        open[di] = 0;
+        nUse--;
+    }
+    ref2qry[0] = (int32_t)ntip + 1;
+    ref2qry[1] = 0;
+    for (u32 i = 1; i < nnode1; i++) {
+        ref2qry[2 * i] = m1[nnode1 - 1 - i];
+        ref2qry[2 * i + 1] = d1[nnode1 - 1 - i];
+    }
+    for (u32 i = 0; i < nnode2; i++) {
+        qry2ref[3 * i] = m2[i];
+        qry2ref[3 * i + 1] = d2[i];
+        qry2ref[3 * i + 2] = size2[ntip + i];
+    }
+    qry2ref[0] = (int32_t)ntip + 1;
+    qry2ref[1] = 0;
+done:
+    free(par1); free(stop); free(size2); free(bits); free(open); free(kidOff); free(kids); free(fill);
+    free(d1); free(m1); free(d2); free(m2);
+    return st;
+}

@@ -117,6 +117,18 @@ int oracle_node_des(uint32_t ntip, uint32_t nnode, uint32_t nedge, const uint32_
 int oracle_tip_merge(uint32_t ntip, const uint32_t *counts, const uint32_t *idx, double pShared,
                      int32_t *member_out);
 
+/* approximateCompare2_AVX2 (src/functions.cpp:5450-5600): transfer-style
+ * matching of the clades of a query tree (edge2) against those of a
+ * reference tree (edge1, clade rows as nodeDesBig writes them: row k = node
+ * ntip+nnode1-1-k).  Edges are 0-based (parent, child) pairs in cladewise
+ * order, tips 0..ntip-1, root ntip.  ref2qry: nnode1 x 2 row-major (1-based
+ * node of the query tree, distance), qry2ref: nnode2 x 3 row-major (1-based
+ * node of the reference tree, distance, size).  Returns ORACLE_ERANGE where
+ * the reference runs out of its cacheSize open rows. */
+int oracle_approx_compare(uint32_t ntip, uint32_t nnode1, uint32_t nbin, const uint32_t *clade, uint32_t nedge1,
+                          const uint32_t *edge1, uint32_t nedge2, const uint32_t *edge2, uint32_t nnode2,
+                          uint32_t cacheSize, float threshold, int32_t *ref2qry, int32_t *qry2ref);
+
 #ifdef __cplusplus
 }
 #endif

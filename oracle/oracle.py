@@ -216,3 +216,24 @@ def node_des(edge, ntip, nnode=None):
                                np.ascontiguousarray(edge.reshape(-1)).ctypes.data_as(C.c_void_p),
                                rows.ctypes.data_as(C.c_void_p), sizes.ctypes.data_as(C.c_void_p)), "node_des")
     return rows[: nnode - 1], sizes[: nnode - 1]
+
+
+def approx_compare(clade_rows, ntip, edge1, edge2, nnode2=None, cache_size=8192, threshold=0.1):
+    """approximateCompare2_AVX2 restated: clade_rows = the reference tree's
+    nodeDesBig rows ((nnode1 - 1) x nbin), edges 0-based cladewise.  Returns
+    (ref2qry nnode1 x 2, qry2ref nnode2 x 3) as the reference's matrices."""
+    clade = _u32(clade_rows)
+    nnode1, nbin = clade.shape[0] + 1, clade.shape[1]
+    e1 = _u32(np.asarray(edge1).reshape(-1, 2))
+    e2 = _u32(np.asarray(edge2).reshape(-1, 2))
+    nnode2 = int(e2.max()) + 1 - ntip if nnode2 is None else int(nnode2)
+    r = np.zeros((nnode1, 2), np.int32)
+    q = np.zeros((nnode2, 3), np.int32)
+    P = C.c_void_p
+    f = lib().oracle_approx_compare
+    f.argtypes = [C.c_uint32] * 3 + [P, C.c_uint32, P, C.c_uint32, P, C.c_uint32, C.c_uint32, C.c_float, P, P]
+    f.restype = C.c_int
+    _chk(f(ntip, nnode1, nbin, clade.ctypes.data_as(P), len(e1), e1.ctypes.data_as(P), len(e2),
+           e2.ctypes.data_as(P), nnode2, int(cache_size), float(threshold), r.ctypes.data_as(P),
+           q.ctypes.data_as(P)), "approx_compare")
+    return r, q

@@ -33,7 +33,34 @@ inline void r_alloc_release() {
 }
 #define Rprintf std::printf
 
+// An R object handle; here only a pointer to a BigMatrix or a null result.
+typedef void* SEXP;
+
+// bigmemory's matrix and column accessor (column-major int storage).
+struct BigMatrix {
+    long nr = 0, nc = 0;
+    int* d = nullptr;
+    long nrow() const { return nr; }
+    long ncol() const { return nc; }
+};
+
+template <class T>
+struct MatrixAccessor {
+    T* d;
+    long nr;
+    explicit MatrixAccessor(BigMatrix& m) : d(reinterpret_cast<T*>(m.d)), nr(m.nr) {}
+    T* operator[](long j) const { return d + j * nr; }
+};
+
 namespace Rcpp {
+
+template <class T>
+struct XPtr {
+    T* p;
+    explicit XPtr(SEXP s) : p(static_cast<T*>(s)) {}
+    T* operator->() const { return p; }
+    T& operator*() const { return *p; }
+};
 
 template <class T>
 struct Vec {
@@ -114,10 +141,19 @@ struct Named {
     NamedValue<T> operator=(const T& x) const { return NamedValue<T>{name, x}; }
 };
 
-// List::create keeps the matrices and vectors it is given, by name.
+// List::create keeps the matrices and vectors it is given, by name; a List
+// made from a null SEXP (a function's `return 0;`) is marked null.
 struct List {
     std::vector<std::pair<std::string, IntegerMatrix>> mats;
     std::vector<std::pair<std::string, IntegerVector>> vecs;
+    bool null = false;
+    List() = default;
+    List(SEXP s) : null(s == nullptr) {}
+    IntegerVector operator[](const char* name) const {
+        for (auto& x : vecs)
+            if (x.first == name) return x.second;
+        return IntegerVector(0);
+    }
     void add(const NamedValue<IntegerMatrix>& x) { mats.emplace_back(x.name, x.value); }
     void add(const NamedValue<IntegerVector>& x) { vecs.emplace_back(x.name, x.value); }
     template <class... A>
