@@ -19,6 +19,8 @@
 // reference (8192 rows) only decides whether the function runs out of cache;
 // the host replays it per tree.
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include <vector>
 
 #include "common.cuh"
@@ -113,6 +115,34 @@ __global__ void __launch_bounds__(kThreads) k_search(Trees T, const Item* __rest
     }
 }
 
+// Per query tree: the qry2ref rows before the search (root (ntip+1, 0),
+// others (0, 2 ntip), with the clade size; zero rows for a tree beyond the
+// cache) and the node of each visiting rank.
+__global__ void k_tree_init(u32 ntip, const u64* __restrict__ nodeBase, const u32* __restrict__ size,
+                            const u32* __restrict__ rank, const u32* __restrict__ ok, const u32* __restrict__ roots,
+                            u32* __restrict__ rankNode, int32_t* __restrict__ q2r) {
+    const u32 t = blockIdx.x;
+    const u64 nb = nodeBase[t], nn = nodeBase[t + 1] - nb;
+    const bool good = ok[t] != 0;
+    const u32 root = roots[t];
+    for (u64 i = threadIdx.x; i < nn; i += blockDim.x) {
+        int32_t* q = q2r + (nb + i) * 3;
+        const u32 sz = size[nb + i];
+        if (!good) {
+            q[0] = q[1] = q[2] = 0;
+        } else if (i == root) {
+            q[0] = (int32_t)ntip + 1;
+            q[1] = 0;
+            q[2] = (int32_t)sz;
+        } else {
+            q[0] = 0;
+            q[1] = (int32_t)(2u * ntip);
+            q[2] = (int32_t)sz;
+            rankNode[nb + rank[nb + i]] = (u32)i;
+        }
+    }
+}
+
 // ref2qry rows of every query tree from the keys: row 0 the root (ntip+1, 0),
 // row i the reference node ntip+i; untouched nodes keep (0, 2 ntip).
 __global__ void k_ref2qry(u32 ntree, u32 nnode1, u32 ntip, const unsigned long long* __restrict__ key,
@@ -184,6 +214,25 @@ __global__ void k_clade_rows(u32 ntip, u32 nbin, const u32* __restrict__ order, 
 namespace {
 
 inline u32 nblocks(u64 n, u32 t) { return (u32)((n + t - 1) / t); }
+
+// f(i) for i < n on up to 32 host threads (the per-tree host work).
+template <class F>
+void parallel_for(u32 n, F f) {
+    const u32 hw = std::max(1u, std::thread::hardware_concurrency());
+    const u32 nt = std::min(n, std::min(hw, 32u));
+    if (nt <= 1) {
+        for (u32 i = 0; i < n; i++) f(i);
+        return;
+    }
+    std::atomic<u32> next{0};
+    std::vector<std::thread> th;
+    th.reserve(nt);
+    for (u32 k = 0; k < nt; k++)
+        th.emplace_back([&] {
+            for (u32 i; (i = next.fetch_add(1)) < n;) f(i);
+        });
+    for (auto& t : th) t.join();
+}
 
 // One rooted tree as the reference's loops see it: children in edge order,
 // heights, sizes, the reverse-edge visiting rank of internal children and
@@ -354,7 +403,7 @@ int compare_all(u32 ntip, u32 nnode1, const std::vector<u32>& par1, const u32* r
         int32_t *r2q, *nodeSize;
         double* support;
         u64* nodeBase;
-        u32 *kidOff, *kid, *size, *rank, *rankNode, *stop, *rows, *ok;
+        u32 *kidOff, *kid, *size, *rank, *rankNode, *stop, *rows, *ok, *roots;
         int32_t* q2r;
         Item* items;
     };
@@ -380,6 +429,7 @@ int compare_all(u32 ntip, u32 nnode1, const std::vector<u32>& par1, const u32* r
         l.stop = c.take<u32>(mxNode);
         l.rows = c.take<u32>(mxNode * nbin);
         l.ok = c.take<u32>(mxTree);
+        l.roots = c.take<u32>(mxTree);
         l.q2r = c.take<int32_t>(mxNode * 3);
         l.items = c.take<Item>(mxItem);
         return l;
@@ -430,63 +480,65 @@ int compare_all(u32 ntip, u32 nnode1, const std::vector<u32>& par1, const u32* r
     u64 qOut = 0;  // qry2ref rows written so far
     for (const Group& g : groups) {
         const u32 nt = g.t1 - g.t0;
-        std::vector<u64> nodeBase(nt + 1, 0);
-        for (u32 t = 0; t < nt; t++) nodeBase[t + 1] = nodeBase[t] + Q[g.t0 + t].nnode;
-        const u64 nNode = nodeBase[nt];
-        std::vector<u32> kidOff(nNode + nt), kid(std::max<u64>(g.nKid, 1)), size(nNode), rank(nNode), rankNode(nNode),
-            ok(nt);
-        std::vector<int32_t> q0(nNode * 3, 0);
+        std::vector<u64> nodeBase(nt + 1, 0), kidBase(nt + 1, 0);
+        std::vector<u32> ok(nt), roots(nt);
         u32 H = 0;
-        u64 kb = 0;
         for (u32 t = 0; t < nt; t++) {
             const QTree& q = Q[g.t0 + t];
-            const u64 nb = nodeBase[t];
+            nodeBase[t + 1] = nodeBase[t] + q.nnode;
+            kidBase[t + 1] = kidBase[t] + q.kid.size();
+            ok[t] = q.cacheOk;
+            roots[t] = q.root - ntip;
+            if (q.cacheOk) H = std::max(H, q.height);
+        }
+        const u64 nNode = nodeBase[nt];
+        if (kidBase[nt] > 0xFFFFFFFFull) return CASPHY_ERANGE;
+        // the searched nodes (internal, not the root) counted per tree and
+        // height, then placed height by height
+        const u64 nh = (u64)H + 1;
+        std::vector<u64> cnt((u64)nt * nh, 0), pos((u64)nt * nh, 0), lvlOff(nh + 1, 0);
+        parallel_for(nt, [&](u32 t) {
+            const QTree& q = Q[g.t0 + t];
+            if (!q.cacheOk) return;
+            u64* c = cnt.data() + t * nh;
+            for (u32 i = 0; i < q.nnode; i++)
+                if (i != q.root - ntip) c[q.h[i]]++;
+        });
+        {
+            u64 o = 0;
+            for (u64 l = 0; l < nh; l++) {
+                lvlOff[l] = o;
+                for (u32 t = 0; t < nt; t++) {
+                    pos[t * nh + l] = o;
+                    o += cnt[t * nh + l];
+                }
+            }
+            lvlOff[nh] = o;
+        }
+        std::vector<u32> kidOff(nNode + nt), kid(std::max<u64>(kidBase[nt], 1)), size(nNode), rank(nNode);
+        std::vector<Item> items(std::max<u64>(lvlOff[nh], 1));
+        parallel_for(nt, [&](u32 t) {
+            const QTree& q = Q[g.t0 + t];
+            const u64 nb = nodeBase[t], kb = kidBase[t];
             for (u32 i = 0; i <= q.nnode; i++) kidOff[nb + t + i] = (u32)(kb + q.kidOff[i]);
             std::copy(q.kid.begin(), q.kid.end(), kid.begin() + kb);
             std::copy(q.size.begin(), q.size.end(), size.begin() + nb);
             std::copy(q.rank.begin(), q.rank.end(), rank.begin() + nb);
-            std::copy(q.rankNode.begin(), q.rankNode.end(), rankNode.begin() + nb);
-            kb += q.kid.size();
-            ok[t] = q.cacheOk;
-            if (!q.cacheOk) continue;
-            H = std::max(H, q.height);
-            for (u32 i = 0; i < q.nnode; i++) {
-                int32_t* r = q0.data() + (nb + i) * 3;
-                r[1] = (int32_t)(2 * ntip);
-                r[2] = (int32_t)q.size[i];
-            }
-            int32_t* r = q0.data() + (nb + (q.root - ntip)) * 3;
-            r[0] = (int32_t)ntip + 1;
-            r[1] = 0;
-        }
-        if (kb > 0xFFFFFFFFull) return CASPHY_ERANGE;
-        std::vector<u64> lvlOff(H + 2, 0);
-        for (u32 t = 0; t < nt; t++) {
-            const QTree& q = Q[g.t0 + t];
-            if (!q.cacheOk) continue;
+            if (!q.cacheOk) return;
+            u64* p = pos.data() + t * nh;
             for (u32 i = 0; i < q.nnode; i++)
-                if (i != q.root - ntip) lvlOff[q.h[i] + 1]++;
-        }
-        for (u32 l = 1; l <= H + 1; l++) lvlOff[l] += lvlOff[l - 1];
-        std::vector<Item> items(std::max<u64>(lvlOff[H + 1], 1));
-        {
-            std::vector<u64> pos(lvlOff.begin(), lvlOff.end() - 1);
-            for (u32 t = 0; t < nt; t++) {
-                const QTree& q = Q[g.t0 + t];
-                if (!q.cacheOk) continue;
-                for (u32 i = 0; i < q.nnode; i++)
-                    if (i != q.root - ntip) items[pos[q.h[i]]++] = Item{t, i};
-            }
-        }
+                if (i != q.root - ntip) items[p[q.h[i]]++] = Item{t, i};
+        });
         CASPHY_CUDA_TRY(cudaMemcpyAsync(L.nodeBase, nodeBase.data(), 8ull * (nt + 1), cudaMemcpyHostToDevice, st));
         CASPHY_CUDA_TRY(cudaMemcpyAsync(L.kidOff, kidOff.data(), 4ull * kidOff.size(), cudaMemcpyHostToDevice, st));
         CASPHY_CUDA_TRY(cudaMemcpyAsync(L.kid, kid.data(), 4ull * kid.size(), cudaMemcpyHostToDevice, st));
         CASPHY_CUDA_TRY(cudaMemcpyAsync(L.size, size.data(), 4ull * nNode, cudaMemcpyHostToDevice, st));
         CASPHY_CUDA_TRY(cudaMemcpyAsync(L.rank, rank.data(), 4ull * nNode, cudaMemcpyHostToDevice, st));
-        CASPHY_CUDA_TRY(cudaMemcpyAsync(L.rankNode, rankNode.data(), 4ull * nNode, cudaMemcpyHostToDevice, st));
         CASPHY_CUDA_TRY(cudaMemcpyAsync(L.ok, ok.data(), 4ull * nt, cudaMemcpyHostToDevice, st));
-        CASPHY_CUDA_TRY(cudaMemcpyAsync(L.q2r, q0.data(), 12ull * nNode, cudaMemcpyHostToDevice, st));
+        CASPHY_CUDA_TRY(cudaMemcpyAsync(L.roots, roots.data(), 4ull * nt, cudaMemcpyHostToDevice, st));
         CASPHY_CUDA_TRY(cudaMemcpyAsync(L.items, items.data(), sizeof(Item) * items.size(), cudaMemcpyHostToDevice, st));
+        k_tree_init<<<nt, 256, 0, st>>>(ntip, L.nodeBase, L.size, L.rank, L.ok, L.roots, L.rankNode, L.q2r);
+        const u32 H1 = H;
         Trees T;
         T.ntip = ntip;
         T.nbin = nbin;
@@ -503,9 +555,9 @@ int compare_all(u32 ntip, u32 nnode1, const std::vector<u32>& par1, const u32* r
         T.q2r = L.q2r;
         T.key = L.key + (u64)g.t0 * nnode1;
         T.threshold = threshold;
-        for (u32 l = 1; l <= H; l++) {
-            const u64 cnt = lvlOff[l + 1] - lvlOff[l];
-            if (cnt) k_search<<<nblocks(cnt * 32, kThreads), kThreads, 0, st>>>(T, L.items + lvlOff[l], (u32)cnt);
+        for (u32 l = 1; l <= H1; l++) {
+            const u64 c = lvlOff[l + 1] - lvlOff[l];
+            if (c) k_search<<<nblocks(c * 32, kThreads), kThreads, 0, st>>>(T, L.items + lvlOff[l], (u32)c);
         }
         CASPHY_CUDA_TRY(cudaGetLastError());
         if (ref2qry)
@@ -533,14 +585,22 @@ int compare_all(u32 ntip, u32 nnode1, const std::vector<u32>& par1, const u32* r
 int parse_queries(u32 ntip, u32 ntree, const uint64_t* edge_off, const uint32_t* edges2, u32 cacheSize,
                   std::vector<QTree>& Q) {
     if (!edge_off || !edges2) return CASPHY_EINVAL;
-    Q.resize(ntree);
-    for (u32 t = 0; t < ntree; t++) {
+    for (u32 t = 0; t < ntree; t++)
         if (edge_off[t + 1] < edge_off[t] || edge_off[t + 1] - edge_off[t] > 0xFFFFFFFFull) return CASPHY_EINVAL;
-        const int rc = parse_tree(ntip, (u32)(edge_off[t + 1] - edge_off[t]), edges2 + 2 * edge_off[t], cacheSize,
-                                  Q[t], "approximateCompare: each query tree must be one rooted tree, edges in "
-                                        "cladewise order (a node's parent edge before its own edges)");
-        if (rc) return rc;
-    }
+    static const char* kMsg =
+        "approximateCompare: each query tree must be one rooted tree, edges in cladewise order (a node's parent "
+        "edge before its own edges)";
+    Q.resize(ntree);
+    std::vector<int> rcs(ntree, 0);
+    parallel_for(ntree, [&](u32 t) {
+        rcs[t] = parse_tree(ntip, (u32)(edge_off[t + 1] - edge_off[t]), edges2 + 2 * edge_off[t], cacheSize, Q[t],
+                            kMsg);
+    });
+    for (u32 t = 0; t < ntree; t++)
+        if (rcs[t]) {
+            casphy_set_last_error_msg(kMsg);  // the workers' messages stay on their threads
+            return rcs[t];
+        }
     return CASPHY_OK;
 }
 
