@@ -14,10 +14,11 @@ timed region.
 
 Under torchrun every rank builds its own replica of the tree (the greedy join
 has a sequential argmax dependence and does not shard); value = pair-scores of
-all ranks / max-over-ranks time.  --impl reference times the reference
-algorithm's CPU restatement (oracle/, "port": the reference's own CPU code
-needs Rcpp/bigmemory and is not buildable here) on a bounded sample on the
-host cores; under torchrun only rank 0 runs it.
+all ranks / max-over-ranks time.  --impl reference times the reference's
+own CPU join (greedyJoinEdge2 of src/functions.cpp, compiled from its source
+behind an Rcpp stand-in header into oracle/_ref/; the oracle port when that
+library was not built) on a bounded sample on the host cores; under torchrun
+only rank 0 runs it.
 """
 from __future__ import annotations
 
@@ -269,6 +270,8 @@ def bootstrap_suite(L, plain=True):
                         "of the full-data tree's clades at threshold 0.05",
             "batched_s": batched_s, "batched_device_ms": got["stats"]["total_ms"],
             "batched_phases": {k: got["stats"][k] for k in ("prep_ms", "join_ms", "transfer_ms")},
+            "join_groups": {k: got["stats"][k] for k in ("max_ctas_per_rep", "tuned", "join_longest_ms",
+                                                          "join_busy_ms")},
             "plain_s": plain_s, "plain": "casphy_join_bit + clade bitsets + casphy_transfer_dis per replicate",
             "speedup": plain_s / batched_s, "transfer_values_identical": same, "support_identical": sup_same}
 

@@ -16,10 +16,16 @@
 //     (weights as integer bit planes, as the single join's PLANES path).
 //  2. k_bs_init: the initial all-pairs scan of every replicate, tiles of all
 //     replicates drawn from one queue.
-//  3. k_bs_join: persistent, one CTA per replicate (largest first): the same
-//     join engine as the single join with nCTA = 1, so no grid barrier is
-//     needed; then the same CTA lays out the replicate tree's post-order
-//     (heavier child first, so a walk needs a stack of at most log2(n)+1).
+//  3. k_bs_join: persistent and cooperative; each replicate is joined by a
+//     group of G co-resident CTAs running the same join engine as the single
+//     join (G = 1 needs no barrier beyond the block's own).  G comes from a
+//     cost model of the replicate sizes whose constants are fitted to the
+//     per-replicate times of the previous call on the device (the
+//     autotuner): the largest replicates are split until the longest one no
+//     longer outlasts the even share of the work.  Groups run largest first,
+//     so every multi-CTA group forms in the first wave.  Member 0 then lays
+//     out the replicate tree's post-order (heavier child first, so a walk
+//     needs a stack of at most log2(n)+1).
 //  4. k_bs_transfer: one thread per (full-tree clade X, replicate).  X is the
 //     pre-order tip interval [lo, hi] of the full tree; walking the replicate
 //     tree's post-order with a stack of |X n Y| counts gives, for every
@@ -120,6 +126,7 @@ __global__ void k_bs_slot_init(const Rep* __restrict__ reps) {
                 c.slotNode[0][i] = kDead;
             }
         }
+        if (i < 16u * c.nCTA) c.flags[i] = 0u;  // barrier epochs of the replicate's group
         if (i < nnode) {
             c.node2slot[i] = i < ntip ? i : joinx::kNone;
             c.nodeDeath[i] = joinx::kNone;
@@ -160,10 +167,13 @@ __device__ void build_ops(const joinx::Common& c, const u32* __restrict__ rankOf
     }
 }
 
+// Work items (replicate, member) in queue order; the members of one
+// replicate are consecutive and multi-CTA replicates come first.
 template <int PATH>
-__global__ void __launch_bounds__(kThreads, 1) k_bs_join(const Rep* __restrict__ reps, const u32* __restrict__ order,
-                                                         u32 nrep, unsigned int* counter,
-                                                         const u32* __restrict__ rankOf) {
+__global__ void __launch_bounds__(kThreads, 1) k_bs_join(const Rep* __restrict__ reps,
+                                                         const u32* __restrict__ itemRep,
+                                                         const u32* __restrict__ itemMember, u32 nItem,
+                                                         unsigned int* counter, const u32* __restrict__ rankOf) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ u32 s_idx;
     for (;;) {
@@ -171,17 +181,23 @@ __global__ void __launch_bounds__(kThreads, 1) k_bs_join(const Rep* __restrict__
         __syncthreads();
         const u32 idx = s_idx;
         __syncthreads();
-        if (idx >= nrep) break;
-        const u32 r = order[idx];
+        if (idx >= nItem) break;
+        const u32 r = itemRep[idx], b = itemMember[idx];
         const joinx::Common c = reps[r].c;
         const typename BitModel<PATH>::Args m = reps[r].m;
-        if (c.ntip >= 2) joinx::join_run<BitModel<PATH>>(c, m, 0, smem);
+        const u64 t0 = globaltimer_ns();
+        if (c.ntip >= 2) joinx::join_run<BitModel<PATH>>(c, m, b, smem);
         __syncthreads();
+        if (b != 0) continue;
         int err = 0;
         if (threadIdx.x == 0) err = *(volatile int*)c.err;
         if (__syncthreads_or(err)) continue;
         build_ops(c, rankOf + reps[r].off, reps[r].ops, reinterpret_cast<u32*>(smem));
         __syncthreads();
+        if (threadIdx.x == 0) {
+            c.statsOut[6] = t0;
+            c.statsOut[7] = globaltimer_ns();
+        }
     }
 }
 
@@ -326,6 +342,98 @@ static int full_tree_intervals(u32 ntip, const u32* edge, std::vector<u32>& Xlo,
 
 }  // namespace casphy
 
+namespace casphy {
+namespace boot {
+
+// Cost of joining one replicate of n cells with G CTAs: its phases times
+// (alpha + beta * n / G + gamma when G > 1) -- a fixed per-phase part, the
+// scan of the slots each CTA owns, and the cross-CTA barrier.  The constants
+// start from a B200 estimate and are refitted on every call from the
+// measured replicate times, per device.
+struct Tune {
+    int measured = 0;
+    double alpha = 6.0;        // us per phase
+    double beta = 1.8e-3;      // us per phase per slot of a CTA
+    double gamma = 2.0;        // us per phase for the barrier of a group
+    double phasesPerTip = 1.7;
+};
+constexpr int kMaxDev = 64;
+constexpr u32 kMaxGroup = 8;
+Tune g_tune[kMaxDev];  // read and written under the device's workspace lock
+
+inline double cost_us(const Tune& T, u32 n, u32 G) {
+    return T.phasesPerTip * n * (T.alpha + T.beta * (double)n / G + (G > 1 ? T.gamma : 0.0));
+}
+
+// CTAs per replicate: split the replicate with the longest predicted join
+// while it outlasts the even share of all work over `slots` CTAs and a split
+// still shortens it.
+std::vector<u32> split_groups(const Tune& T, const std::vector<u32>& repN, u32 slots) {
+    const u32 nrep = (u32)repN.size();
+    std::vector<u32> G(nrep, 1);
+    std::vector<double> t(nrep);
+    double W = 0;
+    for (u32 r = 0; r < nrep; r++) {
+        t[r] = cost_us(T, repN[r], 1);
+        W += t[r];
+    }
+    u32 inGroups = 0;
+    for (;;) {
+        u32 rm = 0;
+        for (u32 r = 1; r < nrep; r++)
+            if (t[r] > t[rm]) rm = r;
+        if (t[rm] <= W / slots || G[rm] >= kMaxGroup || repN[rm] < 512) break;
+        const u32 g = G[rm] + 1, extra = G[rm] == 1 ? 2 : 1;
+        const double tn = cost_us(T, repN[rm], g);
+        if (tn >= t[rm] || inGroups + extra > slots) break;
+        W += tn * g - t[rm] * G[rm];
+        inGroups += extra;
+        G[rm] = g;
+        t[rm] = tn;
+    }
+    return G;
+}
+
+// Refit alpha and beta on the single-CTA replicates and gamma on the
+// groups, by least squares of the per-phase time; keeps the previous value
+// of a constant the measurements cannot pin down.
+void refit(Tune& T, const std::vector<u32>& repN, const std::vector<u32>& G, const std::vector<double>& us,
+           const std::vector<unsigned long long>& phases) {
+    double s1 = 0, sx = 0, sxx = 0, sy = 0, sxy = 0, ptot = 0, ntot = 0;
+    for (size_t r = 0; r < repN.size(); r++) {
+        if (phases[r] == 0 || us[r] <= 0) continue;
+        ptot += (double)phases[r];
+        ntot += repN[r];
+        if (G[r] != 1) continue;
+        const double x = repN[r], y = us[r] / (double)phases[r];
+        s1 += 1;
+        sx += x;
+        sxx += x * x;
+        sy += y;
+        sxy += x * y;
+    }
+    if (ntot > 0) T.phasesPerTip = ptot / ntot;
+    const double det = s1 * sxx - sx * sx;
+    if (s1 >= 8 && det > 0) {
+        const double b = (s1 * sxy - sx * sy) / det, a = (sy - b * sx) / s1;
+        if (a > 0 && b > 0) {
+            T.alpha = a;
+            T.beta = b;
+            T.measured = 1;
+        }
+    }
+    double gs = 0, gn = 0;
+    for (size_t r = 0; r < repN.size(); r++) {
+        if (G[r] == 1 || phases[r] == 0 || us[r] <= 0) continue;
+        gs += us[r] / (double)phases[r] - T.alpha - T.beta * repN[r] / G[r];
+        gn += 1;
+    }
+    if (gn > 0) T.gamma = std::max(0.1, gs / gn);
+}
+
+}  // namespace boot
+}  // namespace casphy
+
 extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t* words, const uint32_t* full_edge,
                                     uint32_t nrep, const uint32_t* rep_offsets, const uint32_t* rep_cells,
                                     const double* rep_weights, int ancestralType, double threshold,
@@ -389,6 +497,12 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
     DeviceScope ds;
     int nSM = 0;
     CASPHY_CUDA_TRY(cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, ds.dev));
+    // CTAs per replicate from the device's cost model (one join CTA per SM)
+    boot::Tune& tune = boot::g_tune[(ds.dev >= 0 && ds.dev < boot::kMaxDev) ? ds.dev : 0];
+    const int tunedBefore = tune.measured;
+    std::vector<u32> Gs = boot::split_groups(tune, repN, (u32)nSM);
+    u32 nItemAll = 0;
+    for (u32 g : Gs) nItemAll += g;
     struct RepBufs {
         u32 *planeMask, *nodeSeq, *nodeBis, *colT0, *colT1, *lm[6], *node2slot, *nodeDeath, *nodeSize, *rawEdge;
         u32 *eW, *eQ, *eLen, *pubCnt, *counts, *flags;
@@ -398,7 +512,7 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
         u64* chunkStart;
         unsigned long long* stats;
     };
-    auto rep_layout = [&](Carve& c, u32 n) {
+    auto rep_layout = [&](Carve& c, u32 n, u32 G) {
         RepBufs b;
         const u32 Sp = (n + 7u) & ~7u, nnode = 2 * n - 1, nChunks = (n + kCap - 1) / kCap;
         b.planeMask = c.take<u32>((size_t)P * nbin);
@@ -415,18 +529,18 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
         b.eQ = c.take<u32>((size_t)n * eStride);
         b.eLen = c.take<u32>(n);
         b.initKey = c.take<unsigned long long>(n);
-        b.pub = c.take<joinx::BlockRec>(4);
-        b.pubCnt = c.take<u32>(2);
-        b.partial = c.take<u64>(2);
-        b.counts = c.take<u32>(1);
-        b.flags = c.take<u32>(16);
+        b.pub = c.take<joinx::BlockRec>(4 * G);
+        b.pubCnt = c.take<u32>(2 * G);
+        b.partial = c.take<u64>(2 * G);
+        b.counts = c.take<u32>(G);
+        b.flags = c.take<u32>(16 * G);
         b.chunkStart = c.take<u64>(nChunks + 1);
         b.stats = c.take<unsigned long long>(8);
         return b;
     };
     struct Glob {
         Rep* reps;
-        u32 *repOfWarp, *cells, *words, *order, *rankOf, *sortedRank, *ops, *Xlo, *Xhi, *repN, *repOff, *repOpsOff;
+        u32 *repOfWarp, *cells, *words, *itemRep, *itemMember, *rankOf, *sortedRank, *ops, *Xlo, *Xhi, *repN, *repOff, *repOpsOff;
         u32 *ymin, *ysize, *support;
         u64* tileStart;
         unsigned long long* counter;
@@ -440,7 +554,8 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
         g.repOfWarp = c.take<u32>(totalTips);
         g.cells = c.take<u32>(totalTips);
         g.words = c.take<u32>((size_t)ntip * nbin);
-        g.order = c.take<u32>(nrep);
+        g.itemRep = c.take<u32>(nItemAll);
+        g.itemMember = c.take<u32>(nItemAll);
         g.rankOf = c.take<u32>(totalTips);
         g.sortedRank = c.take<u32>(totalTips);
         g.ops = c.take<u32>(repOpsOff[nrep]);
@@ -461,7 +576,7 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
     };
     Carve cv;
     glob_layout(cv);
-    for (u32 r = 0; r < nrep; r++) rep_layout(cv, repN[r]);
+    for (u32 r = 0; r < nrep; r++) rep_layout(cv, repN[r], Gs[r]);
     void* base = nullptr;
     if ((rc = ds.reserve(cv.off + 256, &base))) return rc;
     Carve c2;
@@ -472,7 +587,7 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
     std::vector<u64> tileStart(nrep + 1, 0), chunkAll;
     std::vector<std::vector<u64>> chunkStarts(nrep);
     for (u32 r = 0; r < nrep; r++) {
-        rb[r] = rep_layout(c2, repN[r]);
+        rb[r] = rep_layout(c2, repN[r], Gs[r]);
         const u32 n = repN[r], Sp = (n + 7u) & ~7u, nChunks = (n + kCap - 1) / kCap;
         auto& cs = chunkStarts[r];
         cs.assign(nChunks + 1, 0);
@@ -485,13 +600,13 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
         std::memset(&R, 0, sizeof(Rep));
         joinx::Common& c = R.c;
         const RepBufs& b = rb[r];
-        c.ntip = n; c.nnode = 2 * n - 1; c.nCTA = 1; c.align = 8;
+        c.ntip = n; c.nnode = 2 * n - 1; c.nCTA = Gs[r]; c.align = 8;
         c.lmOrd[0] = b.lm[0]; c.lmIdx[0] = b.lm[1]; c.slotNode[0] = b.lm[2];
         c.lmOrd[1] = b.lm[3]; c.lmIdx[1] = b.lm[4]; c.slotNode[1] = b.lm[5];
         c.node2slot = b.node2slot; c.nodeDeath = b.nodeDeath; c.nodeSize = b.nodeSize; c.rawEdge = b.rawEdge;
         c.pub = b.pub; c.pubCnt = b.pubCnt; c.partial = b.partial; c.counts = b.counts; c.flags = b.flags;
         c.err = G.errs + r; c.limitNs = 20ull * 1000 * 1000 * 1000; c.statsOut = b.stats;
-        c.Rmax = Sp; c.ordNeg1 = ORD_F32_NEG1; c.compactMin = 4096; c.compactQ8 = 192; c.bytesPerPairSite = 4000;
+        c.Rmax = ((n + Gs[r] - 1) / Gs[r] + 7u) & ~7u; c.ordNeg1 = ORD_F32_NEG1; c.compactMin = 4096; c.compactQ8 = 192; c.bytesPerPairSite = 4000;
         c.prof = nullptr;
         R.m = BitModel<PATH_PLANES>::Args{nbin, nbinP, P, ancestralType ? 1 : 0, b.planeMask, nullptr,
                                           b.nodeSeq, b.nodeBis, {b.colT0, b.colT1}};
@@ -518,11 +633,26 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
                 return CASPHY_EINVAL;
             }
     }
+    // join items: groups first, then the largest replicates first
     std::iota(order.begin(), order.end(), 0u);
-    std::stable_sort(order.begin(), order.end(), [&](u32 a, u32 b) { return repN[a] > repN[b]; });
-    // shared memory of the join CTA: engine + model, or the post-order offsets
+    std::stable_sort(order.begin(), order.end(),
+                     [&](u32 a, u32 b) { return Gs[a] != Gs[b] ? Gs[a] > Gs[b] : repN[a] > repN[b]; });
+    std::vector<u32> itemRep, itemMember;
+    u32 maxG = 1, inGroups = 0;
+    for (u32 r : order) {
+        for (u32 b = 0; b < Gs[r]; b++) {
+            itemRep.push_back(r);
+            itemMember.push_back(b);
+        }
+        maxG = std::max(maxG, Gs[r]);
+        if (Gs[r] > 1) inGroups += Gs[r];
+    }
+    const u32 nItem = (u32)itemRep.size();
+    // shared memory of a join CTA: engine + model, or the post-order offsets
     using M = BitModel<PATH_PLANES>;
-    const size_t smemJoin = M::engine_smem_bytes(1, (nmax + 7u) & ~7u) + M::model_smem_bytes(reps[order[0]].m);
+    size_t smemJoin = 0;
+    for (u32 r = 0; r < nrep; r++)
+        smemJoin = std::max(smemJoin, M::engine_smem_bytes(Gs[r], reps[r].c.Rmax) + M::model_smem_bytes(reps[r].m));
     const size_t smem = std::max(smemJoin, (size_t)4 * nmax);
     int maxSmem = 0;
     CASPHY_CUDA_TRY(cudaDeviceGetAttribute(&maxSmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ds.dev));
@@ -546,7 +676,8 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
     CASPHY_CUDA_TRY(up(G.repOfWarp, repOfWarp.data(), 4ull * totalTips));
     CASPHY_CUDA_TRY(up(G.cells, rep_cells, 4ull * totalTips));
     CASPHY_CUDA_TRY(up(G.words, words, 4ull * ntip * nbin));
-    CASPHY_CUDA_TRY(up(G.order, order.data(), 4ull * nrep));
+    CASPHY_CUDA_TRY(up(G.itemRep, itemRep.data(), 4ull * nItem));
+    CASPHY_CUDA_TRY(up(G.itemMember, itemMember.data(), 4ull * nItem));
     CASPHY_CUDA_TRY(up(G.rankOf, rankOf.data(), 4ull * totalTips));
     CASPHY_CUDA_TRY(up(G.sortedRank, sortedRank.data(), 4ull * totalTips));
     CASPHY_CUDA_TRY(up(G.Xlo, Xlo.data(), 4ull * nX));
@@ -574,8 +705,17 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
         int per = 0;
         CASPHY_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, kThreads, smem));
         if (per < 1) return CASPHY_ERANGE;
-        const u32 grid = std::min<u32>(nrep, (u32)(nSM * per));
-        k_bs_join<PATH_PLANES><<<grid, kThreads, smem, st>>>(G.reps, G.order, nrep, G.jcounter, G.rankOf);
+        const u32 grid = std::min<u32>(nItem, (u32)(nSM * per));
+        if (inGroups > grid) return CASPHY_EINTERNAL;  // a group could not form
+        // cooperative: every CTA is resident, so each group's members run together
+        const Rep* a0 = G.reps;
+        const u32* a1 = G.itemRep;
+        const u32* a2 = G.itemMember;
+        u32 a3 = nItem;
+        unsigned int* a4 = G.jcounter;
+        const u32* a5 = G.rankOf;
+        void* args[] = {(void*)&a0, (void*)&a1, (void*)&a2, (void*)&a3, (void*)&a4, (void*)&a5};
+        CASPHY_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, smem, st));
         launches++;
     }
     CASPHY_CUDA_TRY(cudaGetLastError());
@@ -607,7 +747,17 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
                                         cudaMemcpyDeviceToHost, st));
     CASPHY_CUDA_TRY(cudaStreamSynchronize(st));
     unsigned long long phases = 0;
-    for (u32 r = 0; r < nrep; r++) phases += hst[8 * r + 3];
+    std::vector<double> repUs(nrep, 0.0);
+    std::vector<unsigned long long> repPhases(nrep, 0);
+    double longest = 0, busy = 0;
+    for (u32 r = 0; r < nrep; r++) {
+        phases += hst[8 * r + 3];
+        repPhases[r] = hst[8 * r + 3];
+        const unsigned long long t0 = hst[8 * r + 6], t1 = hst[8 * r + 7];
+        repUs[r] = t1 > t0 ? (double)(t1 - t0) * 1e-3 : 0.0;
+        longest = std::max(longest, repUs[r]);
+        busy += repUs[r] * Gs[r];
+    }
     for (u32 r = 0; r < nrep; r++)
         if (errs[r]) {
             casphy_set_last_error_msg(errs[r] == CASPHY_ETIMEOUT ? "bootstrap: a replicate join timed out"
@@ -618,6 +768,7 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
         casphy_set_last_error_msg("bootstrap: post-order stack overflow");
         return CASPHY_EINTERNAL;
     }
+    boot::refit(tune, repN, Gs, repUs, repPhases);
     float tInit = 0, tJoin = 0, tX = 0, tAll = 0;
     cudaEventElapsedTime(&tInit, ev[0], ev[1]);
     cudaEventElapsedTime(&tJoin, ev[1], ev[2]);
@@ -634,6 +785,10 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
         s.total_ms = tAll;
         s.kernel_launches = launches;
         s.join_phases = phases;
+        s.max_ctas_per_rep = maxG;
+        s.tuned = tunedBefore ? 1u : 0u;
+        s.join_longest_ms = longest * 1e-3;
+        s.join_busy_ms = busy * 1e-3;
         *stats = s;
     }
     return CASPHY_OK;

@@ -67,13 +67,14 @@ __device__ __forceinline__ u64 globaltimer_ns() {
     return t;
 }
 
-// All-to-all flag barrier for a co-resident grid: CTA b publishes `epoch`
-// in its own flag; threads 0..nCTA-1 each wait for one CTA's flag.  Every
-// wait gives up after limit_ns and records CASPHY_ETIMEOUT.
-__device__ __forceinline__ int flag_barrier(u32* flags, u32 nCTA, u32 epoch, int* err, u64 limit_ns) {
+// All-to-all flag barrier for nCTA co-resident CTAs: CTA `self` (its index
+// among them) publishes `epoch` in its own flag; threads 0..nCTA-1 each wait
+// for one CTA's flag.  Every wait gives up after limit_ns and records
+// CASPHY_ETIMEOUT.
+__device__ __forceinline__ int flag_barrier(u32* flags, u32 nCTA, u32 self, u32 epoch, int* err, u64 limit_ns) {
     __syncthreads();
     if (nCTA == 1) return 0;  // one CTA: the block barrier orders its global accesses
-    if (threadIdx.x == 0) st_release_u32(flags + blockIdx.x * 16u, epoch);  // gpu-scope release, cumulative
+    if (threadIdx.x == 0) st_release_u32(flags + self * 16u, epoch);  // gpu-scope release, cumulative
     int fail = 0;
     if (threadIdx.x < nCTA) {
         const u32* f = flags + threadIdx.x * 16u;

@@ -518,7 +518,7 @@ __device__ bool grid_reduce(const Lb& a, double v[4], u32& epoch) {
             x = threadIdx.x == 3 ? fmax(x, red[i][threadIdx.x]) : x + red[i][threadIdx.x];
         a.part[((size_t)par * a.nCTA + blockIdx.x) * 4 + threadIdx.x] = x;
     }
-    if (flag_barrier(a.flags, a.nCTA, ++epoch, a.err, a.limitNs)) return false;
+    if (flag_barrier(a.flags, a.nCTA, blockIdx.x, ++epoch, a.err, a.limitNs)) return false;
     if (threadIdx.x < 4) {
         double x = 0.0;
         for (u32 i = 0; i < a.nCTA; i++) {

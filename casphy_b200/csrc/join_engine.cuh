@@ -325,7 +325,7 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
 
     own_top2(a, buf, rg, red, &s_rec, s_top, &cnt, wsum);
     publish(a, p, b, s_top, cnt);
-    if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
+    if (flag_barrier(a.flags, nCTA, b, ++p, a.err, a.limitNs)) goto out;
     load_table(a, p - 1, T);
 
     pf.mark(PROF_COMPACT);
@@ -337,7 +337,7 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
             publish(a, p, b, s_top, cnt);
             nRefresh++;
             pf.mark(PROF_POST);
-            if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
+            if (flag_barrier(a.flags, nCTA, b, ++p, a.err, a.limitNs)) goto out;
             pf.mark(PROF_BARRIER);
             load_table(a, p - 1, T);
             pf.mark(PROF_TABLE);
@@ -384,7 +384,7 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
             nStale++;
             nPairs += (a.ntip - k) - 1;
             algMilli += (unsigned long long)a.bytesPerPairSite * (u64)nE * ((a.ntip - k) - 1);
-            if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
+            if (flag_barrier(a.flags, nCTA, b, ++p, a.err, a.limitNs)) goto out;
             pf.mark(PROF_BARRIER);
             u64 pb = make_key(a.ordNeg1, 0u);
             for (u32 i = threadIdx.x; i < nCTA; i += kThreads) {
@@ -494,7 +494,7 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
         nPairs += (a.ntip - k - 1) - 1;
         algMilli += (unsigned long long)a.bytesPerPairSite * (u64)nE * ((a.ntip - k - 1) - 1);
         k++;
-        if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
+        if (flag_barrier(a.flags, nCTA, b, ++p, a.err, a.limitNs)) goto out;
         pf.mark(PROF_BARRIER);
         load_table(a, p - 1, T);
         pf.mark(PROF_TABLE);
@@ -510,7 +510,7 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
                 if (threadIdx.x == 0) a.counts[b] = v;
                 M::compact_prepare(m, ms, buf ^ 1u, make_range(alive, nCTA, b, a.align));
             }
-            if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
+            if (flag_barrier(a.flags, nCTA, b, ++p, a.err, a.limitNs)) goto out;
             if (threadIdx.x == 0) {
                 u32 off = 0, tot = 0;
                 for (u32 i = 0; i < nCTA; i++) {
@@ -535,14 +535,14 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
                     lmOrd_of(a, nb)[x] = a.ordNeg1;
                 }
             }
-            if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
+            if (flag_barrier(a.flags, nCTA, b, ++p, a.err, a.limitNs)) goto out;
             buf = nb;
             rg = make_range(Snew, nCTA, b, a.align);
             M::after_compact(m, ms, buf, rg);
             own_top2(a, buf, rg, red, &s_rec, s_top, &cnt, wsum);
             publish(a, p, b, s_top, cnt);
             nComp++;
-            if (flag_barrier(a.flags, nCTA, ++p, a.err, a.limitNs)) goto out;
+            if (flag_barrier(a.flags, nCTA, b, ++p, a.err, a.limitNs)) goto out;
             load_table(a, p - 1, T);
             pf.mark(PROF_COMPACT);
         }

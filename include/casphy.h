@@ -18,7 +18,7 @@
 extern "C" {
 #endif
 
-#define CASPHY_ABI_VERSION 1
+#define CASPHY_ABI_VERSION 2
 
 #define CASPHY_OK 0
 #define CASPHY_EINVAL 1     /* bad argument (size, weight, code out of range) */
@@ -336,6 +336,10 @@ typedef struct {
     double prep_ms, join_ms, transfer_ms, total_ms;  /* device times */
     uint64_t kernel_launches;
     uint64_t join_phases;                            /* summed over replicates */
+    uint32_t max_ctas_per_rep;                       /* CTAs the largest replicate's join used */
+    uint32_t tuned;                                  /* 1 when the split came from measured costs */
+    double join_longest_ms;                          /* longest single replicate join */
+    double join_busy_ms;                             /* replicate joins summed (CTA-time) */
 } casphy_bootstrap_stats;
 
 int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t *words, const uint32_t *full_edge,

@@ -38,7 +38,7 @@ def test_status_strings(lib):
     lib.casphy_strerror.restype = ctypes.c_char_p
     assert lib.casphy_strerror(0) == b"ok"
     assert lib.casphy_strerror(5) == b"device-side wait timed out"
-    assert lib.casphy_abi_version() == 1
+    assert lib.casphy_abi_version() == 2
 
 
 def test_no_gpu_is_an_error_not_a_fallback(lib):

@@ -47,6 +47,9 @@ def test_batched_equals_sequential(gpu_lib, ncell, nbin, nrep, nmin, nmax, seed)
     assert np.array_equal(got["ymin"], ymin)
     assert np.array_equal(got["ysize"], ysize)
     assert np.array_equal(got["support"], B.support_counts(ymin, ysize, thr))
+    if nmin >= 2000:
+        # few large replicates: each is joined by a group of CTAs
+        assert got["stats"]["max_ctas_per_rep"] > 1
 
 
 def test_oracle_pipeline_agrees_on_a_replicate(gpu_lib):
