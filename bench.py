@@ -40,7 +40,7 @@ UNIT = "pair-scores/s"
 WORKLOAD = dict(ncell=200_000, nsite=1024, depth=20, p_edit=0.02, nallele=256, zipf_s=1.3,
                 p_missing=0.15, seed=5)
 CPU_SAMPLE_CELLS = 5000      # oracle port (multi-threaded restatement of cu/joinEdgeIndel.cu)
-TWIN_SAMPLE_CELLS = 1024     # the reference's own CPU join (greedyJoinEdge2), about 10 s a tree
+TWIN_SAMPLE_CELLS = 1024     # the reference's own CPU join (greedyJoinEdge2), a few seconds a tree
 
 
 def workload_name():
@@ -271,7 +271,8 @@ def bootstrap_suite(L, plain=True):
             "batched_s": batched_s, "batched_device_ms": got["stats"]["total_ms"],
             "batched_phases": {k: got["stats"][k] for k in ("prep_ms", "join_ms", "transfer_ms")},
             "join_groups": {k: got["stats"][k] for k in ("max_ctas_per_rep", "tuned", "join_longest_ms",
-                                                          "join_busy_ms")},
+                                                          "join_busy_ms", "cost_alpha_us", "cost_beta_us",
+                                                          "cost_gamma_us")},
             "plain_s": plain_s, "plain": "casphy_join_bit + clade bitsets + casphy_transfer_dis per replicate",
             "speedup": plain_s / batched_s, "transfer_values_identical": same, "support_identical": sup_same}
 

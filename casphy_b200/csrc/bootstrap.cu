@@ -789,6 +789,9 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
         s.tuned = tunedBefore ? 1u : 0u;
         s.join_longest_ms = longest * 1e-3;
         s.join_busy_ms = busy * 1e-3;
+        s.cost_alpha_us = tune.alpha;
+        s.cost_beta_us = tune.beta;
+        s.cost_gamma_us = tune.gamma;
         *stats = s;
     }
     return CASPHY_OK;
