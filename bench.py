@@ -253,8 +253,10 @@ def bootstrap_suite(L, plain=True):
     t0 = time.perf_counter()
     got = L.bootstrap_bit(words, full_edge, off, cells, w, threshold=0.05)
     batched_s = time.perf_counter() - t0
+    groups = {k: got["stats"][k] for k in ("max_ctas_per_rep", "tuned", "join_longest_ms", "join_busy_ms",
+                                           "cost_alpha_us", "cost_beta_us", "cost_gamma_us")}
     if not plain:
-        return {"batched_s": batched_s, "batched_device_ms": got["stats"]["total_ms"]}
+        return {"batched_s": batched_s, "batched_device_ms": got["stats"]["total_ms"], "join_groups": groups}
     full_bits = B.clade_bits(full_edge, ncell, (ncell + 31) // 32)
     ymin = np.zeros_like(got["ymin"])
     ysize = np.zeros_like(got["ysize"])
@@ -270,9 +272,7 @@ def bootstrap_suite(L, plain=True):
                         "of the full-data tree's clades at threshold 0.05",
             "batched_s": batched_s, "batched_device_ms": got["stats"]["total_ms"],
             "batched_phases": {k: got["stats"][k] for k in ("prep_ms", "join_ms", "transfer_ms")},
-            "join_groups": {k: got["stats"][k] for k in ("max_ctas_per_rep", "tuned", "join_longest_ms",
-                                                          "join_busy_ms", "cost_alpha_us", "cost_beta_us",
-                                                          "cost_gamma_us")},
+            "join_groups": groups,
             "plain_s": plain_s, "plain": "casphy_join_bit + clade bitsets + casphy_transfer_dis per replicate",
             "speedup": plain_s / batched_s, "transfer_values_identical": same, "support_identical": sup_same}
 
