@@ -108,3 +108,29 @@ def test_gpu_matches_oracle_larger(gpu_lib):
         for q, e in enumerate(qs):
             a, b = O.approx_compare(rows, 2000, ref, e, threshold=thr)
             assert np.array_equal(r2q[q], a) and np.array_equal(q2r[q], b)
+
+
+@pytest.mark.gpu
+def test_gpu_rejects_malformed_trees(gpu_lib):
+    c = dict(_cases())["yule300"]
+    ref, rows = c["ref"], c["rows"]
+    q = _queries(c)[0]
+    # a query tree whose rows list a node's own edge before its parent edge
+    moved = q.copy()
+    i = int(np.nonzero(moved[:, 1] >= 301)[0][0])
+    j = int(np.nonzero(moved[:, 0] == moved[i, 1])[0][0])
+    moved[[i, j]] = moved[[j, i]]
+    with pytest.raises(gpu_lib.CasphyError) as err:
+        gpu_lib.approx_compare(rows, 300, ref, [moved])
+    assert err.value.status == 1
+    # a reference tree whose parent links form a cycle u -> v -> u
+    loop = ref.copy()
+    for k in np.nonzero(loop[:, 1] >= 301)[0]:
+        u = loop[k, 1]
+        m = np.nonzero((loop[:, 0] == u) & (loop[:, 1] >= 301))[0]
+        if len(m):
+            loop[k, 0] = loop[m[0], 1]
+            break
+    with pytest.raises(gpu_lib.CasphyError) as err:
+        gpu_lib.approx_compare(rows, 300, loop, [q])
+    assert err.value.status == 1
