@@ -8,7 +8,10 @@
 //   bit rows:  score = sum of w[b] over the bits set in both rows, binary32,
 //              ascending bit order (:33-41); unit weights -> popcount.
 //   DNA rows:  score = number of positions whose 4-bit IUPAC codes intersect
-//              (cu/radiusNeighborDNA.cu:55-87).
+//              (cu/radiusNeighborDNA.cu:55-87).  Here the codes are stored as
+//              four bit planes per block of 32 positions (plane j = bit j of
+//              the code), so one block costs popc((q0&c0)|(q1&c1)|(q2&c2)|
+//              (q3&c3)): nine integer operations for 32 positions.
 // Here the whole neighbour relation is produced as a bit matrix in one
 // tiled all-pairs launch (32 query rows per CTA in shared memory x 256
 // candidate rows, one warp ballot per 32 candidates), rows are counted, and
@@ -32,7 +35,7 @@ template <int MODE>
 __global__ void __launch_bounds__(kThreads) k_mask(const u32* __restrict__ col, u32 nwords, u32 ld, u32 ntip,
                                                    u32 qBegin, u32 qEnd, const float* __restrict__ wf, float radius,
                                                    u32 uradius, u32 maskWords, u32* __restrict__ mask) {
-    extern __shared__ u32 qs[];  // kQ x nwords query words (query rows qBegin..qEnd-1)
+    extern __shared__ __align__(16) u32 qs[];  // kQ x nwords query words (query rows qBegin..qEnd-1)
     const u32 q0 = qBegin + blockIdx.y * kQ;
     const u32 t = blockIdx.x * kThreads + threadIdx.x;
     for (u32 i = threadIdx.x; i < kQ * nwords; i += kThreads) {
@@ -47,20 +50,25 @@ __global__ void __launch_bounds__(kThreads) k_mask(const u32* __restrict__ col, 
         acc[q] = 0u;
         facc[q] = 0.0f;
     }
-    if (t < ntip) {
+    if (t < ntip && MODE == SC_DNA) {
+        // blocks of 32 positions, four plane words each
+        const uint4* q4 = reinterpret_cast<const uint4*>(qs);
+        const u32 nblk = nwords / 4;
+        for (u32 b = 0; b < nblk; b++) {
+            const u32 c0 = col[(size_t)(4 * b) * ld + t], c1 = col[(size_t)(4 * b + 1) * ld + t];
+            const u32 c2 = col[(size_t)(4 * b + 2) * ld + t], c3 = col[(size_t)(4 * b + 3) * ld + t];
+#pragma unroll
+            for (int q = 0; q < kQ; q++) {
+                const uint4 v = q4[q * nblk + b];
+                acc[q] += (u32)__popc((v.x & c0) | (v.y & c1) | (v.z & c2) | (v.w & c3));
+            }
+        }
+    } else if (t < ntip) {
         for (u32 k = 0; k < nwords; k++) {
             const u32 c = col[(size_t)k * ld + t];
             if (MODE == SC_UNIT) {
 #pragma unroll
                 for (int q = 0; q < kQ; q++) acc[q] += (u32)__popc(qs[q * nwords + k] & c);
-            } else if (MODE == SC_DNA) {
-#pragma unroll
-                for (int q = 0; q < kQ; q++) {
-                    u32 x = qs[q * nwords + k] & c;
-                    x |= x >> 1;
-                    x |= x >> 2;
-                    acc[q] += (u32)__popc(x & 0x11111111u);
-                }
             } else {
 #pragma unroll
                 for (int q = 0; q < kQ; q++) {
@@ -127,24 +135,29 @@ __global__ void k_expand(const u32* __restrict__ mask, u32 ntip, u32 maskWords, 
     }
 }
 
-// fasta2bin bytes -> column-major 4-bit nibbles, 8 positions per word
-// (packMatKernel, cu/radiusNeighborDNA.cu:27-53): nibble j of packed word k
-// is the low nibble of the code of position 8k+j.
-__global__ void k_pack_dna(const u32* __restrict__ raw, u32 ntip, u32 nbinRaw, u32 npk, u32 ld,
+// fasta2bin bytes -> column-major bit planes: for block b of 32 positions,
+// word 4b+j holds bit j of the low nibble of the code of position 32b+s at
+// bit s (the reference keeps the same low nibbles, packed eight to a word,
+// cu/radiusNeighborDNA.cu:27-53).
+__global__ void k_pack_dna(const u32* __restrict__ raw, u32 ntip, u32 nbinRaw, u32 nblk, u32 ld,
                            u32* __restrict__ col) {
     const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
-    const u32 k = blockIdx.y;
-    if (t >= ntip || k >= npk) return;
-    u32 v = 0;
-    for (u32 h = 0; h < 2; h++) {
-        const u32 wi = 2 * k + h;
-        if (wi < nbinRaw) {
-            const u32 r = raw[(size_t)t * nbinRaw + wi];
+    const u32 b = blockIdx.y;
+    if (t >= ntip || b >= nblk) return;
+    u32 p[4] = {0u, 0u, 0u, 0u};
+    for (u32 h = 0; h < 8; h++) {
+        const u32 wi = 8 * b + h;
+        if (wi >= nbinRaw) break;
+        const u32 r = raw[(size_t)t * nbinRaw + wi];
 #pragma unroll
-            for (int j = 0; j < 4; j++) v |= ((r >> (8 * j)) & 0xFu) << (4 * (4 * h + j));
+        for (int i = 0; i < 4; i++) {
+            const u32 code = (r >> (8 * i)) & 0xFu, s = 4 * h + i;
+#pragma unroll
+            for (int j = 0; j < 4; j++) p[j] |= ((code >> j) & 1u) << s;
         }
     }
-    col[(size_t)k * ld + t] = v;
+#pragma unroll
+    for (int j = 0; j < 4; j++) col[(size_t)(4 * b + j) * ld + t] = p[j];
 }
 
 // tryRadius: counts[r] = #{t < ntip : score(q_r, t) >= radius}; bit rows
@@ -157,17 +170,22 @@ __global__ void k_try(const u32* __restrict__ col, u32 nwords, u32 ld, u32 ntip,
     const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
     const u32 q = qidx[r];
     bool hit = false;
-    if (t < ntip) {
+    if (t < ntip && MODE == SC_DNA) {
+        u32 acc = 0;
+        for (u32 b = 0; b < nwords / 4; b++) {
+            u32 x = 0;
+#pragma unroll
+            for (int j = 0; j < 4; j++) x |= col[(size_t)(4 * b + j) * ld + q] & col[(size_t)(4 * b + j) * ld + t];
+            acc += (u32)__popc(x);
+        }
+        hit = acc >= uradius;
+    } else if (t < ntip) {
         u32 acc = 0;
         float facc = 0.f;
         for (u32 k = 0; k < nwords; k++) {
             const u32 x = col[(size_t)k * ld + q] & col[(size_t)k * ld + t];
             if (MODE == SC_UNIT) acc += (u32)__popc(x);
-            else if (MODE == SC_DNA) {
-                u32 y = x | (x >> 1);
-                y |= y >> 2;
-                acc += (u32)__popc(y & 0x11111111u);
-            } else {
+            else {
                 u32 m = x;
                 while (m) {
                     const int b = __ffs(m) - 1;
@@ -177,7 +195,6 @@ __global__ void k_try(const u32* __restrict__ col, u32 nwords, u32 ld, u32 ntip,
             }
         }
         if (MODE == SC_UNIT) hit = (float)acc >= radius;
-        else if (MODE == SC_DNA) hit = acc >= uradius;
         else hit = facc >= radius;
     }
     const u32 bal = __ballot_sync(0xFFFFFFFFu, hit);
@@ -190,7 +207,7 @@ using namespace radius;
 
 struct RadiusInput {
     bool dna;
-    u32 ntip, nwords;  // words per row (bit rows: nrow; DNA: packed nibble words)
+    u32 ntip, nwords;  // words per row (bit rows: nrow; DNA: 4 plane words per 32 positions)
     const u32* hostWordPlane;  // bit rows, word-plane-major (the .bmat body)
     const u32* hostRaw;        // DNA rows, fasta2bin layout
     u32 nbinRaw;
@@ -208,8 +225,8 @@ static int upload_rows(const RadiusInput& in, Carve& c, u32** col, float** wf, c
         u32* raw = c.take<u32>((size_t)in.ntip * in.nbinRaw);
         CASPHY_CUDA_TRY(cudaMemcpyAsync(raw, in.hostRaw, sizeof(u32) * (size_t)in.ntip * in.nbinRaw,
                                         cudaMemcpyHostToDevice, st));
-        k_pack_dna<<<dim3((in.ntip + 255) / 256, in.nwords), 256, 0, st>>>(raw, in.ntip, in.nbinRaw, in.nwords, in.ntip,
-                                                                           *col);
+        k_pack_dna<<<dim3((in.ntip + 255) / 256, in.nwords / 4), 256, 0, st>>>(raw, in.ntip, in.nbinRaw, in.nwords / 4,
+                                                                               in.ntip, *col);
     } else {
         CASPHY_CUDA_TRY(cudaMemcpyAsync(*col, in.hostWordPlane, sizeof(u32) * (size_t)in.nwords * in.ntip,
                                         cudaMemcpyHostToDevice, st));
@@ -244,7 +261,7 @@ static int prep_dna(RadiusInput& in, u32 ntip, u32 nbinRaw, const u32* raw, u32 
     in.ntip = ntip;
     in.nbinRaw = nbinRaw;
     in.hostRaw = raw;
-    in.nwords = (nbinRaw - 1) / 2 + 1;
+    in.nwords = 4 * ((nbinRaw + 7) / 8);  // 32 positions = 8 raw words per block
     in.mode = SC_DNA;
     in.radius = 0;
     in.uradius = radius;

@@ -74,6 +74,24 @@ def test_radius_dna_random(gpu_lib, radius):
     assert np.array_equal(gpu_lib.try_radius_dna(raw, radius, q), O.try_radius_dna(raw, radius, q))
 
 
+def test_radius_dna_ambiguity_codes(gpu_lib):
+    """IUPAC ambiguity codes (several nibble bits) intersect any base they
+    include; 1,001 columns leave a ragged last block of positions."""
+    tips, _ = synth.hky85_alignment(700, 1001, 4.0, [0.3, 0.2, 0.2, 0.3], 0.05, 0.05, seed=305)
+    raw, var = synth.dna_to_fasta2bin(tips)
+    rng = np.random.default_rng(6)
+    b = raw.view(np.uint8).copy()
+    m = (rng.random(b.shape) < 0.03) & (b > 0) & (b < 0x10)
+    b[m] = rng.choice([3, 5, 6, 9, 10, 12, 7, 15], size=int(m.sum())).astype(np.uint8)
+    raw = b.view(np.uint32).reshape(raw.shape)
+    for radius in (int(var.sum()) - 60, int(var.sum()) // 2):
+        c1, i1 = gpu_lib.radius_dna(raw, radius)
+        c0, i0 = O.radius_dna(raw, radius)
+        assert np.array_equal(c1, c0) and np.array_equal(i1, i0)
+        q = np.arange(0, 700, 29, dtype=np.uint32)
+        assert np.array_equal(gpu_lib.try_radius_dna(raw, radius, q), O.try_radius_dna(raw, radius, q))
+
+
 @pytest.mark.parametrize("ny,nx,ntip", [(1, 1, 40), (13, 7, 40), (300, 211, 1000), (64, 64, 2048)])
 def test_transfer_dis_random(gpu_lib, ny, nx, ntip):
     rng = np.random.default_rng(ny * 7 + nx)
