@@ -64,6 +64,8 @@ struct Arena {
     std::mutex mu;
     void* base = nullptr;
     size_t cap = 0;
+    void* aux = nullptr;  // second grow-only block for outputs sized mid-call
+    size_t auxCap = 0;
 };
 static std::mutex g_arenas_mu;
 static std::vector<Arena*> g_arenas;
@@ -82,28 +84,44 @@ DeviceScope::DeviceScope() {
 }
 DeviceScope::~DeviceScope() { static_cast<Arena*>(arena)->mu.unlock(); }
 
-int DeviceScope::reserve(size_t bytes, void** out) {
-    Arena* a = static_cast<Arena*>(arena);
-    if (bytes > a->cap) {
-        if (a->base) cudaFree(a->base);
-        a->base = nullptr;
-        a->cap = 0;
+// Grow-only block: a bigger request frees the old block and allocates
+// 1/8 more than asked (or exactly the request when that fails).
+static int grow(void** base, size_t* cap, size_t bytes, const char* what) {
+    if (bytes > *cap) {
+        if (*base) cudaFree(*base);
+        *base = nullptr;
+        *cap = 0;
         size_t want = bytes + (bytes >> 3);
-        cudaError_t e = cudaMalloc(&a->base, want);
+        cudaError_t e = cudaMalloc(base, want);
         if (e != cudaSuccess) {
             cudaGetLastError();
-            e = cudaMalloc(&a->base, bytes);
+            e = cudaMalloc(base, bytes);
             want = bytes;
         }
         if (e != cudaSuccess) {
             cudaGetLastError();
-            a->base = nullptr;
-            casphy_set_last_cuda_error(e, "cudaMalloc(arena)", __FILE__, __LINE__);
+            *base = nullptr;
+            casphy_set_last_cuda_error(e, what, __FILE__, __LINE__);
             return CASPHY_ENOMEM;
         }
-        a->cap = want;
+        *cap = want;
     }
+    return CASPHY_OK;
+}
+
+int DeviceScope::reserve(size_t bytes, void** out) {
+    Arena* a = static_cast<Arena*>(arena);
+    const int rc = grow(&a->base, &a->cap, bytes, "cudaMalloc(arena)");
+    if (rc) return rc;
     *out = a->base;
+    return CASPHY_OK;
+}
+
+int DeviceScope::reserve_aux(size_t bytes, void** out) {
+    Arena* a = static_cast<Arena*>(arena);
+    const int rc = grow(&a->aux, &a->auxCap, bytes, "cudaMalloc(aux)");
+    if (rc) return rc;
+    *out = a->aux;
     return CASPHY_OK;
 }
 

@@ -335,16 +335,15 @@ static int radius_impl(RadiusInput& in, u32 row0, u32 row1, u32* counts, u32* id
     if (total) *total = tot;
     if (!idx) return CASPHY_OK;
     if (tot > cap) return CASPHY_ERANGE;
-    // the index lists get their own buffer: their size is only known now
-    u32* didx = nullptr;
-    CASPHY_CUDA_TRY(cudaMalloc(&didx, sizeof(u32) * (tot ? tot : 1)));
+    // the index lists get the second block: their size is only known now
+    void* auxp = nullptr;
+    if ((rc = ds.reserve_aux(sizeof(u32) * (tot ? tot : 1), &auxp))) return rc;
+    u32* didx = static_cast<u32*>(auxp);
     CASPHY_CUDA_TRY(cudaMemcpyAsync(L.off, off.data(), sizeof(u64) * nq, cudaMemcpyHostToDevice, st));
     k_expand<<<(nq + 7) / 8, 256, 0, st>>>(L.mask, nq, maskWords, L.off, didx);
-    cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess && tot) e = cudaMemcpyAsync(idx, didx, sizeof(u32) * tot, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    cudaFree(didx);
-    CASPHY_CUDA_TRY(e);
+    CASPHY_CUDA_TRY(cudaGetLastError());
+    if (tot) CASPHY_CUDA_TRY(cudaMemcpyAsync(idx, didx, sizeof(u32) * tot, cudaMemcpyDeviceToHost, st));
+    CASPHY_CUDA_TRY(cudaStreamSynchronize(st));
     return CASPHY_OK;
 }
 

@@ -13,7 +13,11 @@ struct DeviceScope {
     DeviceScope();
     ~DeviceScope();
     // Returns a device block of at least `bytes`, valid until the scope ends.
+    // A later reserve() in the same scope may move the block.
     int reserve(size_t bytes, void** out);
+    // A second block, independent of reserve()'s, for outputs whose size is
+    // only known part-way through a call.
+    int reserve_aux(size_t bytes, void** out);
 };
 
 struct Carve {
