@@ -248,7 +248,7 @@ __global__ void __launch_bounds__(kSites) k_loglik_hky(u32 root, Tree T, HkyBuf 
     if (threadIdx.x == 0) part[C.blk0 + blockIdx.x] = v;
 }
 
-__global__ void __launch_bounds__(kSites, 5) k_outside_hky(u32 root, Tree T, HkyBuf B, Chunk C, u32 off, Hky m,
+__global__ void __launch_bounds__(kSites, 6) k_outside_hky(u32 root, Tree T, HkyBuf B, Chunk C, u32 off, Hky m,
                                                         const double* __restrict__ w, double* gpart) {
     __shared__ float2 red[kSites / 32];
     const u32 s = blockIdx.x * kSites + threadIdx.x;
