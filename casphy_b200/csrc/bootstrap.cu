@@ -12,8 +12,14 @@
 //
 // Here all replicates run in one pass:
 //  1. k_bs_prep: one warp per (replicate, tip) gathers the tip's row of the
-//     full matrix and builds the replicate's slot matrix and query entries
-//     (weights as integer bit planes, as the single join's PLANES path).
+//     full matrix and builds the replicate's slot matrix and query entries.
+//     When every replicate's weights sum to at most the site count (a
+//     column resample does), each resampled column is repeated as often as
+//     it was drawn (k_bs_gather) and scored with unit weights: the same
+//     integer scores and per-column merges as weight w on one column, with
+//     one entry per word instead of one per (word, weight bit plane).
+//     Otherwise the weights are integer bit planes (the single join's
+//     PLANES path).
 //  2. k_bs_init: the initial all-pairs scan of every replicate, tiles of all
 //     replicates drawn from one queue.
 //  3. k_bs_join: persistent and cooperative; each replicate is joined by a
@@ -68,16 +74,39 @@ struct Rep {
     u32 eStride;
 };
 
-// One warp per (replicate, tip).
+// Resampled rows: bit b of word j of (replicate r, tip) is the full row's
+// bit colIdx[r][32j+b] (kNone pads).  One warp per (replicate, tip).
+__global__ void k_bs_gather(const u32* __restrict__ repOfWarp, const u32* __restrict__ cells,
+                            const u32* __restrict__ words, const u32* __restrict__ colIdx, u32 nbin, u32 totalTips,
+                            u32* __restrict__ rows) {
+    const u32 warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= totalTips) return;
+    const u32* src = words + (size_t)cells[warp] * nbin;
+    const u32* ci = colIdx + (size_t)repOfWarp[warp] * nbin * 32;
+    for (u32 j = lane; j < nbin; j += 32) {
+        u32 v = 0;
+#pragma unroll 8
+        for (u32 b = 0; b < 32; b++) {
+            const u32 c = ci[32 * j + b];
+            if (c != kNone) v |= ((__ldg(src + (c >> 5)) >> (c & 31)) & 1u) << b;
+        }
+        rows[(size_t)warp * nbin + j] = v;
+    }
+}
+
+// One warp per (replicate, tip); rows: the resampled rows by warp, or null
+// to read the full rows.
 __global__ void k_bs_prep(const Rep* __restrict__ reps, const u32* __restrict__ repOfWarp,
-                          const u32* __restrict__ cells, const u32* __restrict__ words, u32 nbin, u32 totalTips) {
+                          const u32* __restrict__ cells, const u32* __restrict__ words, const u32* __restrict__ rows,
+                          u32 nbin, u32 totalTips) {
     const u32 warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (warp >= totalTips) return;
     const u32 r = repOfWarp[warp];
     const Rep& R = reps[r];
     const u32 tip = warp - R.off;
     const u32 cell = cells[warp];
-    prep_tip(words + (size_t)cell * nbin, tip, nbin, R.m.nbinP, (R.c.ntip + 7u) & ~7u, R.m.nplanes,
+    prep_tip(rows ? rows + (size_t)warp * nbin : words + (size_t)cell * nbin, tip, nbin, R.m.nbinP,
+             (R.c.ntip + 7u) & ~7u, R.m.nplanes,
              R.m.planeMask, R.m.nodeSeq, R.m.nodeBis, R.m.colT[0], R.eW, R.eQ, R.eLen, R.eStride);
     // initial local maximum: value -1, node ~0 (replaced by the initial scan)
     if ((threadIdx.x & 31) == 0) R.init.initKey[tip] = ((u64)ORD_F32_NEG1 << 32) | 0xFFFFFFFFull;
@@ -485,13 +514,32 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
     }
     for (u32 i = 0; i < totalTips; i++)
         if (rep_cells[i] >= ntip) return CASPHY_EINVAL;
-    std::vector<u32> planes((size_t)nrep * P * nbin, 0u);
-    for (u32 r = 0; r < nrep; r++)
-        for (u32 i = 0; i < nsite; i++) {
-            const u32 v = (u32)rep_weights[(size_t)r * nsite + i];
-            for (u32 k = 0; k < P; k++)
-                if ((v >> k) & 1u) planes[((size_t)r * P + k) * nbin + i / 32] |= 1u << (i % 32);
+    // repeated columns when every replicate's draws fit the row, else planes
+    bool repeat = true;
+    for (u32 r = 0; r < nrep && repeat; r++) {
+        double tot = 0;
+        for (u32 i = 0; i < nsite; i++) tot += rep_weights[(size_t)r * nsite + i];
+        repeat = tot <= (double)nsite;
+    }
+    std::vector<u32> colIdx;
+    if (repeat) {
+        P = 1;
+        colIdx.assign((size_t)nrep * nsite, joinx::kNone);
+        for (u32 r = 0; r < nrep; r++) {
+            size_t pos = (size_t)r * nsite;
+            for (u32 i = 0; i < nsite; i++)
+                for (u32 c = (u32)rep_weights[(size_t)r * nsite + i]; c > 0; c--) colIdx[pos++] = i;
         }
+    }
+    const u32 nplanes = repeat ? 0u : P;
+    std::vector<u32> planes((size_t)nrep * P * nbin, 0u);
+    if (!repeat)
+        for (u32 r = 0; r < nrep; r++)
+            for (u32 i = 0; i < nsite; i++) {
+                const u32 v = (u32)rep_weights[(size_t)r * nsite + i];
+                for (u32 k = 0; k < P; k++)
+                    if ((v >> k) & 1u) planes[((size_t)r * P + k) * nbin + i / 32] |= 1u << (i % 32);
+            }
     const u32 eStride = nbin * P;
     // per-replicate layout in one arena
     DeviceScope ds;
@@ -547,6 +595,8 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
         unsigned int* jcounter;
         int* errs;
         int* xerr;
+        u32* colIdx;
+        u32* rrows;
     };
     auto glob_layout = [&](Carve& c) {
         Glob g;
@@ -572,6 +622,8 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
         g.jcounter = c.take<unsigned int>(1);
         g.errs = c.take<int>(nrep);
         g.xerr = c.take<int>(1);
+        g.colIdx = c.take<u32>(repeat ? (size_t)nrep * nsite : 1);
+        g.rrows = c.take<u32>(repeat ? (size_t)totalTips * nbin : 1);
         return g;
     };
     Carve cv;
@@ -608,7 +660,7 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
         c.err = G.errs + r; c.limitNs = 20ull * 1000 * 1000 * 1000; c.statsOut = b.stats;
         c.Rmax = ((n + Gs[r] - 1) / Gs[r] + 7u) & ~7u; c.ordNeg1 = ORD_F32_NEG1; c.compactMin = 4096; c.compactQ8 = 192; c.bytesPerPairSite = 4000;
         c.prof = nullptr;
-        R.m = BitModel<PATH_PLANES>::Args{nbin, nbinP, P, ancestralType ? 1 : 0, b.planeMask, nullptr,
+        R.m = BitModel<PATH_PLANES>::Args{nbin, nbinP, nplanes, ancestralType ? 1 : 0, b.planeMask, nullptr,
                                           b.nodeSeq, b.nodeBis, {b.colT0, b.colT1}};
         R.init = InitArgs{n, nbin, Sp, eStride, b.colT0, b.eW, b.eQ, b.eLen, nullptr, b.chunkStart, nChunks,
                           cs[nChunks], nullptr, b.initKey};
@@ -692,7 +744,14 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
     CASPHY_CUDA_TRY(cudaMemsetAsync(G.errs, 0, sizeof(int) * nrep, st));
     CASPHY_CUDA_TRY(cudaMemsetAsync(G.xerr, 0, sizeof(int), st));
     u64 launches = 0;
-    k_bs_prep<<<(totalTips + 7) / 8, 256, 0, st>>>(G.reps, G.repOfWarp, G.cells, G.words, nbin, totalTips);
+    if (repeat) {
+        CASPHY_CUDA_TRY(up(G.colIdx, colIdx.data(), 4ull * nrep * nsite));
+        k_bs_gather<<<(totalTips + 7) / 8, 256, 0, st>>>(G.repOfWarp, G.cells, G.words, G.colIdx, nbin, totalTips,
+                                                       G.rrows);
+        launches++;
+    }
+    k_bs_prep<<<(totalTips + 7) / 8, 256, 0, st>>>(G.reps, G.repOfWarp, G.cells, G.words, repeat ? G.rrows : nullptr,
+                                                   nbin, totalTips);
     int perSM = 0;
     CASPHY_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_bs_init, kThreads, 0));
     k_bs_init<<<nSM * std::max(perSM, 1), kThreads, 0, st>>>(G.reps, G.tileStart, nrep, G.counter);

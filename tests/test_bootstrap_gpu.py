@@ -70,3 +70,17 @@ def test_bad_replicates_raise(gpu_lib):
         gpu_lib.bootstrap_bit(words, full_edge, off, bad, w)
     with pytest.raises(gpu_lib.CasphyError):
         gpu_lib.bootstrap_bit(words, full_edge, off, cells, w + 0.5)
+
+
+def test_weights_beyond_the_row_use_planes(gpu_lib):
+    """Weights that sum past the site count (here doubled multiplicities)
+    cannot be laid out as repeated columns; the bit-plane path must give the
+    plain pipeline's values too."""
+    words, full_edge, off, cells, w = _case(600, 4, 5, 200, 600, 9)
+    w2 = 2 * w
+    got = gpu_lib.bootstrap_bit(words, full_edge, off, cells, w2)
+    full_bits = B.clade_bits(full_edge, 600, (600 + 31) // 32)
+    for r in range(5):
+        c = cells[off[r]:off[r + 1]]
+        ymin, ysize = B.plain_replicate(gpu_lib, words, full_bits, c, w2[r])
+        assert np.array_equal(got["ymin"][r], ymin) and np.array_equal(got["ysize"][r], ysize)
