@@ -42,6 +42,7 @@
 //     has bits past the tips), in O(clades x nodes) instead of
 //     O(clades x clades x words).
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -400,6 +401,18 @@ inline double cost_us(const Tune& T, u32 n, u32 G) {
 std::vector<u32> split_groups(const Tune& T, const std::vector<u32>& repN, u32 slots) {
     const u32 nrep = (u32)repN.size();
     std::vector<u32> G(nrep, 1);
+    // CASPHY_BS_GROUP=g fixes g CTAs for every replicate of 512 cells or
+    // more while they fit the SMs (the cost model is bypassed)
+    if (const char* env = std::getenv("CASPHY_BS_GROUP")) {
+        const u32 g = std::min<u32>((u32)std::max(1, std::atoi(env)), kMaxGroup);
+        u32 used = 0;
+        for (u32 r = 0; r < nrep; r++)
+            if (g > 1 && repN[r] >= 512 && used + g <= slots) {
+                G[r] = g;
+                used += g;
+            }
+        return G;
+    }
     std::vector<double> t(nrep);
     double W = 0;
     for (u32 r = 0; r < nrep; r++) {

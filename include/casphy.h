@@ -329,7 +329,10 @@ int casphy_ancestral_char(uint32_t ntip, uint32_t nnode, uint32_t nsite, const i
  *   rep_raw_edges optional: per replicate, 2*(n_r-1) raw join edges (parent,
  *                child) in join order over the replicate's tip ids
  * Each replicate tree is the tree joinEdgeBitReverse builds from its rows and
- * weights (the same engine as casphy_join_bit).
+ * weights (the same engine as casphy_join_bit).  The CTAs joining each
+ * replicate come from a cost model refitted after every call on the device;
+ * the environment variable CASPHY_BS_GROUP=g fixes g of them (at most 8) for
+ * every replicate of 512 cells or more instead.
  */
 typedef struct {
     uint32_t nrep, nclade;

@@ -48,8 +48,17 @@ def test_batched_equals_sequential(gpu_lib, ncell, nbin, nrep, nmin, nmax, seed)
     assert np.array_equal(got["ysize"], ysize)
     assert np.array_equal(got["support"], B.support_counts(ymin, ysize, thr))
     if nmin >= 2000:
-        # few large replicates: each is joined by a group of CTAs
-        assert got["stats"]["max_ctas_per_rep"] > 1
+        # the same replicates joined by groups of 4 CTAs give the same trees and values
+        import os
+        os.environ["CASPHY_BS_GROUP"] = "4"
+        try:
+            grouped = gpu_lib.bootstrap_bit(words, full_edge, off, cells, w, threshold=thr, raw_edges=True)
+        finally:
+            del os.environ["CASPHY_BS_GROUP"]
+        assert grouped["stats"]["max_ctas_per_rep"] == 4
+        assert np.array_equal(grouped["ymin"], ymin) and np.array_equal(grouped["ysize"], ysize)
+        for r in range(nrep):
+            assert np.array_equal(grouped["raw_edges"][r], got["raw_edges"][r])
 
 
 def test_oracle_pipeline_agrees_on_a_replicate(gpu_lib):
