@@ -198,6 +198,22 @@ __device__ inline void load_table(const Common& a, u32 p, Table t) {
     __syncthreads();
 }
 
+// The table of a lone CTA is its own just-published top-2: copied from
+// shared memory instead of read back through L2.
+__device__ inline void load_table_self(const BlockRec* top, u32 cnt, Table t) {
+    if (threadIdx.x < 2) t.tab[threadIdx.x] = top[threadIdx.x];
+    if (threadIdx.x == 0) {
+        t.cnt[0] = (unsigned char)min(cnt, 2u);
+        t.exact[0] = cnt <= 2;
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void load_table_any(const Common& a, u32 p, Table t, const BlockRec* top, u32 cnt) {
+    if (a.nCTA == 1) load_table_self(top, cnt, t);
+    else load_table(a, p, t);
+}
+
 // Top-2 of the stored local maxima of this CTA's slots (refresh/compaction).
 __device__ inline void own_top2(const Common& a, u32 buf, const Range& rg, u64* red, BlockRec* s_rec, BlockRec* out,
                          u32* cntOut, u32* wsum) {
@@ -326,7 +342,7 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
     own_top2(a, buf, rg, red, &s_rec, s_top, &cnt, wsum);
     publish(a, p, b, s_top, cnt);
     if (flag_barrier(a.flags, nCTA, b, ++p, a.err, a.limitNs)) goto out;
-    load_table(a, p - 1, T);
+    load_table_any(a, p - 1, T, s_top, cnt);
 
     pf.mark(PROF_COMPACT);
     while (k < nJoin) {
@@ -339,7 +355,7 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
             pf.mark(PROF_POST);
             if (flag_barrier(a.flags, nCTA, b, ++p, a.err, a.limitNs)) goto out;
             pf.mark(PROF_BARRIER);
-            load_table(a, p - 1, T);
+            load_table_any(a, p - 1, T, s_top, cnt);
             pf.mark(PROF_TABLE);
             continue;
         }
@@ -387,11 +403,15 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
             if (flag_barrier(a.flags, nCTA, b, ++p, a.err, a.limitNs)) goto out;
             pf.mark(PROF_BARRIER);
             u64 pb = make_key(a.ordNeg1, 0u);
-            for (u32 i = threadIdx.x; i < nCTA; i += kThreads) {
-                const u64 v = ld_cg_u64(a.partial + ((p - 1) & 1) * nCTA + i);
-                pb = v > pb ? v : pb;
+            if (nCTA == 1) {
+                pb = pr.key > pb ? pr.key : pb;  // the lone CTA's own best
+            } else {
+                for (u32 i = threadIdx.x; i < nCTA; i += kThreads) {
+                    const u64 v = ld_cg_u64(a.partial + ((p - 1) & 1) * nCTA + i);
+                    pb = v > pb ? v : pb;
+                }
+                pb = block_max_u64(pb, red);
             }
-            pb = block_max_u64(pb, red);
             const u32 vOrd = key_ord(pb), vIdx = key_node(pb);
             const u32 ob = c1 / rg.R;
             if (ob == b && threadIdx.x == 0) {
@@ -496,7 +516,7 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
         k++;
         if (flag_barrier(a.flags, nCTA, b, ++p, a.err, a.limitNs)) goto out;
         pf.mark(PROF_BARRIER);
-        load_table(a, p - 1, T);
+        load_table_any(a, p - 1, T, s_top, cnt);
         pf.mark(PROF_TABLE);
 
         // renumber slots densely when too few are alive
@@ -543,7 +563,7 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
             publish(a, p, b, s_top, cnt);
             nComp++;
             if (flag_barrier(a.flags, nCTA, b, ++p, a.err, a.limitNs)) goto out;
-            load_table(a, p - 1, T);
+            load_table_any(a, p - 1, T, s_top, cnt);
             pf.mark(PROF_COMPACT);
         }
     }
