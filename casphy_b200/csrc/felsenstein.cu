@@ -262,23 +262,31 @@ __global__ void __launch_bounds__(kSites, 6) k_outside_hky(u32 root, Tree T, Hky
     int e;
     const u32 ca = nf.y, cb = nf.z;
     const u32 eA = nf.w, eB = T.outEdgeB[off + blockIdx.y];
+    // the block's four edge matrices staged once in shared memory:
+    // P_a, P_b, dP_a, dP_b
+    __shared__ float sm[64];
+    if (threadIdx.x < 64) {
+        const u32 q = threadIdx.x >> 4, i = threadIdx.x & 15;
+        const u32 ed = (q & 1) ? eB : eA;
+        sm[threadIdx.x] = __ldg((q < 2 ? B.P : B.dP) + 16 * ed + i);
+    }
     const float4 la = child_hky(T, B, C, ca, ss, &e);
     const float4 lb = child_hky(T, B, C, cb, ss, &e);
-    const float4 ma = pmatvec(B.P + 16 * eA, la), mb = pmatvec(B.P + 16 * eB, lb);
+    __syncthreads();
+    const float4 ma = pmatvec(sm, la), mb = pmatvec(sm + 16, lb);
     const float ws = ok ? (float)w[C.s0 + s] : 0.f;
     float gs[2];
 #pragma unroll
     for (int side = 0; side < 2; side++) {
         const u32 c = side ? cb : ca;
-        const u32 ec = side ? eB : eA;
         const float4 msib = side ? ma : mb;
         const float4 lc = side ? lb : la;
         const float4 mc = side ? mb : ma;
         const float4 r = make_float4(u.x * msib.x, u.y * msib.y, u.z * msib.z, u.w * msib.w);
-        const float4 dm = matvec(B.dP + 16 * ec, lc);
+        const float4 dm = matvec(sm + 32 + 16 * side, lc);
         gs[side] = ok ? ws * (dot4(r, dm) / dot4(r, mc)) : 0.f;
         if (ok && c >= T.ntip) {
-            float4 uc = pvecmat(r, B.P + 16 * ec);
+            float4 uc = pvecmat(r, sm + 16 * side);
             renorm4(uc);
             B.U[(size_t)(c - T.ntip) * C.W + s] = uc;
         }
