@@ -248,51 +248,75 @@ __global__ void __launch_bounds__(kSites) k_loglik_hky(u32 root, Tree T, HkyBuf 
     if (threadIdx.x == 0) part[C.blk0 + blockIdx.x] = v;
 }
 
-__global__ void __launch_bounds__(kSites, 6) k_outside_hky(u32 root, Tree T, HkyBuf B, Chunk C, u32 off, Hky m,
+__global__ void __launch_bounds__(kSites / 2, 10) k_outside_hky(u32 root, Tree T, HkyBuf B, Chunk C, u32 off, Hky m,
                                                         const double* __restrict__ w, double* gpart) {
-    __shared__ float2 red[kSites / 32];
-    const u32 s = blockIdx.x * kSites + threadIdx.x;
+    __shared__ float sm[64];
     const uint4 nf = T.outInfo[off + blockIdx.y];
     const u32 v = nf.x, vi = v - T.ntip;
-    const bool ok = s < C.w;
-    const u32 ss = ok ? s : 0;
-    float4 u;
-    if (v == root) u = make_float4((float)m.pi[0], (float)m.pi[1], (float)m.pi[2], (float)m.pi[3]);
-    else u = B.U[(size_t)vi * C.W + ss];
-    int e;
     const u32 ca = nf.y, cb = nf.z;
     const u32 eA = nf.w, eB = T.outEdgeB[off + blockIdx.y];
-    // the block's four edge matrices staged once in shared memory:
-    // P_a, P_b, dP_a, dP_b
-    __shared__ float sm[64];
     if (threadIdx.x < 64) {
         const u32 q = threadIdx.x >> 4, i = threadIdx.x & 15;
         const u32 ed = (q & 1) ? eB : eA;
         sm[threadIdx.x] = __ldg((q < 2 ? B.P : B.dP) + 16 * ed + i);
     }
-    const float4 la = child_hky(T, B, C, ca, ss, &e);
-    const float4 lb = child_hky(T, B, C, cb, ss, &e);
-    __syncthreads();
-    const float4 ma = pmatvec(sm, la), mb = pmatvec(sm + 16, lb);
-    const float ws = ok ? (float)w[C.s0 + s] : 0.f;
-    float gs[2];
+    // two sites per thread, 128 apart: all loads first
+    u32 sj[2], ssj[2];
+    bool okj[2];
+    float4 u[2], la[2], lb[2];
+    int e;
 #pragma unroll
-    for (int side = 0; side < 2; side++) {
-        const u32 c = side ? cb : ca;
-        const float4 msib = side ? ma : mb;
-        const float4 lc = side ? lb : la;
-        const float4 mc = side ? mb : ma;
-        const float4 r = make_float4(u.x * msib.x, u.y * msib.y, u.z * msib.z, u.w * msib.w);
-        const float4 dm = matvec(sm + 32 + 16 * side, lc);
-        gs[side] = ok ? ws * (dot4(r, dm) / dot4(r, mc)) : 0.f;
-        if (ok && c >= T.ntip) {
-            float4 uc = pvecmat(r, sm + 16 * side);
-            renorm4(uc);
-            B.U[(size_t)(c - T.ntip) * C.W + s] = uc;
+    for (int j = 0; j < 2; j++) {
+        sj[j] = blockIdx.x * kSites + threadIdx.x + j * (kSites / 2);
+        okj[j] = sj[j] < C.w;
+        ssj[j] = okj[j] ? sj[j] : 0;
+        if (v == root) u[j] = make_float4((float)m.pi[0], (float)m.pi[1], (float)m.pi[2], (float)m.pi[3]);
+        else u[j] = B.U[(size_t)vi * C.W + ssj[j]];
+        la[j] = child_hky(T, B, C, ca, ssj[j], &e);
+        lb[j] = child_hky(T, B, C, cb, ssj[j], &e);
+    }
+    __syncthreads();
+    float gs[2][2] = {{0.f, 0.f}, {0.f, 0.f}};  // [side][j]
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        const float4 ma = pmatvec(sm, la[j]), mb = pmatvec(sm + 16, lb[j]);
+        const float ws = okj[j] ? (float)w[C.s0 + sj[j]] : 0.f;
+#pragma unroll
+        for (int side = 0; side < 2; side++) {
+            const u32 c = side ? cb : ca;
+            const float4 msib = side ? ma : mb;
+            const float4 lc = side ? lb[j] : la[j];
+            const float4 mc = side ? mb : ma;
+            const float4 r = make_float4(u[j].x * msib.x, u[j].y * msib.y, u[j].z * msib.z, u[j].w * msib.w);
+            const float4 dm = matvec(sm + 32 + 16 * side, lc);
+            gs[side][j] = okj[j] ? ws * (dot4(r, dm) / dot4(r, mc)) : 0.f;
+            if (okj[j] && c >= T.ntip) {
+                float4 uc = pvecmat(r, sm + 16 * side);
+                renorm4(uc);
+                B.U[(size_t)(c - T.ntip) * C.W + sj[j]] = uc;
+            }
         }
     }
-    // site terms in binary32 within the block; blocks are added in binary64
-    const float2 g = block_sum2f(gs[0], gs[1], red);
+    // site terms in binary32 within the block, grouped as 32-site warps in
+    // site order (warp w of half j holds sites 128 j + 32 w ..); blocks are
+    // added in binary64
+    __shared__ float2 red8[kSites / 32];
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        float a = gs[0][j], b = gs[1][j];
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(0xFFFFFFFFu, a, o);
+            b += __shfl_xor_sync(0xFFFFFFFFu, b, o);
+        }
+        if ((threadIdx.x & 31) == 0) red8[(threadIdx.x >> 5) + j * (kSites / 64)] = make_float2(a, b);
+    }
+    __syncthreads();
+    float2 g = make_float2(0.f, 0.f);
+    if (threadIdx.x == 0)
+        for (u32 i = 0; i < kSites / 32; i++) {
+            g.x += red8[i].x;
+            g.y += red8[i].y;
+        }
     if (threadIdx.x == 0) {
         gpart[(size_t)eA * C.nblkTot + C.blk0 + blockIdx.x] = g.x;
         gpart[(size_t)eB * C.nblkTot + C.blk0 + blockIdx.x] = g.y;
@@ -867,7 +891,7 @@ struct FelProblem {
             for (size_t lv = 0; lv + 1 < th.outOff.size(); lv++) {
                 const dim3 grid(nb, th.outOff[lv + 1] - th.outOff[lv]);
                 if (model == CASPHY_MODEL_HKY85)
-                    k_outside_hky<<<grid, kSites, 0, st>>>(th.root, T, hb, C, th.outOff[lv], hky, w, gpart);
+                    k_outside_hky<<<grid, kSites / 2, 0, st>>>(th.root, T, hb, C, th.outOff[lv], hky, w, gpart);
                 else k_outside_irr<<<grid, kSites, 0, st>>>(th.root, T, ib, C, th.outOff[lv], w, gpart);
                 n++;
             }
