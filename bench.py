@@ -254,7 +254,7 @@ def bootstrap_suite(L, plain=True):
     got = L.bootstrap_bit(words, full_edge, off, cells, w, threshold=0.05)
     batched_s = time.perf_counter() - t0
     groups = {k: got["stats"][k] for k in ("max_ctas_per_rep", "tuned", "join_longest_ms", "join_busy_ms",
-                                           "cost_alpha_us", "cost_beta_us", "cost_gamma_us")}
+                                           "cost_alpha_us", "cost_beta_us", "cost_gamma_us", "graph")}
     if not plain:
         return {"batched_s": batched_s, "batched_device_ms": got["stats"]["total_ms"], "join_groups": groups}
     full_bits = B.clade_bits(full_edge, ncell, (ncell + 31) // 32)

@@ -729,7 +729,6 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
     cudaEvent_t ev[4];
     for (auto& e : ev) CASPHY_CUDA_TRY(cudaEventCreate(&e));
     auto up = [&](void* d, const void* h, size_t n) { return cudaMemcpyAsync(d, h, n, cudaMemcpyHostToDevice, st); };
-    CASPHY_CUDA_TRY(cudaEventRecord(ev[0], st));
     // per-replicate plane masks and tile tables
     for (u32 r = 0; r < nrep; r++) {
         const RepBufs& b = rb[r];
@@ -756,48 +755,68 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
     CASPHY_CUDA_TRY(cudaMemsetAsync(G.jcounter, 0, sizeof(unsigned int), st));
     CASPHY_CUDA_TRY(cudaMemsetAsync(G.errs, 0, sizeof(int) * nrep, st));
     CASPHY_CUDA_TRY(cudaMemsetAsync(G.xerr, 0, sizeof(int), st));
-    u64 launches = 0;
-    if (repeat) {
-        CASPHY_CUDA_TRY(up(G.colIdx, colIdx.data(), 4ull * nrep * nsite));
-        k_bs_gather<<<(totalTips + 7) / 8, 256, 0, st>>>(G.repOfWarp, G.cells, G.words, G.colIdx, nbin, totalTips,
-                                                       G.rrows);
-        launches++;
-    }
-    k_bs_prep<<<(totalTips + 7) / 8, 256, 0, st>>>(G.reps, G.repOfWarp, G.cells, G.words, repeat ? G.rrows : nullptr,
-                                                   nbin, totalTips);
+    if (repeat) CASPHY_CUDA_TRY(up(G.colIdx, colIdx.data(), 4ull * nrep * nsite));
     int perSM = 0;
     CASPHY_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_bs_init, kThreads, 0));
-    k_bs_init<<<nSM * std::max(perSM, 1), kThreads, 0, st>>>(G.reps, G.tileStart, nrep, G.counter);
-    k_bs_slot_init<<<dim3((2 * nmax + 255) / 256, nrep), 256, 0, st>>>(G.reps);
-    launches += 3;
-    CASPHY_CUDA_TRY(cudaEventRecord(ev[1], st));
-    {
-        void* fn = (void*)k_bs_join<PATH_PLANES>;
-        CASPHY_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        int per = 0;
-        CASPHY_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, kThreads, smem));
-        if (per < 1) return CASPHY_ERANGE;
-        const u32 grid = std::min<u32>(nItem, (u32)(nSM * per));
-        if (inGroups > grid) return CASPHY_EINTERNAL;  // a group could not form
-        // cooperative: every CTA is resident, so each group's members run together
-        const Rep* a0 = G.reps;
-        const u32* a1 = G.itemRep;
-        const u32* a2 = G.itemMember;
-        u32 a3 = nItem;
-        unsigned int* a4 = G.jcounter;
-        const u32* a5 = G.rankOf;
-        void* args[] = {(void*)&a0, (void*)&a1, (void*)&a2, (void*)&a3, (void*)&a4, (void*)&a5};
-        CASPHY_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, smem, st));
-        launches++;
-    }
-    CASPHY_CUDA_TRY(cudaGetLastError());
-    CASPHY_CUDA_TRY(cudaEventRecord(ev[2], st));
+    void* joinFn = (void*)k_bs_join<PATH_PLANES>;
+    CASPHY_CUDA_TRY(cudaFuncSetAttribute(joinFn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per = 0;
+    CASPHY_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, joinFn, kThreads, smem));
+    if (per < 1) return CASPHY_ERANGE;
+    const u32 joinGrid = std::min<u32>(nItem, (u32)(nSM * per));
+    if (inGroups > joinGrid) return CASPHY_EINTERNAL;  // a group could not form
+    const Rep* a0 = G.reps;
+    const u32* a1 = G.itemRep;
+    const u32* a2 = G.itemMember;
+    u32 a3 = nItem;
+    unsigned int* a4 = G.jcounter;
+    const u32* a5 = G.rankOf;
+    void* joinArgs[] = {(void*)&a0, (void*)&a1, (void*)&a2, (void*)&a3, (void*)&a4, (void*)&a5};
     XferArgs xa{nX, nrep, 32u * ((ntip + 31) / 32), G.Xlo, G.Xhi, G.repN, G.repOff, G.repOpsOff, G.sortedRank, G.ops,
                 threshold, G.ymin, G.ysize, G.support, G.xerr};
-    k_bs_transfer<<<dim3((nX + kXThreads - 1) / kXThreads, nrep), kXThreads, 0, st>>>(xa);
-    launches++;
-    CASPHY_CUDA_TRY(cudaGetLastError());
-    CASPHY_CUDA_TRY(cudaEventRecord(ev[3], st));
+    // the whole pass: prep, initial scans, the persistent cooperative join
+    // (every CTA resident, so each group's members run together), transfer
+    const u64 launches = (repeat ? 1 : 0) + 5;
+    auto enqueue = [&](cudaStream_t s) -> cudaError_t {
+        cudaError_t e;
+        if ((e = cudaEventRecord(ev[0], s)) != cudaSuccess) return e;
+        if (repeat)
+            k_bs_gather<<<(totalTips + 7) / 8, 256, 0, s>>>(G.repOfWarp, G.cells, G.words, G.colIdx, nbin, totalTips,
+                                                          G.rrows);
+        k_bs_prep<<<(totalTips + 7) / 8, 256, 0, s>>>(G.reps, G.repOfWarp, G.cells, G.words,
+                                                      repeat ? G.rrows : nullptr, nbin, totalTips);
+        k_bs_init<<<nSM * std::max(perSM, 1), kThreads, 0, s>>>(G.reps, G.tileStart, nrep, G.counter);
+        k_bs_slot_init<<<dim3((2 * nmax + 255) / 256, nrep), 256, 0, s>>>(G.reps);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(ev[1], s)) != cudaSuccess) return e;
+        if ((e = cudaLaunchCooperativeKernel(joinFn, dim3(joinGrid), dim3(kThreads), joinArgs, smem, s)) !=
+            cudaSuccess)
+            return e;
+        if ((e = cudaEventRecord(ev[2], s)) != cudaSuccess) return e;
+        k_bs_transfer<<<dim3((nX + kXThreads - 1) / kXThreads, nrep), kXThreads, 0, s>>>(xa);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        return cudaEventRecord(ev[3], s);
+    };
+    // run it as one captured CUDA graph; launch directly if capture fails
+    CASPHY_CUDA_TRY(cudaStreamSynchronize(st));
+    bool graphed = false;
+    {
+        cudaStream_t cs = nullptr;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            const cudaError_t e = enqueue(cs);
+            const cudaError_t e2 = cudaStreamEndCapture(cs, &graph);
+            if (e == cudaSuccess && e2 == cudaSuccess && graph && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess)
+                graphed = cudaGraphLaunch(exec, cs) == cudaSuccess && cudaStreamSynchronize(cs) == cudaSuccess;
+        }
+        if (!graphed) cudaGetLastError();  // a refused capture is not an error of the call
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (cs) cudaStreamDestroy(cs);
+    }
+    if (!graphed) CASPHY_CUDA_TRY(enqueue(st));
     std::vector<int> errs(nrep);
     int xerr = 0;
     CASPHY_CUDA_TRY(cudaMemcpyAsync(errs.data(), G.errs, sizeof(int) * nrep, cudaMemcpyDeviceToHost, st));
@@ -858,6 +877,7 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
         s.kernel_launches = launches;
         s.join_phases = phases;
         s.max_ctas_per_rep = maxG;
+        s.graph = graphed ? 1u : 0u;
         s.tuned = tunedBefore ? 1u : 0u;
         s.join_longest_ms = longest * 1e-3;
         s.join_busy_ms = busy * 1e-3;

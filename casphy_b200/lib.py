@@ -52,7 +52,8 @@ class BootstrapStats(C.Structure):
                 ("transfer_ms", C.c_double), ("total_ms", C.c_double), ("kernel_launches", C.c_uint64),
                 ("join_phases", C.c_uint64), ("max_ctas_per_rep", C.c_uint32), ("tuned", C.c_uint32),
                 ("join_longest_ms", C.c_double), ("join_busy_ms", C.c_double), ("cost_alpha_us", C.c_double),
-                ("cost_beta_us", C.c_double), ("cost_gamma_us", C.c_double)]
+                ("cost_beta_us", C.c_double), ("cost_gamma_us", C.c_double), ("graph", C.c_uint32),
+                ("reserved", C.c_uint32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -344,6 +344,8 @@ typedef struct {
     double join_longest_ms;                          /* longest single replicate join */
     double join_busy_ms;                             /* replicate joins summed (CTA-time) */
     double cost_alpha_us, cost_beta_us, cost_gamma_us;  /* per-phase cost model after this call */
+    uint32_t graph;                                  /* 1 when the pass ran as one captured CUDA graph */
+    uint32_t reserved;
 } casphy_bootstrap_stats;
 
 int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t *words, const uint32_t *full_edge,
