@@ -779,7 +779,7 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
     const u64 launches = (repeat ? 1 : 0) + 5;
     auto enqueue = [&](cudaStream_t s) -> cudaError_t {
         cudaError_t e;
-        if ((e = cudaEventRecord(ev[0], s)) != cudaSuccess) return e;
+        if ((e = cudaEventRecordWithFlags(ev[0], s, cudaEventRecordExternal)) != cudaSuccess) return e;
         if (repeat)
             k_bs_gather<<<(totalTips + 7) / 8, 256, 0, s>>>(G.repOfWarp, G.cells, G.words, G.colIdx, nbin, totalTips,
                                                           G.rrows);
@@ -788,14 +788,14 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
         k_bs_init<<<nSM * std::max(perSM, 1), kThreads, 0, s>>>(G.reps, G.tileStart, nrep, G.counter);
         k_bs_slot_init<<<dim3((2 * nmax + 255) / 256, nrep), 256, 0, s>>>(G.reps);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        if ((e = cudaEventRecord(ev[1], s)) != cudaSuccess) return e;
+        if ((e = cudaEventRecordWithFlags(ev[1], s, cudaEventRecordExternal)) != cudaSuccess) return e;
         if ((e = cudaLaunchCooperativeKernel(joinFn, dim3(joinGrid), dim3(kThreads), joinArgs, smem, s)) !=
             cudaSuccess)
             return e;
-        if ((e = cudaEventRecord(ev[2], s)) != cudaSuccess) return e;
+        if ((e = cudaEventRecordWithFlags(ev[2], s, cudaEventRecordExternal)) != cudaSuccess) return e;
         k_bs_transfer<<<dim3((nX + kXThreads - 1) / kXThreads, nrep), kXThreads, 0, s>>>(xa);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        return cudaEventRecord(ev[3], s);
+        return cudaEventRecordWithFlags(ev[3], s, cudaEventRecordExternal);
     };
     // run it as one captured CUDA graph; launch directly if capture fails
     CASPHY_CUDA_TRY(cudaStreamSynchronize(st));

@@ -48,6 +48,8 @@ def test_batched_equals_sequential(gpu_lib, ncell, nbin, nrep, nmin, nmax, seed)
     assert np.array_equal(got["ysize"], ysize)
     assert np.array_equal(got["support"], B.support_counts(ymin, ysize, thr))
     assert got["stats"]["graph"] == 1  # the pass ran as one captured CUDA graph
+    st = got["stats"]
+    assert st["join_ms"] > 0 and st["total_ms"] >= st["prep_ms"] + st["join_ms"]  # event nodes time the graph
     if nmin >= 2000:
         # the same replicates joined by groups of 4 CTAs give the same trees and values
         import os
