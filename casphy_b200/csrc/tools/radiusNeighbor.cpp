@@ -1,3 +1,4 @@
+#include <algorithm>
 // Drop-in for `radiusNeighbor <prefix> <radius>` (cu/radiusNeighbor.cu:162-470):
 // <prefix>.bmat (word-plane-major bits) + <prefix>.w -> <prefix>.idx and
 // <prefix>.nNeighbor.
@@ -34,10 +35,13 @@ int main(int argc, char* argv[]) {
     if (dev < 0) return tool::fail("radiusNeighbor", CASPHY_ENODEV);
     std::vector<uint32_t> counts(ntip);
     uint64_t total = 0;
-    int rc = casphy_radius_bit(nrow, ntip, bmat.data(), w.data(), radius, counts.data(), nullptr, 0, &total);
-    if (rc) return tool::fail("radiusNeighbor", rc);
-    std::vector<uint32_t> idx(total ? total : 1);
-    rc = casphy_radius_bit(nrow, ntip, bmat.data(), w.data(), radius, counts.data(), idx.data(), total, &total);
+    // one search when the lists fit a guessed buffer, a second only when not
+    std::vector<uint32_t> idx(std::max<size_t>((size_t)64 * ntip, (size_t)1 << 16));
+    int rc = casphy_radius_bit(nrow, ntip, bmat.data(), w.data(), radius, counts.data(), idx.data(), idx.size(), &total);
+    if (rc == CASPHY_ERANGE && total > idx.size()) {
+        idx.assign(total, 0u);
+        rc = casphy_radius_bit(nrow, ntip, bmat.data(), w.data(), radius, counts.data(), idx.data(), idx.size(), &total);
+    }
     if (rc) return tool::fail("radiusNeighbor", rc);
     if (!tool::write_raw(prefix + ".idx", idx.data(), sizeof(uint32_t) * total) ||
         !tool::write_mat(prefix + ".nNeighbor", 1, ntip, counts.data(), ntip))

@@ -173,12 +173,17 @@ def node_keep(node_state, edge, outmat, cutoff, bit=False):
 
 
 def _lists(call, ntip):
+    """Counts and lists in one search when they fit a guessed buffer (64 per
+    row); a second search only when they do not."""
     counts = np.zeros(max(ntip, 1), dtype=np.uint32)
     tot = C.c_uint64(0)
-    _chk(call(counts, None, 0, C.byref(tot)), "casphy_radius")
-    idx = np.zeros(max(tot.value, 1), dtype=np.uint32)
-    _chk(call(counts, idx.ctypes.data_as(C.c_void_p), tot.value, C.byref(tot)), "casphy_radius")
-    return counts[:ntip], idx[: tot.value]
+    idx = np.empty(max(64 * ntip, 1 << 16), dtype=np.uint32)
+    st = call(counts, idx.ctypes.data_as(C.c_void_p), idx.size, C.byref(tot))
+    if st == 2 and tot.value > idx.size:  # CASPHY_ERANGE: the lists need a bigger buffer
+        idx = np.empty(tot.value, dtype=np.uint32)
+        st = call(counts, idx.ctypes.data_as(C.c_void_p), idx.size, C.byref(tot))
+    _chk(st, "casphy_radius")
+    return counts[:ntip], (idx if idx.size == tot.value else idx[: tot.value].copy())
 
 
 def radius_bit(bmat, w, radius):

@@ -123,7 +123,10 @@ int casphy_node_keep_bit(uint32_t nnodeRows, uint32_t nbin, const uint32_t *node
  * radius the integer argv value.  counts[ntip] receives the .nNeighbor body;
  * when idx is non-NULL and idx_cap >= the total, idx receives the .idx body
  * (for every row the ascending rows j with score >= radius).  *total gets the
- * list length either way (call once with idx = NULL to size the buffer).
+ * list length either way.  Either call once with idx = NULL to size the
+ * buffer, or pass a buffer of a guessed size: when the lists do not fit, the
+ * call returns CASPHY_ERANGE with counts and *total filled (*total > idx_cap)
+ * and a second call with a large enough buffer is needed.
  */
 int casphy_radius_bit(uint32_t nrow, uint32_t ntip, const uint32_t *bmat, const double *weight,
                       int32_t radius, uint32_t *counts, uint32_t *idx, uint64_t idx_cap,
