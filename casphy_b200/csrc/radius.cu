@@ -17,6 +17,7 @@
 // candidate rows, one warp ballot per 32 candidates), rows are counted, and
 // a second launch expands the bits into the ascending index lists.
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <vector>
 
@@ -270,12 +271,17 @@ static int prep_dna(RadiusInput& in, u32 ntip, u32 nbinRaw, const u32* raw, u32 
 
 // Lists of the query rows [row0, row1) (counts[0 .. row1-row0) and their
 // concatenated index lists); the whole matrix is [0, ntip).
-static int radius_impl(RadiusInput& in, u32 row0, u32 row1, u32* counts, u32* idx, u64 cap, u64* total) {
+// allocOut non-null: the lists go to a host buffer of the exact size,
+// allocated here once they are counted (freed with casphy_free).
+static int radius_impl(RadiusInput& in, u32 row0, u32 row1, u32* counts, u32* idx, u64 cap, u64* total,
+                       u32** allocOut = nullptr) {
     if (!counts || row0 > row1 || row1 > in.ntip) return CASPHY_EINVAL;
     const u32 ntip = in.ntip, nq = row1 - row0;
+    if (allocOut) *allocOut = nullptr;
     if (nq == 0) {
         if (total) *total = 0;
-        return CASPHY_OK;
+        if (allocOut) *allocOut = static_cast<u32*>(std::malloc(sizeof(u32)));
+        return allocOut && !*allocOut ? CASPHY_ENOMEM : CASPHY_OK;
     }
     const u32 maskWords = (ntip + 31) / 32;
     const size_t smem = sizeof(u32) * kQ * in.nwords;
@@ -333,6 +339,12 @@ static int radius_impl(RadiusInput& in, u32 row0, u32 row1, u32* counts, u32* id
         tot += counts[i];
     }
     if (total) *total = tot;
+    if (allocOut) {
+        idx = static_cast<u32*>(std::malloc(sizeof(u32) * (tot ? tot : 1)));
+        if (!idx) return CASPHY_ENOMEM;
+        cap = tot;
+        *allocOut = idx;
+    }
     if (!idx) return CASPHY_OK;
     if (tot > cap) return CASPHY_ERANGE;
     // the index lists get the second block: their size is only known now
@@ -433,6 +445,40 @@ extern "C" int casphy_radius_dna_rows(uint32_t ntip, uint32_t nbinRaw, const uin
     if (rc) return rc;
     return casphy::radius_impl(in, row_begin, row_end, counts, idx, idx_cap, total);
 }
+
+extern "C" int casphy_radius_bit_lists(uint32_t nrow, uint32_t ntip, const uint32_t* bmat, const double* weight,
+                                       int32_t radius, uint32_t* counts, uint32_t** idx_out, uint64_t* total) {
+    int rc = casphy::require_device();
+    if (rc) return rc;
+    if (!idx_out) return CASPHY_EINVAL;
+    casphy::RadiusInput in;
+    rc = casphy::prep_bit(in, nrow, ntip, bmat, weight, radius);
+    if (rc) return rc;
+    rc = casphy::radius_impl(in, 0, ntip, counts, nullptr, 0, total, idx_out);
+    if (rc && *idx_out) {
+        std::free(*idx_out);
+        *idx_out = nullptr;
+    }
+    return rc;
+}
+
+extern "C" int casphy_radius_dna_lists(uint32_t ntip, uint32_t nbinRaw, const uint32_t* raw, uint32_t radius,
+                                       uint32_t* counts, uint32_t** idx_out, uint64_t* total) {
+    int rc = casphy::require_device();
+    if (rc) return rc;
+    if (!idx_out) return CASPHY_EINVAL;
+    casphy::RadiusInput in;
+    rc = casphy::prep_dna(in, ntip, nbinRaw, raw, radius);
+    if (rc) return rc;
+    rc = casphy::radius_impl(in, 0, ntip, counts, nullptr, 0, total, idx_out);
+    if (rc && *idx_out) {
+        std::free(*idx_out);
+        *idx_out = nullptr;
+    }
+    return rc;
+}
+
+extern "C" void casphy_free(void* p) { std::free(p); }
 
 extern "C" int casphy_try_radius_bit(uint32_t nrow, uint32_t ntip, const uint32_t* bmat, const double* weight,
                                      int32_t radius, uint32_t nrep, const uint32_t* qidx, uint32_t* counts) {

@@ -29,17 +29,14 @@ int main(int argc, char* argv[]) {
     if (dev < 0) return tool::fail("radiusNeighborDNA", CASPHY_ENODEV);
     std::vector<uint32_t> counts(ntip);
     uint64_t total = 0;
-    // one search when the lists fit a guessed buffer, a second only when not
-    std::vector<uint32_t> idx(std::max<size_t>((size_t)64 * ntip, (size_t)1 << 16));
-    int rc = casphy_radius_dna(ntip, nbinRaw, raw.data(), radius, counts.data(), idx.data(), idx.size(), &total);
-    if (rc == CASPHY_ERANGE && total > idx.size()) {
-        idx.assign(total, 0u);
-        rc = casphy_radius_dna(ntip, nbinRaw, raw.data(), radius, counts.data(), idx.data(), idx.size(), &total);
-    }
+    // one search: the library allocates the lists at their counted size
+    uint32_t* lists = nullptr;
+    const int rc = casphy_radius_dna_lists(ntip, nbinRaw, raw.data(), radius, counts.data(), &lists, &total);
     if (rc) return tool::fail("radiusNeighborDNA", rc);
-    if (!tool::write_raw(prefix + ".idx", idx.data(), sizeof(uint32_t) * total) ||
-        !tool::write_mat(prefix + ".nNeighbor", 1, ntip, counts.data(), ntip))
-        return 1;
+    const bool ok = tool::write_raw(prefix + ".idx", lists, sizeof(uint32_t) * total) &&
+                    tool::write_mat(prefix + ".nNeighbor", 1, ntip, counts.data(), ntip);
+    casphy_free(lists);
+    if (!ok) return 1;
     printf("radiusNeighborDNA: %.2fs elapsed for %u tips.\n", tool::now_s() - t0, ntip);
     return 0;
 }

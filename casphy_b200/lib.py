@@ -92,6 +92,11 @@ def lib():
         L.casphy_radius_bit.argtypes = [u32, u32, _u32p, _f64p, C.c_int32, _u32p, vp, C.c_uint64,
                                         C.POINTER(C.c_uint64)]
         L.casphy_radius_dna.argtypes = [u32, u32, _u32p, u32, _u32p, vp, C.c_uint64, C.POINTER(C.c_uint64)]
+        _pp = C.POINTER(C.POINTER(C.c_uint32))
+        L.casphy_radius_bit_lists.argtypes = [u32, u32, _u32p, _f64p, C.c_int32, _u32p, _pp, C.POINTER(C.c_uint64)]
+        L.casphy_radius_dna_lists.argtypes = [u32, u32, _u32p, u32, _u32p, _pp, C.POINTER(C.c_uint64)]
+        L.casphy_free.argtypes = [vp]
+        L.casphy_free.restype = None
         L.casphy_radius_bit_rows.argtypes = [u32, u32, _u32p, _f64p, C.c_int32, u32, u32, _u32p, vp, C.c_uint64,
                                              C.POINTER(C.c_uint64)]
         L.casphy_radius_dna_rows.argtypes = [u32, u32, _u32p, u32, u32, u32, _u32p, vp, C.c_uint64,
@@ -186,19 +191,34 @@ def _lists(call, ntip):
     return counts[:ntip], (idx if idx.size == tot.value else idx[: tot.value].copy())
 
 
+def _lists_owned(call, ntip):
+    """One search; the lists stay in the library's exact-size host buffer,
+    viewed without a copy and released with casphy_free when the array goes."""
+    import weakref
+    counts = np.zeros(max(ntip, 1), dtype=np.uint32)
+    tot = C.c_uint64(0)
+    ptr = C.POINTER(C.c_uint32)()
+    _chk(call(counts, C.byref(ptr), C.byref(tot)), "casphy_radius")
+    n = tot.value
+    idx = np.ctypeslib.as_array(ptr, shape=(max(n, 1),))
+    weakref.finalize(idx.base, lib().casphy_free, C.cast(ptr, C.c_void_p))
+    return counts[:ntip], idx[:n]
+
+
 def radius_bit(bmat, w, radius):
     """radiusNeighbor: bmat (nrow words, ntip) word-plane-major -> (counts, idx)."""
     bmat = _u32(bmat)
     nrow, ntip = bmat.shape
     w = np.ascontiguousarray(w, dtype=np.float64)
-    return _lists(lambda c, i, cap, t: lib().casphy_radius_bit(nrow, ntip, bmat, w, int(radius), c, i, cap, t), ntip)
+    return _lists_owned(lambda c, p, t: lib().casphy_radius_bit_lists(nrow, ntip, bmat, w, int(radius), c, p, t),
+                        ntip)
 
 
 def radius_dna(raw, radius):
     """radiusNeighborDNA on fasta2bin rows -> (counts, idx)."""
     raw = _u32(raw)
     ntip, nb = raw.shape
-    return _lists(lambda c, i, cap, t: lib().casphy_radius_dna(ntip, nb, raw, int(radius), c, i, cap, t), ntip)
+    return _lists_owned(lambda c, p, t: lib().casphy_radius_dna_lists(ntip, nb, raw, int(radius), c, p, t), ntip)
 
 
 def radius_bit_rows(bmat, w, radius, row_begin, row_end):

@@ -135,6 +135,16 @@ int casphy_radius_bit(uint32_t nrow, uint32_t ntip, const uint32_t *bmat, const 
  * .bin body (ntip x nbinRaw u32, four 8-bit codes per word). */
 int casphy_radius_dna(uint32_t ntip, uint32_t nbinRaw, const uint32_t *raw, uint32_t radius,
                       uint32_t *counts, uint32_t *idx, uint64_t idx_cap, uint64_t *total);
+/* The same searches with the lists in a host buffer the library allocates
+ * at their exact size once they are counted, so every search runs once
+ * whatever its result size (the caller-buffer forms above need a second
+ * search when the lists outgrow the buffer).  *idx_out receives the .idx body
+ * (total entries), to be released with casphy_free; on failure it is NULL. */
+int casphy_radius_bit_lists(uint32_t nrow, uint32_t ntip, const uint32_t *bmat, const double *weight,
+                            int32_t radius, uint32_t *counts, uint32_t **idx_out, uint64_t *total);
+int casphy_radius_dna_lists(uint32_t ntip, uint32_t nbinRaw, const uint32_t *raw, uint32_t radius,
+                            uint32_t *counts, uint32_t **idx_out, uint64_t *total);
+void casphy_free(void *p);
 /* The lists of query rows [row_begin, row_end) only (counts has row_end -
  * row_begin entries, idx their concatenated lists): one GPU's share when the
  * rows are split over several GPUs. */

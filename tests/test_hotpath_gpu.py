@@ -123,3 +123,21 @@ def test_radius_row_ranges_concatenate_to_full_lists(gpu_lib):
     parts = [gpu_lib.radius_dna_rows(raw, r, lo, hi) for lo, hi in ((0, 250), (250, 251), (251, 500))]
     assert np.array_equal(np.concatenate([p[0] for p in parts]), dc)
     assert np.array_equal(np.concatenate([p[1] for p in parts]), di)
+
+
+def test_radius_lists_outgrowing_the_guess(gpu_lib):
+    """Radius 0 makes every pair a neighbour: the row-range call's guessed
+    buffer (64 per row) is too small and it searches again into an exact one;
+    the full call's library-allocated lists come from one search.  Both equal
+    the oracle's."""
+    from casphy_b200 import synth
+    words = synth.binary_workload(1500, 64, 10, 0.05, 0.05, seed=32)
+    bmat = np.ascontiguousarray(words.T)
+    w = np.ones(64)
+    c0, i0 = O.radius_bit(bmat, w, 0)
+    c1, i1 = gpu_lib.radius_bit(bmat, w, 0)
+    c2, i2 = gpu_lib.radius_bit_rows(bmat, w, 0, 0, 1500)
+    assert int(c0.sum()) == 1500 * 1500
+    assert np.array_equal(c1, c0) and np.array_equal(i1, i0)
+    assert np.array_equal(c2, c0) and np.array_equal(i2, i0)
+    del i1  # the library's list buffer is released with the array
