@@ -131,7 +131,7 @@ def test_radius_lists_outgrowing_the_guess(gpu_lib):
     the full call's library-allocated lists come from one search.  Both equal
     the oracle's."""
     from casphy_b200 import synth
-    words = synth.binary_workload(1500, 64, 10, 0.05, 0.05, seed=32)
+    words = synth.binary_workload(1500, 64, 11, 0.05, 0.05, seed=32)
     bmat = np.ascontiguousarray(words.T)
     w = np.ones(64)
     c0, i0 = O.radius_bit(bmat, w, 0)
