@@ -245,34 +245,60 @@ __global__ void __launch_bounds__(kThreads) k_init_scan(InitArgs a) {
 // ---------------------------------------------------------------------------
 // persistent join loop: the dense (column-major u16) model for the engine
 
+__device__ __forceinline__ u32 merge_code(int mode, u32 x, u32 y) {
+    if (mode == 0 || mode == 2) return x;
+    if (mode == 1) return y;
+    return (x == 0) ? y : ((y >= 1 && x != y) ? 1u : x);
+}
+
 // Builds the query site list (ascending sites with code > 1) from a row.
 // mode 0: query = row1; 1: copy row2; 2: keep row1; 3: ancestral merge of
 // row1 and row2 (updateAncestralKernel, cu/joinEdgeIndel.cu:87-99).  When
-// mrow is given the row is also left there for the write-back.
+// mrow is given the row is also left there for the write-back, and when orow
+// is given row1 itself (all ncolP entries) is left there too.
+// With at most kPerSmall sites per thread (ncolP <= 2048) every thread issues
+// all its row loads before it uses one, so the build costs one L2 round trip.
+constexpr u32 kPerSmall = 4;
 __device__ int build_indel_query(u32 ncol, u32 ncolP, int unitW, const u16* Wsel, const u16* row1, const u16* row2,
-                                 int mode, u16* mrow, u32* eSC, u16* eW, u32* wcount) {
+                                 int mode, u16* mrow, u16* orow, u32* eSC, u16* eW, u32* wcount) {
     const u32 lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const u32 per = (ncolP + kThreads - 1) / kThreads;
     const u32 s0 = threadIdx.x * per;
+    const bool wantX = mode != 1 || orow != nullptr, wantY = mode == 1 || mode == 3;
     u32 cnt = 0;
-    u32 codes[4];
-    const bool small = per <= 4;
-    for (u32 i = 0; i < per; i++) {
-        const u32 s = s0 + i;
-        u32 c = 0;
-        if (s < ncol) {
-            const u32 x = ld_cg_u16(row1 + s);
-            if (mode == 0 || mode == 2) {
-                c = x;
-            } else {
-                const u32 y = ld_cg_u16(row2 + s);
-                if (mode == 1) c = y;
-                else c = (x == 0) ? y : ((y >= 1 && x != y) ? 1u : x);
-            }
+    u32 codes[kPerSmall];
+    const bool small = per <= kPerSmall;
+    if (small) {
+        u32 xs[kPerSmall], ys[kPerSmall];
+#pragma unroll
+        for (u32 i = 0; i < kPerSmall; i++) {
+            const u32 s = s0 + i;
+            xs[i] = (i < per && s < ncolP && wantX) ? (u32)ld_cg_u16(row1 + s) : 0u;
+            ys[i] = (i < per && s < ncol && wantY) ? (u32)ld_cg_u16(row2 + s) : 0u;
         }
-        if (s < ncolP && mrow) mrow[s] = (u16)c;
-        if (small) codes[i] = c;
-        cnt += c > 1;
+#pragma unroll
+        for (u32 i = 0; i < kPerSmall; i++) {
+            const u32 s = s0 + i;
+            const u32 c = (i < per && s < ncol) ? merge_code(mode, xs[i], ys[i]) : 0u;
+            if (i < per && s < ncolP) {
+                if (mrow) mrow[s] = (u16)c;
+                if (orow) orow[s] = (u16)xs[i];
+            }
+            codes[i] = c;
+            cnt += c > 1;
+        }
+    } else {
+        for (u32 i = 0; i < per; i++) {
+            const u32 s = s0 + i;
+            const u32 x = (s < ncolP && wantX) ? (u32)ld_cg_u16(row1 + s) : 0u;
+            const u32 y = (s < ncol && wantY) ? (u32)ld_cg_u16(row2 + s) : 0u;
+            const u32 c = s < ncol ? merge_code(mode, x, y) : 0u;
+            if (s < ncolP) {
+                if (mrow) mrow[s] = (u16)c;
+                if (orow) orow[s] = (u16)x;
+            }
+            cnt += c > 1;
+        }
     }
     u32 incl = cnt;
 #pragma unroll
@@ -295,15 +321,25 @@ __device__ int build_indel_query(u32 ncol, u32 ncolP, int unitW, const u16* Wsel
     }
     __syncthreads();
     u32 pos = wcount[16 + wid] + incl - cnt;
-    for (u32 i = 0; i < per; i++) {
-        const u32 s = s0 + i;
-        u32 c;
-        if (small) c = codes[i];
-        else c = (s < ncolP && mrow) ? mrow[s] : (s < ncol ? ld_cg_u16(row1 + s) : 0u);
-        if (c > 1) {
-            eSC[pos] = s | (c << 16);
-            eW[pos] = unitW ? (u16)1 : Wsel[(size_t)(c - 2) * ncol + s];
-            pos++;
+    if (small) {
+#pragma unroll
+        for (u32 i = 0; i < kPerSmall; i++) {
+            const u32 s = s0 + i, c = codes[i];
+            if (c > 1) {
+                eSC[pos] = s | (c << 16);
+                eW[pos] = unitW ? (u16)1 : Wsel[(size_t)(c - 2) * ncol + s];
+                pos++;
+            }
+        }
+    } else {
+        for (u32 i = 0; i < per; i++) {
+            const u32 s = s0 + i;
+            const u32 c = (s < ncolP && mrow) ? mrow[s] : (s < ncol ? ld_cg_u16(row1 + s) : 0u);
+            if (c > 1) {
+                eSC[pos] = s | (c << 16);
+                eW[pos] = unitW ? (u16)1 : Wsel[(size_t)(c - 2) * ncol + s];
+                pos++;
+            }
         }
     }
     const int n = (int)wcount[32];
@@ -340,7 +376,7 @@ struct IndelDense {
     __device__ static u16* col(const Args& m, u32 buf) { return buf ? m.colT[1] : m.colT[0]; }
     __device__ static int build_stale(const Args& m, Smem& s, u32 j1, u32* wc) {
         return build_indel_query(m.ncol, m.ncolP, m.unitW, m.Wsel, m.nodeRow + (size_t)j1 * m.ncolP, nullptr, 0,
-                                 nullptr, s.eSC, s.eW, wc);
+                                 nullptr, nullptr, s.eSC, s.eW, wc);
     }
     // minSize / minRatio rule of cu/joinEdgeIndel.cu:407-413
     __device__ static int build_join(const Args& m, Smem& s, u32 j1, u32 j2, u32 s1, u32 s2, u32* wc) {
@@ -349,7 +385,7 @@ struct IndelDense {
         else if (s2 < m.minSize && __uint2float_rn(s2) * m.minRatio < __uint2float_rn(s1)) mode = 2;
         else mode = 3;
         return build_indel_query(m.ncol, m.ncolP, m.unitW, m.Wsel, m.nodeRow + (size_t)j1 * m.ncolP,
-                                 m.nodeRow + (size_t)j2 * m.ncolP, mode, s.mrow, s.eSC, s.eW, wc);
+                                 m.nodeRow + (size_t)j2 * m.ncolP, mode, s.mrow, nullptr, s.eSC, s.eW, wc);
     }
     __device__ static void store_node(const Args& m, Smem& s, u32 newNode) {
         u16* dst = m.nodeRow + (size_t)newNode * m.ncolP;
@@ -596,17 +632,16 @@ struct IndelBits {
     __device__ static u32* bitsOf(const Args& m, u32 buf) { return buf ? m.bits[1] : m.bits[0]; }
     __device__ static int build_stale(const Args& m, Smem& s, u32 j1, u32* wc) {
         return build_indel_query(m.ncol, m.ncolP, m.unitW, m.Wsel, m.nodeRow + (size_t)j1 * m.ncolP, nullptr, 0,
-                                 nullptr, s.eSC, s.eW, wc);
+                                 nullptr, nullptr, s.eSC, s.eW, wc);
     }
     __device__ static int build_join(const Args& m, Smem& s, u32 j1, u32 j2, u32 s1, u32 s2, u32* wc) {
         int mode;
         if (s1 < m.minSize && __uint2float_rn(s1) * m.minRatio < __uint2float_rn(s2)) mode = 1;
         else if (s2 < m.minSize && __uint2float_rn(s2) * m.minRatio < __uint2float_rn(s1)) mode = 2;
         else mode = 3;
-        const u16* r1 = m.nodeRow + (size_t)j1 * m.ncolP;
-        for (u32 i = threadIdx.x; i < m.ncolP; i += kThreads) s.orow[i] = ld_cg_u16(r1 + i);
-        return build_indel_query(m.ncol, m.ncolP, m.unitW, m.Wsel, r1, m.nodeRow + (size_t)j2 * m.ncolP, mode,
-                                 s.mrow, s.eSC, s.eW, wc);
+        // j1's row is left in orow for store_slot by the same loads
+        return build_indel_query(m.ncol, m.ncolP, m.unitW, m.Wsel, m.nodeRow + (size_t)j1 * m.ncolP,
+                                 m.nodeRow + (size_t)j2 * m.ncolP, mode, s.mrow, s.orow, s.eSC, s.eW, wc);
     }
     __device__ static void store_node(const Args& m, Smem& s, u32 newNode) {
         u16* dst = m.nodeRow + (size_t)newNode * m.ncolP;
