@@ -190,3 +190,20 @@ def test_benchmark_small_case_reaches_fp64_optimum(gpu_lib):
     assert abs(la - best) <= 1e-6 * abs(best)
     assert lf <= la + 1e-7 * abs(la)
     assert abs(sa["loglik_end"] - la) <= LL_RTOL * abs(la)
+
+
+def test_parsimony_warm_start_edit_model(gpu_lib):
+    """The bench's edit-model leg on a small join tree: charAncestralEC on the
+    GPU equals the oracle, and L-BFGS started from the parsimony times
+    (casphy_b200.branch_lengths.parsimony_start) starts higher than the flat
+    start and ends at the same optimum."""
+    import bench
+    raw = synth.lineage_states(1500, 256, 11, 0.04, 32, 1.5, 0.1, 21)
+    codes, nstate = synth.regularize(raw)
+    edge, _, _ = gpu_lib.join_indel(codes, nstate, np.ones((nstate, 256)))
+    res = bench.blopt_c5(gpu_lib, codes, nstate, edge)
+    par = res["charAncestralEC"]
+    ws = par["warm_start"]
+    assert par["identical"]
+    assert ws["loglik_start"] > res["loglik_start"]
+    assert abs(ws["loglik_end_rel_diff_to_flat_start"]) <= 1e-6
