@@ -363,6 +363,232 @@ done:
 }
 
 /* ------------------------------------------------------------------ */
+/* A phased schedule of the same indel join: fewer decision rounds, the  */
+/* same tree.  This is test infrastructure for a parallel engine (one    */
+/* phase = one round of decisions between grid barriers), not a          */
+/* restatement of the reference; it checks two rules against             */
+/* oracle_join_indel above.                                              */
+/*  - Stale rescans run early: a row whose partner died is rescanned     */
+/*    together with every other such row whose stored value beats the    */
+/*    best fresh record (up to maxBatch rows, in decision order).  A     */
+/*    rescan gives the row's true best over the live rows, and the join  */
+/*    decision is the best true value, so rescanning early never changes */
+/*    a decision.                                                        */
+/*  - Two joins in one phase: when the phase joins a and b into n, let    */
+/*    (c -> d) be the best record among the other rows.  If d is alive   */
+/*    and is neither a nor b, and no row that n improves gets a record   */
+/*    that beats (c -> d), the sequential loop's next decision is the    */
+/*    join of c and d, so it is done in the same phase.                  */
+/* ------------------------------------------------------------------ */
+
+typedef struct {
+    JoinBook b;
+    IndelCtx k;
+    u32 ntip, ncol, minSize, nodeCount;
+    float minRatio;
+    u16 *localMax, *shared;
+    u32 *cache, *rawState, *nodeSize;
+    u64 nPairs;
+    int nthreads;
+} IndelRun;
+
+/* One join of cache rows c1 (node j1) and c2 (node j2), as the sequential
+ * loop does it.  When `ok` is given it is cleared if a row improved by the
+ * new node gets a record that beats (vcd, cNode). */
+static void indel_join_step(IndelRun *R, u32 j1, u32 j2, u32 c1, u32 c2, double vcd, u32 cNode, int *ok) {
+    JoinBook *b = &R->b;
+    const u32 ntip = R->ntip, ncol = R->ncol, nodeCount = R->nodeCount;
+    const u32 r = nodeCount - ntip;
+    memcpy(R->rawState + (size_t)(2 * r) * ncol, R->cache + (size_t)c1 * ncol, sizeof(u32) * ncol);
+    memcpy(R->rawState + (size_t)(2 * r + 1) * ncol, R->cache + (size_t)c2 * ncol, sizeof(u32) * ncol);
+    const u32 s1 = R->nodeSize[j1], s2 = R->nodeSize[j2];
+    if (s1 < R->minSize && (float)s1 * R->minRatio < (float)s2)
+        memcpy(R->cache + (size_t)c1 * ncol, R->cache + (size_t)c2 * ncol, sizeof(u32) * ncol);
+    else if (!(s2 < R->minSize && (float)s2 * R->minRatio < (float)s1))
+        indel_merge(R->cache + (size_t)c1 * ncol, R->cache + (size_t)c2 * ncol, ncol);
+    R->nodeSize[nodeCount] = s1 + s2;
+    b->rawEdge[4 * r] = nodeCount; b->rawEdge[4 * r + 1] = j1;
+    b->rawEdge[4 * r + 2] = nodeCount; b->rawEdge[4 * r + 3] = j2;
+    b->node2cache[j1] = ntip; b->node2cache[j2] = ntip; b->node2cache[nodeCount] = c1;
+    b->cache2node[c1] = nodeCount; b->cache2node[c2] = b->nnode;
+    book_remove_valid(b, c2);
+    u16 *shared = R->shared;
+#pragma omp parallel for num_threads(R->nthreads) schedule(static)
+    for (long p = 0; p < (long)b->nvalid; p++) {
+        u32 c = b->valid[p];
+        if (c != c1) shared[c] = indel_score(&R->k, c1, c);
+    }
+    R->nPairs += b->nvalid - 1;
+    for (u32 p = 0; p < b->nvalid; p++) {
+        u32 c = b->valid[p];
+        if (c == c1) continue;
+        const double v = oracle_f16_to_f64(shared[c]);
+        if (v > oracle_f16_to_f64(R->localMax[c])) {
+            if (ok && better(v, b->cache2node[c], vcd, cNode)) *ok = 0;
+            R->localMax[c] = shared[c];
+            b->localMaxIdx[c] = nodeCount;
+        }
+    }
+    R->localMax[c1] = H_NEG_ONE;
+    R->localMax[c2] = H_NEG_ONE;
+    R->nodeCount++;
+}
+
+/* Rescan of cache row t against every valid row (the sequential loop's
+ * stale step). */
+static void indel_rescan(IndelRun *R, u32 t) {
+    JoinBook *b = &R->b;
+    u16 *shared = R->shared;
+#pragma omp parallel for num_threads(R->nthreads) schedule(static)
+    for (long p = 0; p < (long)b->nvalid; p++) {
+        u32 c = b->valid[p];
+        shared[c] = c == t ? H_NEG_ONE : indel_score(&R->k, t, c);
+    }
+    R->nPairs += b->nvalid - 1;
+    double bv = -1.0;
+    u32 bi = 0;
+    for (u32 p = 0; p < b->nvalid; p++) {
+        u32 c = b->valid[p];
+        double v = oracle_f16_to_f64(shared[c]);
+        if (better(v, b->cache2node[c], bv, bi)) { bv = v; bi = b->cache2node[c]; }
+    }
+    R->localMax[t] = oracle_f64_to_f16(bv);
+    b->localMaxIdx[t] = bi;
+}
+
+static int rec_fresh(const IndelRun *R, u32 c) {
+    const u32 d = R->b.localMaxIdx[c];
+    return d < R->b.nnode && R->b.node2cache[d] < R->ntip;
+}
+
+int oracle_join_indel_phased(uint32_t ntip, uint32_t ncol, const uint32_t *codes, uint32_t nState,
+                             const double *w, const uint32_t *tipSize, uint32_t minSize, float minRatio,
+                             uint32_t maxBatch, int pairJoins, uint32_t *edge_out, uint32_t *state_out,
+                             uint64_t *stats, int nthreads) {
+    if (ntip == 0 || ncol == 0 || maxBatch == 0) return ORACLE_EINVAL;
+    for (size_t i = 0; i < (size_t)ntip * ncol; i++)
+        if (codes[i] > 1 && codes[i] - 2 >= nState) return ORACLE_ERANGE;
+    IndelRun R;
+    memset(&R, 0, sizeof(R));
+    R.ntip = ntip; R.ncol = ncol; R.minSize = minSize; R.minRatio = minRatio;
+    R.nthreads = nthreads_or_default(nthreads);
+    const size_t nw = (size_t)nState * ncol;
+    const u32 nnode = 2 * ntip - 1;
+    u16 *w16 = (u16 *)malloc(sizeof(u16) * (nw ? nw : 1));
+    u16 *wint = NULL;
+    u32 *batch = (u32 *)malloc(sizeof(u32) * ntip);
+    R.cache = (u32 *)malloc(sizeof(u32) * (size_t)ntip * ncol);
+    R.localMax = (u16 *)malloc(sizeof(u16) * ntip);
+    R.shared = (u16 *)malloc(sizeof(u16) * ntip);
+    R.rawState = (u32 *)malloc(sizeof(u32) * (size_t)nnode * ncol);
+    R.nodeSize = (u32 *)malloc(sizeof(u32) * (size_t)ntip * 2);
+    int st = book_init(&R.b, ntip);
+    if (st || !w16 || !batch || !R.cache || !R.localMax || !R.shared || !R.rawState || !R.nodeSize) {
+        st = ORACLE_ENOMEM;
+        goto done;
+    }
+    for (size_t i = 0; i < nw; i++) w16[i] = oracle_f64_to_f16(w[i]);
+    memcpy(R.cache, codes, sizeof(u32) * (size_t)ntip * ncol);
+    memcpy(R.nodeSize, tipSize, sizeof(u32) * ntip);
+    wint = oracle_force_f16 ? NULL : exact_int_weights(w16, nState, ncol);
+    R.k.ncol = ncol; R.k.cache = R.cache; R.k.w16 = w16; R.k.wint = wint;
+    JoinBook *b = &R.b;
+    u64 nStale = 0, nJoin = 0, nPhase = 0, nPaired = 0;
+
+    for (u32 i = 0; i + 1 < ntip; i++) {
+#pragma omp parallel for num_threads(R.nthreads) schedule(static)
+        for (long j = (long)i + 1; j < (long)ntip; j++) R.shared[j] = indel_score(&R.k, i, (u32)j);
+        double bv = -1.0;
+        u32 bi = 0;
+        for (u32 j = i + 1; j < ntip; j++) {
+            double v = oracle_f16_to_f64(R.shared[j]);
+            if (better(v, j, bv, bi)) { bv = v; bi = j; }
+        }
+        R.localMax[i] = oracle_f64_to_f16(bv);
+        b->localMaxIdx[i] = bi;
+        R.nPairs += ntip - i - 1;
+    }
+    R.localMax[ntip - 1] = H_NEG_ONE;
+    R.nodeCount = ntip;
+
+    while (R.nodeCount < nnode) {
+        double bv = -1.0, fv = -1.0;
+        u32 bi = 0, fi = 0;
+        for (u32 c = 0; c < ntip; c++) {
+            const double v = oracle_f16_to_f64(R.localMax[c]);
+            const u32 node = b->cache2node[c];
+            if (better(v, node, bv, bi)) { bv = v; bi = node; }
+            if (node < nnode && rec_fresh(&R, c) && better(v, node, fv, fi)) { fv = v; fi = node; }
+        }
+        const u32 j1 = bi;
+        if (j1 >= nnode || b->node2cache[j1] >= ntip) { st = ORACLE_EINTERNAL; goto done; }
+        const u32 c1 = b->node2cache[j1];
+        if (!rec_fresh(&R, c1)) {
+            /* one phase: the stale rows that beat the best fresh record, best first */
+            u32 n = 0;
+            for (u32 c = 0; c < ntip; c++) {
+                const u32 node = b->cache2node[c];
+                if (node >= nnode || rec_fresh(&R, c)) continue;
+                const double v = oracle_f16_to_f64(R.localMax[c]);
+                if (v >= 0 && better(v, node, fv, fi)) batch[n++] = c;
+            }
+            for (u32 x = 1; x < n; x++) { /* insertion sort, decision order */
+                const u32 t = batch[x];
+                const double tv = oracle_f16_to_f64(R.localMax[t]);
+                u32 y = x;
+                while (y > 0 && better(tv, b->cache2node[t], oracle_f16_to_f64(R.localMax[batch[y - 1]]),
+                                       b->cache2node[batch[y - 1]])) {
+                    batch[y] = batch[y - 1];
+                    y--;
+                }
+                batch[y] = t;
+            }
+            if (n == 0 || batch[0] != c1) { st = ORACLE_EINTERNAL; goto done; }
+            if (n > maxBatch) n = maxBatch;
+            for (u32 x = 0; x < n; x++) indel_rescan(&R, batch[x]);
+            nStale += n;
+            nPhase++;
+            continue;
+        }
+        const u32 j2 = b->localMaxIdx[c1], c2 = b->node2cache[j2];
+        /* the best record among the other rows, before this join */
+        double vcd = -1.0;
+        u32 cNode = 0;
+        for (u32 c = 0; c < ntip; c++) {
+            if (c == c1 || c == c2) continue;
+            const double v = oracle_f16_to_f64(R.localMax[c]);
+            if (better(v, b->cache2node[c], vcd, cNode)) { vcd = v; cNode = b->cache2node[c]; }
+        }
+        int ok = 0;
+        u32 cc = ntip, dNode = nnode;
+        if (pairJoins && vcd >= 0 && cNode < nnode && b->node2cache[cNode] < ntip) {
+            cc = b->node2cache[cNode];
+            dNode = b->localMaxIdx[cc];
+            ok = rec_fresh(&R, cc) && dNode != j1 && dNode != j2;
+        }
+        indel_join_step(&R, j1, j2, c1, c2, vcd, cNode, ok ? &ok : NULL);
+        nJoin++;
+        nPhase++;
+        if (ok && R.nodeCount < nnode) {
+            indel_join_step(&R, cNode, dNode, cc, b->node2cache[dNode], 0.0, 0, NULL);
+            nJoin++;
+            nPaired++;
+        }
+    }
+    memcpy(R.rawState + (size_t)(nnode - 1) * ncol, R.cache + (size_t)b->node2cache[R.nodeCount - 1] * ncol,
+           sizeof(u32) * ncol);
+    st = dfs_output(b, R.rawState, ncol, edge_out, state_out);
+    if (stats) {
+        stats[0] = nStale; stats[1] = R.nPairs; stats[2] = nJoin; stats[3] = nPhase; stats[4] = nPaired;
+    }
+done:
+    book_free(&R.b);
+    free(w16); free(wint); free(batch); free(R.cache); free(R.localMax); free(R.shared); free(R.rawState);
+    free(R.nodeSize);
+    return st;
+}
+
+/* ------------------------------------------------------------------ */
 /* joinEdgeBitReverse (cu/joinEdgeBitReverse.cu:53-121, 285-597)       */
 /* ------------------------------------------------------------------ */
 

@@ -37,6 +37,8 @@ def lib():
         L.oracle_f16_add.restype = C.c_uint16
         L.oracle_join_indel.argtypes = [u32, u32, _u32p, u32, _f64p, _u32p, u32, f32,
                                         _u32p, _u32p, _u64p, i]
+        L.oracle_join_indel_phased.argtypes = [u32, u32, _u32p, u32, _f64p, _u32p, u32, f32, u32, i,
+                                               _u32p, _u32p, _u64p, i]
         L.oracle_join_bit.argtypes = [u32, u32, _u32p, _f64p, i, _u32p, _u32p, _u64p, i]
         for name in ("oracle_node_keep_indel", "oracle_node_keep_bit"):
             getattr(L, name).argtypes = [u32, u32, _u32p, u32, _u32p, u32, _u32p, u32,
@@ -73,6 +75,24 @@ def join_indel(codes, nstate, w, tip_size=None, min_size=0, min_ratio=2.0, nthre
     stats = np.zeros(3, dtype=np.uint64)
     _chk(lib().oracle_join_indel(ntip, ncol, codes, nstate, w, ts, min_size, min_ratio,
                                  edge, state, stats, nthreads or os.cpu_count()), "join_indel")
+    return edge[: 2 * nedge].reshape(nedge, 2), state.reshape(-1, ncol), stats
+
+
+def join_indel_phased(codes, nstate, w, tip_size=None, min_size=0, min_ratio=2.0, max_batch=8, pair_joins=True,
+                      nthreads=0):
+    """The indel join in phases (oracle_join_indel_phased); stats adds
+    [3] phases and [4] phases with two joins."""
+    codes = _u32(codes)
+    ntip, ncol = codes.shape
+    w = np.ascontiguousarray(w, dtype=np.float64).reshape(-1)
+    ts = _u32(np.ones(ntip) if tip_size is None else tip_size)
+    nedge = 2 * ntip - 2
+    edge = np.zeros(max(nedge, 1) * 2, dtype=np.uint32)
+    state = np.zeros(max(ntip - 1, 1) * ncol, dtype=np.uint32)
+    stats = np.zeros(5, dtype=np.uint64)
+    _chk(lib().oracle_join_indel_phased(ntip, ncol, codes, nstate, w, ts, min_size, min_ratio, max_batch,
+                                        1 if pair_joins else 0, edge, state, stats, nthreads or os.cpu_count()),
+         "join_indel_phased")
     return edge[: 2 * nedge].reshape(nedge, 2), state.reshape(-1, ncol), stats
 
 
