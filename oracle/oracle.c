@@ -363,11 +363,11 @@ done:
 }
 
 /* ------------------------------------------------------------------ */
-/* A phased schedule of the same indel join: fewer decision rounds, the  */
-/* same tree.  This is test infrastructure for a parallel engine (one    */
-/* phase = one round of decisions between grid barriers), not a          */
-/* restatement of the reference; it checks two rules against             */
-/* oracle_join_indel above.                                              */
+/* The greedy join on a phased schedule: fewer decision rounds, the same */
+/* tree.  This is test infrastructure for a parallel engine (one phase = */
+/* one round of decisions between grid barriers), not a restatement of   */
+/* the reference; it checks two rules against the sequential joins above */
+/* and below, for either scoring model.                                  */
 /*  - Stale rescans run early: a row whose partner died is rescanned     */
 /*    together with every other such row whose stored value beats the    */
 /*    best fresh record (up to maxBatch rows, in decision order).  A     */
@@ -379,164 +379,148 @@ done:
 /*    and is neither a nor b, and no row that n improves gets a record   */
 /*    that beats (c -> d), the sequential loop's next decision is the    */
 /*    join of c and d, so it is done in the same phase.                  */
+/* Values are held as doubles: each model's stored values (binary16 or   */
+/* binary32) convert exactly, so comparisons are those of its own loop.  */
 /* ------------------------------------------------------------------ */
 
 typedef struct {
+    void *ctx;
+    double (*score)(void *ctx, u32 q, u32 c);                  /* as the model stores it */
+    void (*row_out)(void *ctx, u32 c, u32 *dst);               /* a cache row's output state */
+    void (*merge)(void *ctx, u32 c1, u32 c2, u32 j1, u32 j2, u32 newNode); /* new node into row c1 */
+    u32 rowlen;
+} PhasedModel;
+
+typedef struct {
     JoinBook b;
-    IndelCtx k;
-    u32 ntip, ncol, minSize, nodeCount;
-    float minRatio;
-    u16 *localMax, *shared;
-    u32 *cache, *rawState, *nodeSize;
+    const PhasedModel *m;
+    u32 ntip, nodeCount;
+    double *localMax, *shared;
+    u32 *rawState;
     u64 nPairs;
     int nthreads;
-} IndelRun;
+} PhasedRun;
 
 /* One join of cache rows c1 (node j1) and c2 (node j2), as the sequential
- * loop does it.  When `ok` is given it is cleared if a row improved by the
+ * loops do it.  When `ok` is given it is cleared if a row improved by the
  * new node gets a record that beats (vcd, cNode). */
-static void indel_join_step(IndelRun *R, u32 j1, u32 j2, u32 c1, u32 c2, double vcd, u32 cNode, int *ok) {
+static void phased_join(PhasedRun *R, u32 j1, u32 j2, u32 c1, u32 c2, double vcd, u32 cNode, int *ok) {
     JoinBook *b = &R->b;
-    const u32 ntip = R->ntip, ncol = R->ncol, nodeCount = R->nodeCount;
-    const u32 r = nodeCount - ntip;
-    memcpy(R->rawState + (size_t)(2 * r) * ncol, R->cache + (size_t)c1 * ncol, sizeof(u32) * ncol);
-    memcpy(R->rawState + (size_t)(2 * r + 1) * ncol, R->cache + (size_t)c2 * ncol, sizeof(u32) * ncol);
-    const u32 s1 = R->nodeSize[j1], s2 = R->nodeSize[j2];
-    if (s1 < R->minSize && (float)s1 * R->minRatio < (float)s2)
-        memcpy(R->cache + (size_t)c1 * ncol, R->cache + (size_t)c2 * ncol, sizeof(u32) * ncol);
-    else if (!(s2 < R->minSize && (float)s2 * R->minRatio < (float)s1))
-        indel_merge(R->cache + (size_t)c1 * ncol, R->cache + (size_t)c2 * ncol, ncol);
-    R->nodeSize[nodeCount] = s1 + s2;
+    const PhasedModel *m = R->m;
+    const u32 ntip = R->ntip, nodeCount = R->nodeCount, r = nodeCount - ntip;
+    m->row_out(m->ctx, c1, R->rawState + (size_t)(2 * r) * m->rowlen);
+    m->row_out(m->ctx, c2, R->rawState + (size_t)(2 * r + 1) * m->rowlen);
+    m->merge(m->ctx, c1, c2, j1, j2, nodeCount);
     b->rawEdge[4 * r] = nodeCount; b->rawEdge[4 * r + 1] = j1;
     b->rawEdge[4 * r + 2] = nodeCount; b->rawEdge[4 * r + 3] = j2;
     b->node2cache[j1] = ntip; b->node2cache[j2] = ntip; b->node2cache[nodeCount] = c1;
     b->cache2node[c1] = nodeCount; b->cache2node[c2] = b->nnode;
     book_remove_valid(b, c2);
-    u16 *shared = R->shared;
+    double *shared = R->shared;
 #pragma omp parallel for num_threads(R->nthreads) schedule(static)
     for (long p = 0; p < (long)b->nvalid; p++) {
         u32 c = b->valid[p];
-        if (c != c1) shared[c] = indel_score(&R->k, c1, c);
+        if (c != c1) shared[c] = m->score(m->ctx, c1, c);
     }
     R->nPairs += b->nvalid - 1;
     for (u32 p = 0; p < b->nvalid; p++) {
         u32 c = b->valid[p];
         if (c == c1) continue;
-        const double v = oracle_f16_to_f64(shared[c]);
-        if (v > oracle_f16_to_f64(R->localMax[c])) {
-            if (ok && better(v, b->cache2node[c], vcd, cNode)) *ok = 0;
+        if (shared[c] > R->localMax[c]) {
+            if (ok && better(shared[c], b->cache2node[c], vcd, cNode)) *ok = 0;
             R->localMax[c] = shared[c];
             b->localMaxIdx[c] = nodeCount;
         }
     }
-    R->localMax[c1] = H_NEG_ONE;
-    R->localMax[c2] = H_NEG_ONE;
+    R->localMax[c1] = -1.0;
+    R->localMax[c2] = -1.0;
     R->nodeCount++;
 }
 
-/* Rescan of cache row t against every valid row (the sequential loop's
- * stale step). */
-static void indel_rescan(IndelRun *R, u32 t) {
+/* Rescan of cache row t against every valid row (the stale step). */
+static void phased_rescan(PhasedRun *R, u32 t) {
     JoinBook *b = &R->b;
-    u16 *shared = R->shared;
+    const PhasedModel *m = R->m;
+    double *shared = R->shared;
 #pragma omp parallel for num_threads(R->nthreads) schedule(static)
     for (long p = 0; p < (long)b->nvalid; p++) {
         u32 c = b->valid[p];
-        shared[c] = c == t ? H_NEG_ONE : indel_score(&R->k, t, c);
+        shared[c] = c == t ? -1.0 : m->score(m->ctx, t, c);
     }
     R->nPairs += b->nvalid - 1;
     double bv = -1.0;
     u32 bi = 0;
     for (u32 p = 0; p < b->nvalid; p++) {
         u32 c = b->valid[p];
-        double v = oracle_f16_to_f64(shared[c]);
-        if (better(v, b->cache2node[c], bv, bi)) { bv = v; bi = b->cache2node[c]; }
+        if (better(shared[c], b->cache2node[c], bv, bi)) { bv = shared[c]; bi = b->cache2node[c]; }
     }
-    R->localMax[t] = oracle_f64_to_f16(bv);
+    R->localMax[t] = bv;
     b->localMaxIdx[t] = bi;
 }
 
-static int rec_fresh(const IndelRun *R, u32 c) {
+static int phased_fresh(const PhasedRun *R, u32 c) {
     const u32 d = R->b.localMaxIdx[c];
     return d < R->b.nnode && R->b.node2cache[d] < R->ntip;
 }
 
-int oracle_join_indel_phased(uint32_t ntip, uint32_t ncol, const uint32_t *codes, uint32_t nState,
-                             const double *w, const uint32_t *tipSize, uint32_t minSize, float minRatio,
-                             uint32_t maxBatch, int pairJoins, uint32_t *edge_out, uint32_t *state_out,
-                             uint64_t *stats, int nthreads) {
-    if (ntip == 0 || ncol == 0 || maxBatch == 0) return ORACLE_EINVAL;
-    for (size_t i = 0; i < (size_t)ntip * ncol; i++)
-        if (codes[i] > 1 && codes[i] - 2 >= nState) return ORACLE_ERANGE;
-    IndelRun R;
+/* stats (nullable): [0] stale rescans, [1] pair-scores, [2] joins, [3]
+ * phases, [4] phases with two joins. */
+static int phased_join_run(const PhasedModel *m, u32 ntip, u32 maxBatch, int pairJoins, u32 *edge_out,
+                           u32 *state_out, u64 *stats, int nthreads) {
+    if (ntip == 0 || maxBatch == 0) return ORACLE_EINVAL;
+    PhasedRun R;
     memset(&R, 0, sizeof(R));
-    R.ntip = ntip; R.ncol = ncol; R.minSize = minSize; R.minRatio = minRatio;
+    R.m = m;
+    R.ntip = ntip;
     R.nthreads = nthreads_or_default(nthreads);
-    const size_t nw = (size_t)nState * ncol;
     const u32 nnode = 2 * ntip - 1;
-    u16 *w16 = (u16 *)malloc(sizeof(u16) * (nw ? nw : 1));
-    u16 *wint = NULL;
     u32 *batch = (u32 *)malloc(sizeof(u32) * ntip);
-    R.cache = (u32 *)malloc(sizeof(u32) * (size_t)ntip * ncol);
-    R.localMax = (u16 *)malloc(sizeof(u16) * ntip);
-    R.shared = (u16 *)malloc(sizeof(u16) * ntip);
-    R.rawState = (u32 *)malloc(sizeof(u32) * (size_t)nnode * ncol);
-    R.nodeSize = (u32 *)malloc(sizeof(u32) * (size_t)ntip * 2);
+    R.localMax = (double *)malloc(sizeof(double) * ntip);
+    R.shared = (double *)malloc(sizeof(double) * ntip);
+    R.rawState = (u32 *)malloc(sizeof(u32) * (size_t)nnode * m->rowlen);
     int st = book_init(&R.b, ntip);
-    if (st || !w16 || !batch || !R.cache || !R.localMax || !R.shared || !R.rawState || !R.nodeSize) {
-        st = ORACLE_ENOMEM;
-        goto done;
-    }
-    for (size_t i = 0; i < nw; i++) w16[i] = oracle_f64_to_f16(w[i]);
-    memcpy(R.cache, codes, sizeof(u32) * (size_t)ntip * ncol);
-    memcpy(R.nodeSize, tipSize, sizeof(u32) * ntip);
-    wint = oracle_force_f16 ? NULL : exact_int_weights(w16, nState, ncol);
-    R.k.ncol = ncol; R.k.cache = R.cache; R.k.w16 = w16; R.k.wint = wint;
+    if (st || !batch || !R.localMax || !R.shared || !R.rawState) { st = ORACLE_ENOMEM; goto done; }
     JoinBook *b = &R.b;
     u64 nStale = 0, nJoin = 0, nPhase = 0, nPaired = 0;
 
     for (u32 i = 0; i + 1 < ntip; i++) {
 #pragma omp parallel for num_threads(R.nthreads) schedule(static)
-        for (long j = (long)i + 1; j < (long)ntip; j++) R.shared[j] = indel_score(&R.k, i, (u32)j);
+        for (long j = (long)i + 1; j < (long)ntip; j++) R.shared[j] = m->score(m->ctx, i, (u32)j);
         double bv = -1.0;
         u32 bi = 0;
-        for (u32 j = i + 1; j < ntip; j++) {
-            double v = oracle_f16_to_f64(R.shared[j]);
-            if (better(v, j, bv, bi)) { bv = v; bi = j; }
-        }
-        R.localMax[i] = oracle_f64_to_f16(bv);
+        for (u32 j = i + 1; j < ntip; j++)
+            if (better(R.shared[j], j, bv, bi)) { bv = R.shared[j]; bi = j; }
+        R.localMax[i] = bv;
         b->localMaxIdx[i] = bi;
         R.nPairs += ntip - i - 1;
     }
-    R.localMax[ntip - 1] = H_NEG_ONE;
+    R.localMax[ntip - 1] = -1.0;
     R.nodeCount = ntip;
 
     while (R.nodeCount < nnode) {
         double bv = -1.0, fv = -1.0;
         u32 bi = 0, fi = 0;
         for (u32 c = 0; c < ntip; c++) {
-            const double v = oracle_f16_to_f64(R.localMax[c]);
+            const double v = R.localMax[c];
             const u32 node = b->cache2node[c];
             if (better(v, node, bv, bi)) { bv = v; bi = node; }
-            if (node < nnode && rec_fresh(&R, c) && better(v, node, fv, fi)) { fv = v; fi = node; }
+            if (node < nnode && phased_fresh(&R, c) && better(v, node, fv, fi)) { fv = v; fi = node; }
         }
         const u32 j1 = bi;
         if (j1 >= nnode || b->node2cache[j1] >= ntip) { st = ORACLE_EINTERNAL; goto done; }
         const u32 c1 = b->node2cache[j1];
-        if (!rec_fresh(&R, c1)) {
+        if (!phased_fresh(&R, c1)) {
             /* one phase: the stale rows that beat the best fresh record, best first */
             u32 n = 0;
             for (u32 c = 0; c < ntip; c++) {
                 const u32 node = b->cache2node[c];
-                if (node >= nnode || rec_fresh(&R, c)) continue;
-                const double v = oracle_f16_to_f64(R.localMax[c]);
-                if (v >= 0 && better(v, node, fv, fi)) batch[n++] = c;
+                if (node >= nnode || phased_fresh(&R, c)) continue;
+                if (R.localMax[c] >= 0 && better(R.localMax[c], node, fv, fi)) batch[n++] = c;
             }
             for (u32 x = 1; x < n; x++) { /* insertion sort, decision order */
                 const u32 t = batch[x];
-                const double tv = oracle_f16_to_f64(R.localMax[t]);
                 u32 y = x;
-                while (y > 0 && better(tv, b->cache2node[t], oracle_f16_to_f64(R.localMax[batch[y - 1]]),
+                while (y > 0 && better(R.localMax[t], b->cache2node[t], R.localMax[batch[y - 1]],
                                        b->cache2node[batch[y - 1]])) {
                     batch[y] = batch[y - 1];
                     y--;
@@ -545,7 +529,7 @@ int oracle_join_indel_phased(uint32_t ntip, uint32_t ncol, const uint32_t *codes
             }
             if (n == 0 || batch[0] != c1) { st = ORACLE_EINTERNAL; goto done; }
             if (n > maxBatch) n = maxBatch;
-            for (u32 x = 0; x < n; x++) indel_rescan(&R, batch[x]);
+            for (u32 x = 0; x < n; x++) phased_rescan(&R, batch[x]);
             nStale += n;
             nPhase++;
             continue;
@@ -556,35 +540,88 @@ int oracle_join_indel_phased(uint32_t ntip, uint32_t ncol, const uint32_t *codes
         u32 cNode = 0;
         for (u32 c = 0; c < ntip; c++) {
             if (c == c1 || c == c2) continue;
-            const double v = oracle_f16_to_f64(R.localMax[c]);
-            if (better(v, b->cache2node[c], vcd, cNode)) { vcd = v; cNode = b->cache2node[c]; }
+            if (better(R.localMax[c], b->cache2node[c], vcd, cNode)) { vcd = R.localMax[c]; cNode = b->cache2node[c]; }
         }
         int ok = 0;
         u32 cc = ntip, dNode = nnode;
         if (pairJoins && vcd >= 0 && cNode < nnode && b->node2cache[cNode] < ntip) {
             cc = b->node2cache[cNode];
             dNode = b->localMaxIdx[cc];
-            ok = rec_fresh(&R, cc) && dNode != j1 && dNode != j2;
+            ok = phased_fresh(&R, cc) && dNode != j1 && dNode != j2;
         }
-        indel_join_step(&R, j1, j2, c1, c2, vcd, cNode, ok ? &ok : NULL);
+        phased_join(&R, j1, j2, c1, c2, vcd, cNode, ok ? &ok : NULL);
         nJoin++;
         nPhase++;
         if (ok && R.nodeCount < nnode) {
-            indel_join_step(&R, cNode, dNode, cc, b->node2cache[dNode], 0.0, 0, NULL);
+            phased_join(&R, cNode, dNode, cc, b->node2cache[dNode], 0.0, 0, NULL);
             nJoin++;
             nPaired++;
         }
     }
-    memcpy(R.rawState + (size_t)(nnode - 1) * ncol, R.cache + (size_t)b->node2cache[R.nodeCount - 1] * ncol,
-           sizeof(u32) * ncol);
-    st = dfs_output(b, R.rawState, ncol, edge_out, state_out);
+    m->row_out(m->ctx, b->node2cache[R.nodeCount - 1], R.rawState + (size_t)(nnode - 1) * m->rowlen);
+    st = dfs_output(b, R.rawState, m->rowlen, edge_out, state_out);
     if (stats) {
         stats[0] = nStale; stats[1] = R.nPairs; stats[2] = nJoin; stats[3] = nPhase; stats[4] = nPaired;
     }
 done:
     book_free(&R.b);
-    free(w16); free(wint); free(batch); free(R.cache); free(R.localMax); free(R.shared); free(R.rawState);
-    free(R.nodeSize);
+    free(batch); free(R.localMax); free(R.shared); free(R.rawState);
+    return st;
+}
+
+/* Indel model for the phased join (the same steps as oracle_join_indel). */
+typedef struct {
+    IndelCtx k;
+    u32 *cache, *nodeSize;
+    u32 ncol, minSize;
+    float minRatio;
+} IndelPhased;
+
+static double ip_score(void *p, u32 q, u32 c) {
+    return oracle_f16_to_f64(indel_score(&((IndelPhased *)p)->k, q, c));
+}
+
+static void ip_row(void *p, u32 c, u32 *dst) {
+    IndelPhased *x = (IndelPhased *)p;
+    memcpy(dst, x->cache + (size_t)c * x->ncol, sizeof(u32) * x->ncol);
+}
+
+static void ip_merge(void *p, u32 c1, u32 c2, u32 j1, u32 j2, u32 newNode) {
+    IndelPhased *x = (IndelPhased *)p;
+    const u32 s1 = x->nodeSize[j1], s2 = x->nodeSize[j2], ncol = x->ncol;
+    if (s1 < x->minSize && (float)s1 * x->minRatio < (float)s2)
+        memcpy(x->cache + (size_t)c1 * ncol, x->cache + (size_t)c2 * ncol, sizeof(u32) * ncol);
+    else if (!(s2 < x->minSize && (float)s2 * x->minRatio < (float)s1))
+        indel_merge(x->cache + (size_t)c1 * ncol, x->cache + (size_t)c2 * ncol, ncol);
+    x->nodeSize[newNode] = s1 + s2;
+}
+
+int oracle_join_indel_phased(uint32_t ntip, uint32_t ncol, const uint32_t *codes, uint32_t nState,
+                             const double *w, const uint32_t *tipSize, uint32_t minSize, float minRatio,
+                             uint32_t maxBatch, int pairJoins, uint32_t *edge_out, uint32_t *state_out,
+                             uint64_t *stats, int nthreads) {
+    if (ntip == 0 || ncol == 0 || maxBatch == 0) return ORACLE_EINVAL;
+    for (size_t i = 0; i < (size_t)ntip * ncol; i++)
+        if (codes[i] > 1 && codes[i] - 2 >= nState) return ORACLE_ERANGE;
+    const size_t nw = (size_t)nState * ncol;
+    IndelPhased x;
+    memset(&x, 0, sizeof(x));
+    u16 *w16 = (u16 *)malloc(sizeof(u16) * (nw ? nw : 1));
+    x.cache = (u32 *)malloc(sizeof(u32) * (size_t)ntip * ncol);
+    x.nodeSize = (u32 *)malloc(sizeof(u32) * (size_t)ntip * 2);
+    int st = ORACLE_ENOMEM;
+    if (w16 && x.cache && x.nodeSize) {
+        for (size_t i = 0; i < nw; i++) w16[i] = oracle_f64_to_f16(w[i]);
+        memcpy(x.cache, codes, sizeof(u32) * (size_t)ntip * ncol);
+        memcpy(x.nodeSize, tipSize, sizeof(u32) * ntip);
+        x.ncol = ncol; x.minSize = minSize; x.minRatio = minRatio;
+        x.k.ncol = ncol; x.k.cache = x.cache; x.k.w16 = w16;
+        x.k.wint = oracle_force_f16 ? NULL : exact_int_weights(w16, nState, ncol);
+        PhasedModel m = {&x, ip_score, ip_row, ip_merge, ncol};
+        st = phased_join_run(&m, ntip, maxBatch, pairJoins, edge_out, state_out, stats, nthreads);
+        free((void *)x.k.wint);
+    }
+    free(w16); free(x.cache); free(x.nodeSize);
     return st;
 }
 
@@ -730,6 +767,62 @@ int oracle_join_bit(uint32_t ntip, uint32_t nbin, const uint32_t *words,
 done:
     book_free(&b);
     free(wf); free(seq); free(bis); free(localMax); free(shared); free(rawState);
+    return st;
+}
+
+/* Bit model for the phased join (the same steps as oracle_join_bit). */
+typedef struct {
+    BitCtx k;
+    u32 *seq, *bis;
+    u32 nbin;
+    int ancestralType;
+} BitPhased;
+
+static double bp_score(void *p, u32 q, u32 c) { return (double)bit_score(&((BitPhased *)p)->k, q, c); }
+
+static void bp_row(void *p, u32 c, u32 *dst) {
+    BitPhased *x = (BitPhased *)p;
+    for (u32 j = 0; j < x->nbin; j++) dst[j] = x->seq[(size_t)c * x->nbin + j] & ~x->bis[(size_t)c * x->nbin + j];
+}
+
+static void bp_merge(void *p, u32 c1, u32 c2, u32 j1, u32 j2, u32 newNode) {
+    BitPhased *x = (BitPhased *)p;
+    const u32 nbin = x->nbin;
+    for (u32 j = 0; j < nbin; j++) {
+        u32 s1 = x->seq[(size_t)c1 * nbin + j], s2 = x->seq[(size_t)c2 * nbin + j];
+        u32 b1 = x->bis[(size_t)c1 * nbin + j], b2 = x->bis[(size_t)c2 * nbin + j];
+        if (x->ancestralType == 0) {
+            u32 diff = s1 ^ s2, conflict = diff & (b1 | b2);
+            x->seq[(size_t)c1 * nbin + j] = (s1 | s2) & ~conflict;
+            x->bis[(size_t)c1 * nbin + j] = (diff & ~(b1 ^ b2)) | (b1 & b2);
+        } else {
+            x->seq[(size_t)c1 * nbin + j] = (s1 & s2) | (b1 & s2) | (b2 & s1);
+            x->bis[(size_t)c1 * nbin + j] = (s1 ^ s2) & ~(b1 | b2);
+        }
+    }
+}
+
+int oracle_join_bit_phased(uint32_t ntip, uint32_t nbin, const uint32_t *words, const double *w,
+                           int ancestralType, uint32_t maxBatch, int pairJoins, uint32_t *edge_out,
+                           uint32_t *state_out, uint64_t *stats, int nthreads) {
+    if (ntip == 0 || nbin == 0 || maxBatch == 0) return ORACLE_EINVAL;
+    const u32 nsite = nbin * 32;
+    BitPhased x;
+    memset(&x, 0, sizeof(x));
+    float *wf = (float *)malloc(sizeof(float) * nsite);
+    x.seq = (u32 *)malloc(sizeof(u32) * (size_t)ntip * nbin);
+    x.bis = (u32 *)calloc((size_t)ntip * nbin, sizeof(u32));
+    int st = ORACLE_ENOMEM;
+    if (wf && x.seq && x.bis) {
+        for (u32 i = 0; i < nsite; i++) wf[i] = (float)w[i];
+        memcpy(x.seq, words, sizeof(u32) * (size_t)ntip * nbin);
+        x.nbin = nbin;
+        x.ancestralType = ancestralType ? 1 : 0;
+        x.k.nbin = nbin; x.k.seq = x.seq; x.k.wf = wf;
+        PhasedModel m = {&x, bp_score, bp_row, bp_merge, nbin};
+        st = phased_join_run(&m, ntip, maxBatch, pairJoins, edge_out, state_out, stats, nthreads);
+    }
+    free(wf); free(x.seq); free(x.bis);
     return st;
 }
 

@@ -58,6 +58,12 @@ int oracle_join_indel_phased(uint32_t ntip, uint32_t ncol, const uint32_t *codes
                              uint32_t maxBatch, int pairJoins, uint32_t *edge_out, uint32_t *state_out,
                              uint64_t *stats, int nthreads);
 
+/* The bit join on the same phased schedule; outputs and stats as
+ * oracle_join_bit plus [3] phases and [4] phases with two joins. */
+int oracle_join_bit_phased(uint32_t ntip, uint32_t nbin, const uint32_t *words, const double *w,
+                           int ancestralType, uint32_t maxBatch, int pairJoins, uint32_t *edge_out,
+                           uint32_t *state_out, uint64_t *stats, int nthreads);
+
 /* joinEdgeBitReverse.  words: ntip x nbin row-major bit rows.  w: nbin*32
  * doubles.  ancestralType 0 or 1 (any non-zero value selects rule 1). */
 int oracle_join_bit(uint32_t ntip, uint32_t nbin, const uint32_t *words,

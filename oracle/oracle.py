@@ -40,6 +40,7 @@ def lib():
         L.oracle_join_indel_phased.argtypes = [u32, u32, _u32p, u32, _f64p, _u32p, u32, f32, u32, i,
                                                _u32p, _u32p, _u64p, i]
         L.oracle_join_bit.argtypes = [u32, u32, _u32p, _f64p, i, _u32p, _u32p, _u64p, i]
+        L.oracle_join_bit_phased.argtypes = [u32, u32, _u32p, _f64p, i, u32, i, _u32p, _u32p, _u64p, i]
         for name in ("oracle_node_keep_indel", "oracle_node_keep_bit"):
             getattr(L, name).argtypes = [u32, u32, _u32p, u32, _u32p, u32, _u32p, u32,
                                          _u32p, C.POINTER(u32)]
@@ -257,3 +258,19 @@ def approx_compare(clade_rows, ntip, edge1, edge2, nnode2=None, cache_size=8192,
            e2.ctypes.data_as(P), nnode2, int(cache_size), float(threshold), r.ctypes.data_as(P),
            q.ctypes.data_as(P)), "approx_compare")
     return r, q
+
+
+def join_bit_phased(words, w=None, ancestral_type=1, max_batch=8, pair_joins=True, nthreads=0):
+    """The bit join in phases (oracle_join_bit_phased); stats adds [3] phases
+    and [4] phases with two joins."""
+    words = _u32(words)
+    ntip, nbin = words.shape
+    w = np.ones(nbin * 32) if w is None else w
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    nedge = 2 * ntip - 2
+    edge = np.zeros(max(nedge, 1) * 2, dtype=np.uint32)
+    state = np.zeros(max(ntip - 1, 1) * nbin, dtype=np.uint32)
+    stats = np.zeros(5, dtype=np.uint64)
+    _chk(lib().oracle_join_bit_phased(ntip, nbin, words, w, ancestral_type, max_batch, 1 if pair_joins else 0,
+                                      edge, state, stats, nthreads or os.cpu_count()), "join_bit_phased")
+    return edge[: 2 * nedge].reshape(nedge, 2), state.reshape(-1, nbin), stats

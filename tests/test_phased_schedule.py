@@ -1,6 +1,6 @@
-"""The indel join in phases (oracle_join_indel_phased): batched early stale
+"""The greedy joins in phases (oracle_join_indel_phased, oracle_join_bit_phased): batched early stale
 rescans and two provably independent joins per phase give the same tree and
-node states as the sequential join (oracle_join_indel), in fewer phases.  This
+node states as the sequential joins (oracle_join_indel, oracle_join_bit), in fewer phases.  This
 pins the schedule a parallel engine may use against the pinned oracle."""
 import numpy as np
 import pytest
@@ -49,3 +49,22 @@ def test_phased_join_rejects_a_zero_batch():
     codes, nstate, w, ts, ms, mr = _case(CASES[0])
     with pytest.raises(RuntimeError):
         O.join_indel_phased(codes, nstate, w, ts, ms, mr, 0, True)
+
+
+BIT_CASES = [(400, 1, 0, "unit"), (400, 1, 1, "float"), (1500, 2, 0, "float"), (1500, 2, 1, "unit")]
+
+
+@pytest.mark.parametrize("n,seed,atype,wk", BIT_CASES, ids=[f"{c[0]}cells-type{c[2]}-{c[3]}" for c in BIT_CASES])
+def test_phased_bit_join_gives_the_sequential_tree(n, seed, atype, wk):
+    """The same schedule on the bit model (joinEdgeBitReverse): the rules use
+    only records, rescans and strict-improvement updates, which it shares."""
+    words = synth.binary_workload(n, 256, 11, 0.03, 0.05, seed=seed)
+    w = np.ones(256) if wk == "unit" else np.random.default_rng(seed).uniform(0.2, 3.0, 256)
+    e0, s0, st0 = O.join_bit(words, w, atype)
+    seq_phases = int(st0[0] + st0[2])
+    for max_batch, pairs in [(1, False), (8, True)]:
+        e1, s1, st1 = O.join_bit_phased(words, w, atype, max_batch, pairs)
+        assert np.array_equal(e1, e0) and np.array_equal(s1, s0), (max_batch, pairs)
+        if (max_batch, pairs) == (1, False):
+            assert int(st1[3]) == seq_phases
+    assert int(st1[3]) <= 0.75 * seq_phases
