@@ -464,8 +464,46 @@ static int phased_fresh(const PhasedRun *R, u32 c) {
 }
 
 /* stats (nullable): [0] stale rescans, [1] pair-scores, [2] joins, [3]
- * phases, [4] phases with two joins. */
-static int phased_join_run(const PhasedModel *m, u32 ntip, u32 maxBatch, int pairJoins, u32 *edge_out,
+ * phases, [4] phases with two joins, [5] pairs given up because a table of
+ * each CTA's top two records could not vouch for them.
+ * tableCTAs > 0 models such a table: the live rows are split by rank into
+ * tableCTAs equal ranges (as if renumbered densely every phase), and a
+ * pair is given up when a and b are the two best records of one range
+ * that holds more live records, which hides that range's third best. */
+
+/* Position of cache row c among the valid rows (ascending). */
+static u32 valid_rank(const JoinBook *b, u32 c) {
+    u32 lo = 0, hi = b->nvalid;
+    while (lo < hi) {
+        const u32 mid = (lo + hi) / 2;
+        if (b->valid[mid] < c) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+/* Would a top-2-per-range table hide the best record outside rows c1, c2? */
+static int table_hides(const PhasedRun *R, u32 c1, u32 c2, u32 tableCTAs) {
+    const JoinBook *b = &R->b;
+    const u32 per = (b->nvalid + tableCTAs - 1) / tableCTAs;
+    const u32 t = valid_rank(b, c1) / per;
+    if (valid_rank(b, c2) / per != t) return 0;
+    const u32 p0 = t * per, p1 = p0 + per < b->nvalid ? p0 + per : b->nvalid;
+    double v0 = -1.0, v1 = -1.0;
+    u32 n0 = 0, n1 = 0, s0 = ~0u, s1 = ~0u, cnt = 0;
+    for (u32 p = p0; p < p1; p++) {
+        const u32 c = b->valid[p];
+        const double v = R->localMax[c];
+        if (v < 0) continue;
+        cnt++;
+        const u32 node = b->cache2node[c];
+        if (better(v, node, v0, n0)) { v1 = v0; n1 = n0; s1 = s0; v0 = v; n0 = node; s0 = c; }
+        else if (better(v, node, v1, n1)) { v1 = v; n1 = node; s1 = c; }
+    }
+    return cnt > 2 && ((s0 == c1 && s1 == c2) || (s0 == c2 && s1 == c1));
+}
+
+static int phased_join_run(const PhasedModel *m, u32 ntip, u32 maxBatch, int pairJoins, u32 tableCTAs, u32 *edge_out,
                            u32 *state_out, u64 *stats, int nthreads) {
     if (ntip == 0 || maxBatch == 0) return ORACLE_EINVAL;
     PhasedRun R;
@@ -481,7 +519,7 @@ static int phased_join_run(const PhasedModel *m, u32 ntip, u32 maxBatch, int pai
     int st = book_init(&R.b, ntip);
     if (st || !batch || !R.localMax || !R.shared || !R.rawState) { st = ORACLE_ENOMEM; goto done; }
     JoinBook *b = &R.b;
-    u64 nStale = 0, nJoin = 0, nPhase = 0, nPaired = 0;
+    u64 nStale = 0, nJoin = 0, nPhase = 0, nPaired = 0, nHidden = 0;
 
     for (u32 i = 0; i + 1 < ntip; i++) {
 #pragma omp parallel for num_threads(R.nthreads) schedule(static)
@@ -548,6 +586,10 @@ static int phased_join_run(const PhasedModel *m, u32 ntip, u32 maxBatch, int pai
             cc = b->node2cache[cNode];
             dNode = b->localMaxIdx[cc];
             ok = phased_fresh(&R, cc) && dNode != j1 && dNode != j2;
+            if (ok && tableCTAs && table_hides(&R, c1, c2, tableCTAs)) {
+                ok = 0;
+                nHidden++;
+            }
         }
         phased_join(&R, j1, j2, c1, c2, vcd, cNode, ok ? &ok : NULL);
         nJoin++;
@@ -562,6 +604,7 @@ static int phased_join_run(const PhasedModel *m, u32 ntip, u32 maxBatch, int pai
     st = dfs_output(b, R.rawState, m->rowlen, edge_out, state_out);
     if (stats) {
         stats[0] = nStale; stats[1] = R.nPairs; stats[2] = nJoin; stats[3] = nPhase; stats[4] = nPaired;
+        stats[5] = nHidden;
     }
 done:
     book_free(&R.b);
@@ -598,8 +641,8 @@ static void ip_merge(void *p, u32 c1, u32 c2, u32 j1, u32 j2, u32 newNode) {
 
 int oracle_join_indel_phased(uint32_t ntip, uint32_t ncol, const uint32_t *codes, uint32_t nState,
                              const double *w, const uint32_t *tipSize, uint32_t minSize, float minRatio,
-                             uint32_t maxBatch, int pairJoins, uint32_t *edge_out, uint32_t *state_out,
-                             uint64_t *stats, int nthreads) {
+                             uint32_t maxBatch, int pairJoins, uint32_t tableCTAs, uint32_t *edge_out,
+                             uint32_t *state_out, uint64_t *stats, int nthreads) {
     if (ntip == 0 || ncol == 0 || maxBatch == 0) return ORACLE_EINVAL;
     for (size_t i = 0; i < (size_t)ntip * ncol; i++)
         if (codes[i] > 1 && codes[i] - 2 >= nState) return ORACLE_ERANGE;
@@ -618,7 +661,7 @@ int oracle_join_indel_phased(uint32_t ntip, uint32_t ncol, const uint32_t *codes
         x.k.ncol = ncol; x.k.cache = x.cache; x.k.w16 = w16;
         x.k.wint = oracle_force_f16 ? NULL : exact_int_weights(w16, nState, ncol);
         PhasedModel m = {&x, ip_score, ip_row, ip_merge, ncol};
-        st = phased_join_run(&m, ntip, maxBatch, pairJoins, edge_out, state_out, stats, nthreads);
+        st = phased_join_run(&m, ntip, maxBatch, pairJoins, tableCTAs, edge_out, state_out, stats, nthreads);
         free((void *)x.k.wint);
     }
     free(w16); free(x.cache); free(x.nodeSize);
@@ -803,8 +846,8 @@ static void bp_merge(void *p, u32 c1, u32 c2, u32 j1, u32 j2, u32 newNode) {
 }
 
 int oracle_join_bit_phased(uint32_t ntip, uint32_t nbin, const uint32_t *words, const double *w,
-                           int ancestralType, uint32_t maxBatch, int pairJoins, uint32_t *edge_out,
-                           uint32_t *state_out, uint64_t *stats, int nthreads) {
+                           int ancestralType, uint32_t maxBatch, int pairJoins, uint32_t tableCTAs,
+                           uint32_t *edge_out, uint32_t *state_out, uint64_t *stats, int nthreads) {
     if (ntip == 0 || nbin == 0 || maxBatch == 0) return ORACLE_EINVAL;
     const u32 nsite = nbin * 32;
     BitPhased x;
@@ -820,7 +863,7 @@ int oracle_join_bit_phased(uint32_t ntip, uint32_t nbin, const uint32_t *words, 
         x.ancestralType = ancestralType ? 1 : 0;
         x.k.nbin = nbin; x.k.seq = x.seq; x.k.wf = wf;
         PhasedModel m = {&x, bp_score, bp_row, bp_merge, nbin};
-        st = phased_join_run(&m, ntip, maxBatch, pairJoins, edge_out, state_out, stats, nthreads);
+        st = phased_join_run(&m, ntip, maxBatch, pairJoins, tableCTAs, edge_out, state_out, stats, nthreads);
     }
     free(wf); free(x.seq); free(x.bis);
     return st;

@@ -52,17 +52,19 @@ int oracle_join_indel(uint32_t ntip, uint32_t ncol, const uint32_t *codes,
  * maxBatch stale rescans per phase, and with pairJoins a second join in a
  * phase when it is provably the sequential loop's next decision.  Same
  * outputs as oracle_join_indel; stats (nullable): [0] stale rescans, [1]
- * pair-scores, [2] joins, [3] phases, [4] phases with two joins. */
+ * pair-scores, [2] joins, [3] phases, [4] phases with two joins, [5] pairs
+ * given up because a table of each of tableCTAs ranges' top two records
+ * could not vouch for them (tableCTAs 0: every record is visible). */
 int oracle_join_indel_phased(uint32_t ntip, uint32_t ncol, const uint32_t *codes, uint32_t nState,
                              const double *w, const uint32_t *tipSize, uint32_t minSize, float minRatio,
-                             uint32_t maxBatch, int pairJoins, uint32_t *edge_out, uint32_t *state_out,
-                             uint64_t *stats, int nthreads);
+                             uint32_t maxBatch, int pairJoins, uint32_t tableCTAs, uint32_t *edge_out,
+                             uint32_t *state_out, uint64_t *stats, int nthreads);
 
 /* The bit join on the same phased schedule; outputs and stats as
  * oracle_join_bit plus [3] phases and [4] phases with two joins. */
 int oracle_join_bit_phased(uint32_t ntip, uint32_t nbin, const uint32_t *words, const double *w,
-                           int ancestralType, uint32_t maxBatch, int pairJoins, uint32_t *edge_out,
-                           uint32_t *state_out, uint64_t *stats, int nthreads);
+                           int ancestralType, uint32_t maxBatch, int pairJoins, uint32_t tableCTAs,
+                           uint32_t *edge_out, uint32_t *state_out, uint64_t *stats, int nthreads);
 
 /* joinEdgeBitReverse.  words: ntip x nbin row-major bit rows.  w: nbin*32
  * doubles.  ancestralType 0 or 1 (any non-zero value selects rule 1). */

@@ -37,10 +37,10 @@ def lib():
         L.oracle_f16_add.restype = C.c_uint16
         L.oracle_join_indel.argtypes = [u32, u32, _u32p, u32, _f64p, _u32p, u32, f32,
                                         _u32p, _u32p, _u64p, i]
-        L.oracle_join_indel_phased.argtypes = [u32, u32, _u32p, u32, _f64p, _u32p, u32, f32, u32, i,
+        L.oracle_join_indel_phased.argtypes = [u32, u32, _u32p, u32, _f64p, _u32p, u32, f32, u32, i, u32,
                                                _u32p, _u32p, _u64p, i]
         L.oracle_join_bit.argtypes = [u32, u32, _u32p, _f64p, i, _u32p, _u32p, _u64p, i]
-        L.oracle_join_bit_phased.argtypes = [u32, u32, _u32p, _f64p, i, u32, i, _u32p, _u32p, _u64p, i]
+        L.oracle_join_bit_phased.argtypes = [u32, u32, _u32p, _f64p, i, u32, i, u32, _u32p, _u32p, _u64p, i]
         for name in ("oracle_node_keep_indel", "oracle_node_keep_bit"):
             getattr(L, name).argtypes = [u32, u32, _u32p, u32, _u32p, u32, _u32p, u32,
                                          _u32p, C.POINTER(u32)]
@@ -80,9 +80,10 @@ def join_indel(codes, nstate, w, tip_size=None, min_size=0, min_ratio=2.0, nthre
 
 
 def join_indel_phased(codes, nstate, w, tip_size=None, min_size=0, min_ratio=2.0, max_batch=8, pair_joins=True,
-                      nthreads=0):
+                      table_ctas=0, nthreads=0):
     """The indel join in phases (oracle_join_indel_phased); stats adds
-    [3] phases and [4] phases with two joins."""
+    [3] phases, [4] phases with two joins and [5] pairs a top-2 table over
+    `table_ctas` ranges could not vouch for."""
     codes = _u32(codes)
     ntip, ncol = codes.shape
     w = np.ascontiguousarray(w, dtype=np.float64).reshape(-1)
@@ -90,9 +91,10 @@ def join_indel_phased(codes, nstate, w, tip_size=None, min_size=0, min_ratio=2.0
     nedge = 2 * ntip - 2
     edge = np.zeros(max(nedge, 1) * 2, dtype=np.uint32)
     state = np.zeros(max(ntip - 1, 1) * ncol, dtype=np.uint32)
-    stats = np.zeros(5, dtype=np.uint64)
+    stats = np.zeros(6, dtype=np.uint64)
     _chk(lib().oracle_join_indel_phased(ntip, ncol, codes, nstate, w, ts, min_size, min_ratio, max_batch,
-                                        1 if pair_joins else 0, edge, state, stats, nthreads or os.cpu_count()),
+                                        1 if pair_joins else 0, table_ctas, edge, state, stats,
+                                        nthreads or os.cpu_count()),
          "join_indel_phased")
     return edge[: 2 * nedge].reshape(nedge, 2), state.reshape(-1, ncol), stats
 
@@ -260,9 +262,10 @@ def approx_compare(clade_rows, ntip, edge1, edge2, nnode2=None, cache_size=8192,
     return r, q
 
 
-def join_bit_phased(words, w=None, ancestral_type=1, max_batch=8, pair_joins=True, nthreads=0):
-    """The bit join in phases (oracle_join_bit_phased); stats adds [3] phases
-    and [4] phases with two joins."""
+def join_bit_phased(words, w=None, ancestral_type=1, max_batch=8, pair_joins=True, table_ctas=0, nthreads=0):
+    """The bit join in phases (oracle_join_bit_phased); stats adds [3] phases,
+    [4] phases with two joins and [5] pairs a top-2 table over `table_ctas`
+    ranges could not vouch for."""
     words = _u32(words)
     ntip, nbin = words.shape
     w = np.ones(nbin * 32) if w is None else w
@@ -270,7 +273,7 @@ def join_bit_phased(words, w=None, ancestral_type=1, max_batch=8, pair_joins=Tru
     nedge = 2 * ntip - 2
     edge = np.zeros(max(nedge, 1) * 2, dtype=np.uint32)
     state = np.zeros(max(ntip - 1, 1) * nbin, dtype=np.uint32)
-    stats = np.zeros(5, dtype=np.uint64)
+    stats = np.zeros(6, dtype=np.uint64)
     _chk(lib().oracle_join_bit_phased(ntip, nbin, words, w, ancestral_type, max_batch, 1 if pair_joins else 0,
-                                      edge, state, stats, nthreads or os.cpu_count()), "join_bit_phased")
+                                      table_ctas, edge, state, stats, nthreads or os.cpu_count()), "join_bit_phased")
     return edge[: 2 * nedge].reshape(nedge, 2), state.reshape(-1, nbin), stats

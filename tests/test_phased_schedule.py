@@ -68,3 +68,16 @@ def test_phased_bit_join_gives_the_sequential_tree(n, seed, atype, wk):
         if (max_batch, pairs) == (1, False):
             assert int(st1[3]) == seq_phases
     assert int(st1[3]) <= 0.75 * seq_phases
+
+
+def test_phased_join_under_a_top2_table():
+    """Deciding pairs from a table of each CTA range's top two records (16
+    ranges here) gives up a pair only when a range's third best is hidden;
+    the tree is still the sequential one."""
+    codes, nstate, w, ts, ms, mr = _case(CASES[3])
+    e0, s0, _ = O.join_indel(codes, nstate, w, ts, ms, mr)
+    e1, s1, st1 = O.join_indel_phased(codes, nstate, w, ts, ms, mr, 8, True, 16)
+    assert np.array_equal(e1, e0) and np.array_equal(s1, s0)
+    _, _, full = O.join_indel_phased(codes, nstate, w, ts, ms, mr, 8, True, 0)
+    assert int(full[5]) == 0  # with every record visible nothing is given up
+    assert int(st1[4]) > 0 and int(st1[5]) < int(st1[4])
