@@ -237,6 +237,246 @@ static void indel_merge(u32 *a, const u32 *b, u32 n) {
     }
 }
 
+/* ------------------------------------------------------------------ */
+/* Column-scan engine for the indel join (integer weights only).        */
+/* The same loop as oracle_join_indel below, with the pair scores of one */
+/* query against many rows taken from a site-major u16 copy of the cache */
+/* rows: for each site the query has edited, one contiguous pass over    */
+/* that site's codes adds the weight where they are equal.  Exact        */
+/* integer sums (the condition exact_int_weights checks) make the values */
+/* and comparisons those of the binary16 loop; values are held as int,   */
+/* -1 standing for the reference's -1 (H_NEG_ONE).  This is an execution */
+/* strategy of the oracle for large trees; oracle_join_indel's row-wise  */
+/* scoring is the default, and the CPU tests check that both engines     */
+/* write the same tree.                                                  */
+/* ------------------------------------------------------------------ */
+
+/* Non-zero: oracle_join_indel uses the column-scan engine whenever the
+ * weights are exact integers (oracle_force_f16 off). */
+int oracle_indel_colscan = 0;
+
+#define CS_CHUNK 1024u  /* candidates per accumulator block */
+#define CS_QB 64u       /* queries per block in the initial pass */
+
+typedef struct { u32 site; u16 code, w; } CsSite;
+
+typedef struct {
+    u32 ntip, ncol, cap;  /* cap: columns of colT (live and dead rows) */
+    u16 *colT;            /* ncol x cap site-major codes */
+    u32 *pos2cache;       /* column -> cache row, ntip when dead */
+    u32 *cache2pos;       /* cache row -> column */
+    const u16 *wint;
+} ColScan;
+
+/* Edited sites of cache row q with a non-zero weight. */
+static u32 cs_query_sites(const u32 *row, u32 ncol, const u16 *wint, CsSite *out) {
+    u32 n = 0;
+    for (u32 i = 0; i < ncol; i++) {
+        const u32 t = row[i];
+        if (t > 1) {
+            const u16 w = wint[(size_t)(t - 2) * ncol + i];
+            if (w) { out[n].site = i; out[n].code = (u16)t; out[n].w = w; n++; }
+        }
+    }
+    return n;
+}
+
+/* score[p] for every column p of colT against the query's sites. */
+static void cs_scan(const ColScan *S, const CsSite *qs, u32 nqs, u16 *score, int nthreads) {
+    const u32 cap = S->cap, nchunk = (cap + CS_CHUNK - 1) / CS_CHUNK;
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+    for (long k = 0; k < (long)nchunk; k++) {
+        const u32 c0 = (u32)k * CS_CHUNK, n = cap - c0 < CS_CHUNK ? cap - c0 : CS_CHUNK;
+        u16 acc[CS_CHUNK];
+        memset(acc, 0, sizeof(acc));
+        for (u32 s = 0; s < nqs; s++) {
+            const u16 *col = S->colT + (size_t)qs[s].site * cap + c0;
+            const u16 t = qs[s].code, w = qs[s].w;
+            for (u32 c = 0; c < n; c++) acc[c] += (u16)(col[c] == t ? w : 0);
+        }
+        memcpy(score + c0, acc, sizeof(u16) * n);
+    }
+}
+
+/* Site-major copy of the live cache rows, columns in ascending cache order. */
+static int cs_compact(ColScan *S, const u32 *cache, const JoinBook *b) {
+    const u32 cap = b->nvalid;
+    u16 *colT = (u16 *)malloc(sizeof(u16) * (size_t)S->ncol * (cap ? cap : 1));
+    if (!colT) return ORACLE_ENOMEM;
+    for (u32 p = 0; p < cap; p++) {
+        const u32 c = b->valid[p];
+        const u32 *row = cache + (size_t)c * S->ncol;
+        for (u32 i = 0; i < S->ncol; i++) colT[(size_t)i * cap + p] = (u16)row[i];
+        S->pos2cache[p] = c;
+        S->cache2pos[c] = p;
+    }
+    free(S->colT);
+    S->colT = colT;
+    S->cap = cap;
+    return ORACLE_OK;
+}
+
+static void cs_store_row(ColScan *S, u32 c, const u32 *row) {
+    const u32 p = S->cache2pos[c];
+    for (u32 i = 0; i < S->ncol; i++) S->colT[(size_t)i * S->cap + p] = (u16)row[i];
+}
+
+/* Initial upper-triangle local maxima (cu/joinEdgeIndel.cu:355-369) in
+ * blocks of CS_QB queries, each site's codes read once per block. */
+static void cs_initial(const ColScan *S, const u32 *cache, int *localMax, u32 *localMaxIdx, int nthreads) {
+    const u32 ntip = S->ntip, ncol = S->ncol, nblk = (ntip + CS_QB - 1) / CS_QB;
+#pragma omp parallel num_threads(nthreads)
+    {
+        u16 *acc = (u16 *)malloc(sizeof(u16) * CS_QB * CS_CHUNK);
+        u16 *qcode = (u16 *)malloc(sizeof(u16) * CS_QB * ncol);
+        u16 *qw = (u16 *)malloc(sizeof(u16) * CS_QB * ncol);
+        u32 *act = (u32 *)malloc(sizeof(u32) * CS_QB * ncol);  /* active queries, site by site */
+        u32 *actOff = (u32 *)malloc(sizeof(u32) * (ncol + 1));
+#pragma omp for schedule(dynamic, 1)
+        for (long blk = 0; blk < (long)nblk; blk++) {
+            const u32 i0 = (u32)blk * CS_QB, nq = ntip - i0 < CS_QB ? ntip - i0 : CS_QB;
+            int bv[CS_QB];
+            u32 bi[CS_QB];
+            for (u32 q = 0; q < nq; q++) {
+                bv[q] = -1; bi[q] = 0;
+                const u32 *row = cache + (size_t)(i0 + q) * ncol;
+                for (u32 i = 0; i < ncol; i++) {
+                    const u32 t = row[i];
+                    const u16 w = t > 1 ? S->wint[(size_t)(t - 2) * ncol + i] : 0;
+                    qcode[(size_t)i * CS_QB + q] = (u16)t;
+                    qw[(size_t)i * CS_QB + q] = w;
+                }
+            }
+            u32 na = 0;
+            for (u32 i = 0; i < ncol; i++) {
+                actOff[i] = na;
+                for (u32 q = 0; q < nq; q++)
+                    if (qw[(size_t)i * CS_QB + q]) act[na++] = q;
+            }
+            actOff[ncol] = na;
+            for (u32 c0 = i0 + 1; c0 < ntip; c0 += CS_CHUNK) {
+                const u32 n = ntip - c0 < CS_CHUNK ? ntip - c0 : CS_CHUNK;
+                memset(acc, 0, sizeof(u16) * CS_QB * CS_CHUNK);
+                for (u32 i = 0; i < ncol; i++) {
+                    const u16 *col = S->colT + (size_t)i * S->cap + c0;
+                    for (u32 a = actOff[i]; a < actOff[i + 1]; a++) {
+                        const u32 q = act[a];
+                        const u16 t = qcode[(size_t)i * CS_QB + q], w = qw[(size_t)i * CS_QB + q];
+                        u16 *ac = acc + (size_t)q * CS_CHUNK;
+                        for (u32 c = 0; c < n; c++) ac[c] += (u16)(col[c] == t ? w : 0);
+                    }
+                }
+                /* ascending candidates, strict '>' keeps the smallest index */
+                for (u32 q = 0; q < nq; q++) {
+                    const u32 i = i0 + q;
+                    const u16 *ac = acc + (size_t)q * CS_CHUNK;
+                    for (u32 c = 0; c < n; c++) {
+                        const u32 j = c0 + c;
+                        if (j > i && (int)ac[c] > bv[q]) { bv[q] = ac[c]; bi[q] = j; }
+                    }
+                }
+            }
+            for (u32 q = 0; q < nq; q++) { localMax[i0 + q] = bv[q]; localMaxIdx[i0 + q] = bi[q]; }
+        }
+        free(acc); free(qcode); free(qw); free(act); free(actOff);
+    }
+    localMax[ntip - 1] = -1;
+}
+
+static int join_indel_colscan(u32 ntip, u32 ncol, u32 *cache, const u16 *wint, u32 *nodeSize, u32 minSize,
+                              float minRatio, JoinBook *b, u32 *rawState, u64 *counts, int nthreads) {
+    ColScan S;
+    memset(&S, 0, sizeof(S));
+    S.ntip = ntip; S.ncol = ncol; S.wint = wint;
+    S.pos2cache = (u32 *)malloc(sizeof(u32) * ntip);
+    S.cache2pos = (u32 *)malloc(sizeof(u32) * ntip);
+    int *localMax = (int *)malloc(sizeof(int) * ntip);
+    u16 *score = (u16 *)malloc(sizeof(u16) * ntip);
+    CsSite *qs = (CsSite *)malloc(sizeof(CsSite) * ncol);
+    int st = ORACLE_OK;
+    u64 nStale = 0, nPairs = 0, nJoin = 0;
+    if (!S.pos2cache || !S.cache2pos || !localMax || !score || !qs) { st = ORACLE_ENOMEM; goto out; }
+    if ((st = cs_compact(&S, cache, b))) goto out;
+    cs_initial(&S, cache, localMax, b->localMaxIdx, nthreads);
+    nPairs = (u64)ntip * (ntip - 1) / 2;
+
+    for (u32 nodeCount = ntip; nodeCount < b->nnode; nodeCount++) {
+        u32 j1, j2, c1, c2;
+        for (;;) {
+            /* decision: best (value, smallest node) over the live rows (a
+             * dead row holds (-1, nnode) and never wins) */
+            int bv = -1;
+            u32 bi = 0;
+            for (u32 p = 0; p < b->nvalid; p++) {
+                const u32 c = b->valid[p];
+                const int v = localMax[c];
+                const u32 node = b->cache2node[c];
+                if (v > bv || (v == bv && node < bi)) { bv = v; bi = node; }
+            }
+            j1 = bi;
+            if (j1 >= b->nnode) { st = ORACLE_EINTERNAL; goto out; }
+            c1 = b->node2cache[j1];
+            if (c1 >= ntip) { st = ORACLE_EINTERNAL; goto out; }
+            j2 = b->localMaxIdx[c1];
+            c2 = j2 < b->nnode ? b->node2cache[j2] : ntip;
+            if (c2 < ntip) break;
+            /* stale partner: rescore c1 against every valid row (:387-399) */
+            nStale++;
+            const u32 nqs = cs_query_sites(cache + (size_t)c1 * ncol, ncol, wint, qs);
+            cs_scan(&S, qs, nqs, score, nthreads);
+            nPairs += b->nvalid - 1;
+            bv = -1; bi = 0;
+            for (u32 p = 0; p < b->nvalid; p++) {
+                const u32 c = b->valid[p];
+                const int v = c == c1 ? -1 : (int)score[S.cache2pos[c]];
+                const u32 node = b->cache2node[c];
+                if (v > bv || (v == bv && node < bi)) { bv = v; bi = node; }
+            }
+            localMax[c1] = bv;
+            b->localMaxIdx[c1] = bi;
+        }
+        const u32 r = nodeCount - ntip;
+        u32 *row1 = cache + (size_t)c1 * ncol, *row2 = cache + (size_t)c2 * ncol;
+        memcpy(rawState + (size_t)(2 * r) * ncol, row1, sizeof(u32) * ncol);
+        memcpy(rawState + (size_t)(2 * r + 1) * ncol, row2, sizeof(u32) * ncol);
+        const u32 s1 = nodeSize[j1], s2 = nodeSize[j2];
+        if (s1 < minSize && (float)s1 * minRatio < (float)s2) memcpy(row1, row2, sizeof(u32) * ncol);
+        else if (s2 < minSize && (float)s2 * minRatio < (float)s1) ;
+        else indel_merge(row1, row2, ncol);
+        nodeSize[nodeCount] = s1 + s2;
+        b->rawEdge[4 * r] = nodeCount; b->rawEdge[4 * r + 1] = j1;
+        b->rawEdge[4 * r + 2] = nodeCount; b->rawEdge[4 * r + 3] = j2;
+        b->node2cache[j1] = ntip; b->node2cache[j2] = ntip; b->node2cache[nodeCount] = c1;
+        b->cache2node[c1] = nodeCount; b->cache2node[c2] = b->nnode;
+        book_remove_valid(b, c2);
+        S.pos2cache[S.cache2pos[c2]] = ntip;
+        if (b->nvalid * 2 < S.cap && S.cap > 4 * CS_CHUNK) {
+            if ((st = cs_compact(&S, cache, b))) goto out;
+        } else {
+            cs_store_row(&S, c1, row1);
+        }
+        /* new node against every valid row, strict improvement (:439-463) */
+        const u32 nqs = cs_query_sites(row1, ncol, wint, qs);
+        cs_scan(&S, qs, nqs, score, nthreads);
+        nPairs += b->nvalid - 1;
+        for (u32 p = 0; p < b->nvalid; p++) {
+            const u32 c = b->valid[p];
+            if (c == c1) continue;
+            const int v = score[S.cache2pos[c]];
+            if (v > localMax[c]) { localMax[c] = v; b->localMaxIdx[c] = nodeCount; }
+        }
+        localMax[c1] = -1;
+        localMax[c2] = -1;
+        nJoin++;
+    }
+    memcpy(rawState + (size_t)(b->nnode - 1) * ncol, cache + (size_t)b->node2cache[b->nnode - 1] * ncol,
+           sizeof(u32) * ncol);
+out:
+    counts[0] = nStale; counts[1] = nPairs; counts[2] = nJoin;
+    free(S.colT); free(S.pos2cache); free(S.cache2pos); free(localMax); free(score); free(qs);
+    return st;
+}
+
 int oracle_join_indel(uint32_t ntip, uint32_t ncol, const uint32_t *codes,
                       uint32_t nState, const double *w, const uint32_t *tipSize,
                       uint32_t minSize, float minRatio, uint32_t *edge_out,
@@ -263,6 +503,13 @@ int oracle_join_indel(uint32_t ntip, uint32_t ncol, const uint32_t *codes,
     wint = oracle_force_f16 ? NULL : exact_int_weights(w16, nState, ncol);
     IndelCtx k = {ncol, cache, w16, wint};
     u64 nStale = 0, nPairs = 0, nJoin = 0;
+    if (wint && oracle_indel_colscan && nState + 1 <= 0xFFFFu) {
+        u64 cnt[3];
+        st = join_indel_colscan(ntip, ncol, cache, wint, nodeSize, minSize, minRatio, &b, rawState, cnt, nthreads);
+        if (!st) st = dfs_output(&b, rawState, ncol, edge_out, state_out);
+        if (!st && stats) { stats[0] = cnt[0]; stats[1] = cnt[1]; stats[2] = cnt[2]; }
+        goto done;
+    }
 
     /* initial upper-triangle local maxima (cu/joinEdgeIndel.cu:355-369) */
     for (u32 i = 0; i + 1 < ntip; i++) {

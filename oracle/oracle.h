@@ -32,6 +32,9 @@ extern "C" {
 /* Non-zero forces joinEdgeIndel's binary16 emulation even when an exact
  * integer sum would give the same values. */
 extern int oracle_force_f16;
+/* Non-zero selects the indel join's column-scan engine (integer weights
+ * only; same outputs, for trees of 10^5 cells). */
+extern int oracle_indel_colscan;
 
 /* binary16 helpers (exposed for unit tests) */
 uint16_t oracle_f64_to_f16(double x);
