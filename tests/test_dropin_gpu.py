@@ -13,14 +13,18 @@ pytestmark = pytest.mark.gpu
 BIN = os.path.join(os.path.dirname(__file__), "..", "casphy_b200", "bin")
 
 
-def test_dropin_outputs_match_reference_files(golden, gpu_lib):
+@pytest.fixture(scope="module")
+def tool_outputs(gpu_lib):
+    """Every golden case run through the drop-in executables."""
+    return make_golden.run_tools(BIN)
+
+
+def test_dropin_outputs_match_reference_files(golden, tool_outputs):
     cases, ref = golden
-    got = make_golden.run_tools(BIN)
+    got = tool_outputs
     checked, bad = 0, []
     for key, want in sorted(ref.items()):
         if key not in got:
-            if key.startswith("fs/"):
-                continue  # bootstrap resampler checked in its own test
             bad.append(f"missing {key}")
             continue
         have = got[key]
@@ -43,3 +47,16 @@ def test_dropin_outputs_match_reference_files(golden, gpu_lib):
             bad.append(f"differs: {key}")
     assert checked > 50
     assert not bad, "\n".join(bad)
+
+
+def test_felsenstein_resampler_matches_reference_files(golden, tool_outputs):
+    """`Felsenstein <prefix> 7` (cu/Felsenstein.cu:56-66): the mt19937 column
+    draw (.idx) and the gathered matrix (.bin) equal the reference tool's
+    files byte for byte on both alignments."""
+    _, ref = golden
+    got = tool_outputs
+    keys = sorted(k for k in ref if k.startswith("fs/"))
+    assert len(keys) == 4
+    for key in keys:
+        assert key in got, f"drop-in wrote no {key}"
+        assert got[key].shape == ref[key].shape and np.array_equal(got[key], ref[key]), key
