@@ -98,3 +98,19 @@ def test_large_compaction_properties(gpu_lib, scan_path):
     assert st1["compactions"] > 0
     e0, s0, st0 = O.join_indel(codes, ns, w)
     assert np.array_equal(e1, e0) and np.array_equal(s1, s0)
+
+
+@pytest.mark.parametrize("name", ["w3k_unit", "w2k_int", "w1500_half"])
+def test_reference_digests_at_1024_sites(gpu_lib, scan_path, name):
+    """The GPU join (and nodeKeepIndel on the unit case) against the files
+    the reference tools built with MAXCOL 1024 wrote for the same inputs."""
+    import json
+    import make_wide_golden as W
+    ref = json.load(open(W.OUT))[name]
+    codes, ns, w, out = W.case_inputs(name)
+    e, s, _ = gpu_lib.join_indel(codes, ns, w)
+    assert W.sha_bytes(W.edge2_file_bytes(e)) == ref["edge2"]
+    assert W.sha_bytes(W.node_state2_file_bytes(s, *codes.shape)) == ref["nodeState2"]
+    for cut in (1, 2):
+        if f"retain{cut}" in ref:
+            assert W.retain_digest(gpu_lib.node_keep(s, e, out, cut)) == ref[f"retain{cut}"]

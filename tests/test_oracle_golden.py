@@ -41,3 +41,18 @@ def test_binary16_helpers_match_numpy(seed):
     for a, b in zip(h[::2], h[1::2]):
         want = (np.float64(np.uint16(a).view(np.float16)) + np.float64(np.uint16(b).view(np.float16)))
         assert L.oracle_f16_add(int(a), int(b)) == int(np.float16(want).view(np.uint16))
+
+
+def test_oracle_matches_reference_at_1024_sites():
+    """The oracle against the reference joinEdgeIndel / nodeKeepIndel built
+    with MAXCOL 1024, on three 1,024-site cases of the 200k generator's
+    settings (unit, integer and fractional weights; digests in
+    tests/golden/wide_reference.json)."""
+    import json
+    import os
+    import make_wide_golden as W
+    ref = json.load(open(W.OUT))
+    for name in W.CASES:
+        got = W.oracle_digests(name)
+        for k, v in ref[name].items():
+            assert got[k] == v, f"{name}/{k}"
