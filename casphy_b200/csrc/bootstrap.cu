@@ -592,7 +592,7 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
         b.initKey = c.take<unsigned long long>(n);
         b.pub = c.take<joinx::BlockRec>(4 * G);
         b.pubCnt = c.take<u32>(2 * G);
-        b.partial = c.take<u64>(2 * G);
+        b.partial = c.take<u64>((size_t)2 * G * joinx::kMaxBatch);
         b.counts = c.take<u32>(G);
         b.flags = c.take<u32>(16 * G);
         b.chunkStart = c.take<u64>(nChunks + 1);
@@ -673,6 +673,7 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
         c.err = G.errs + r; c.limitNs = 20ull * 1000 * 1000 * 1000; c.statsOut = b.stats;
         c.Rmax = ((n + Gs[r] - 1) / Gs[r] + 7u) & ~7u; c.ordNeg1 = ORD_F32_NEG1; c.compactMin = 4096; c.compactQ8 = 192; c.bytesPerPairSite = 4000;
         c.prof = nullptr;
+        c.maxBatch = joinx::stale_batch_setting();
         R.m = BitModel<PATH_PLANES>::Args{nbin, nbinP, nplanes, ancestralType ? 1 : 0, b.planeMask, nullptr,
                                           b.nodeSeq, b.nodeBis, {b.colT0, b.colT1}};
         R.init = InitArgs{n, nbin, Sp, eStride, b.colT0, b.eW, b.eQ, b.eLen, nullptr, b.chunkStart, nChunks,

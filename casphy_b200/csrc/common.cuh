@@ -48,6 +48,15 @@ __device__ __forceinline__ uint4 ld_cg_v4(const void* p) {
                  : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p));
     return v;
 }
+// Asynchronous 16-byte global -> shared copy through L2 only (cp.async.cg);
+// both addresses 16-byte aligned.  cp_async_wait_all() waits for this
+// thread's copies; a block barrier after it publishes them to the block.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const u32 sa = static_cast<u32>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 __device__ __forceinline__ u16 ld_cg_u16(const u16* p) {
     u16 v;
     asm volatile("ld.global.cg.u16 %0, [%1];" : "=h"(v) : "l"(p));

@@ -67,7 +67,13 @@ using namespace bitjoin;
 template <int PATH>
 static int launch_bit_join(joinx::Common& c, typename BitModel<PATH>::Args m, u32 nCTA, cudaStream_t st) {
     using M = BitModel<PATH>;
-    const size_t smem = M::engine_smem_bytes(nCTA, c.Rmax) + M::model_smem_bytes(m);
+    // the joined-node bitmap only where shared memory allows it
+    int smemMax = 0, dev = 0;
+    CASPHY_CUDA_TRY(cudaGetDevice(&dev));
+    CASPHY_CUDA_TRY(cudaDeviceGetAttribute(&smemMax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    if (M::engine_smem_bytes(nCTA, c.Rmax, c.deathWords) + M::model_smem_bytes(m) > (size_t)smemMax - 4096)
+        c.deathWords = 0;
+    const size_t smem = M::engine_smem_bytes(nCTA, c.Rmax, c.deathWords) + M::model_smem_bytes(m);
     void* fn = (void*)joinx::k_join<M>;
     CASPHY_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int perSM = 0;
@@ -165,7 +171,7 @@ static int join_bit_impl(u32 ntip, u32 nbin, const u32* d_words, const u32* h_wo
         b.initKey = c.take<unsigned long long>(ntip);
         b.pub = c.take<joinx::BlockRec>(4 * nCTA);
         b.pubCnt = c.take<u32>(2 * nCTA);
-        b.partial = c.take<u64>(2 * nCTA);
+        b.partial = c.take<u64>((size_t)2 * nCTA * joinx::kMaxBatch);
         b.counts = c.take<u32>(nCTA);
         b.flags = c.take<u32>(16 * nCTA);
         b.jerr = c.take<int>(1);
@@ -241,6 +247,8 @@ static int join_bit_impl(u32 ntip, u32 nbin, const u32* d_words, const u32* h_wo
         c.err = L.jerr; c.limitNs = 20ull * 1000 * 1000 * 1000; c.statsOut = L.stats;
         c.Rmax = (((ntip + nCTA - 1) / nCTA) + 7u) & ~7u;
         c.ordNeg1 = ORD_F32_NEG1; c.compactMin = 4096; c.compactQ8 = 192; c.bytesPerPairSite = 4000;
+        c.maxBatch = joinx::stale_batch_setting();
+        c.deathWords = (nnode + 31) / 32;
         if (path == PATH_UNIT) {
             BitModel<PATH_UNIT>::Args m{nbin, nbinP, 0, ancType, L.planeMask, L.wf, L.nodeSeq, L.nodeBis,
                                         {L.colT0, L.colT1}};

@@ -131,6 +131,7 @@ __device__ __forceinline__ void score4(const u32* __restrict__ col, u32 Sp, u32 
 
 template <int PATH>
 struct BitModel {
+    static constexpr bool kFusedStale = false;  // stale batches rescan one query at a time
     struct Args {
         u32 nbin, nbinP, nplanes;
         int ancType;
@@ -147,7 +148,9 @@ struct BitModel {
         u32* mseq;
         u32* mbis;
     };
-    __host__ __device__ static size_t engine_smem_bytes(u32 nCTA, u32 Rmax) { return joinx::engine_smem(nCTA, Rmax); }
+    __host__ __device__ static size_t engine_smem_bytes(u32 nCTA, u32 Rmax, u32 deathWords = 0) {
+        return joinx::engine_smem(nCTA, Rmax, deathWords);
+    }
     __host__ static size_t model_smem_bytes(const Args& m) {
         const size_t ne = (size_t)m.nbin * (m.nplanes ? m.nplanes : 1);
         return sizeof(u32) * (kCap + 2 * ne + 2 * m.nbinP) + 16;

@@ -24,6 +24,8 @@
 // or merged children), where node and slot data live, how one pass of
 // candidate scores is computed, and how slot data moves in a compaction.
 #pragma once
+#include <cstdlib>
+
 #include "common.cuh"
 
 namespace casphy {
@@ -33,6 +35,11 @@ constexpr int kThreads = 512;
 constexpr u32 kDead = 0xFFFFFFFFu;
 constexpr u32 kNone = 0xFFFFFFFFu;
 constexpr u32 kMaxCap = 4096;  // candidates per scoring pass (ordOut in smem)
+constexpr u32 kMaxBatch = 8;   // stale rows rescanned in one phase
+constexpr u32 kBatchRecPerLane = 10;  // batch selection reads 2 x nCTA <= 320 table records
+
+// Words of the joined-node bitmap rounded up to keep what follows 16-byte aligned.
+__host__ __device__ inline u32 death_words_padded(u32 deathWords) { return (deathWords + 3u) & ~3u; }
 
 struct BlockRec {
     u64 key;
@@ -52,7 +59,7 @@ struct Common {
     u32* rawEdge;
     BlockRec* pub;        // 2 phases x nCTA x 2
     u32* pubCnt;          // 2 phases x nCTA
-    u64* partial;         // 2 phases x nCTA
+    u64* partial;         // 2 phases x nCTA x kMaxBatch
     u32* counts;          // nCTA
     u32* flags;           // nCTA x 16
     int* err;
@@ -63,27 +70,41 @@ struct Common {
     u32 compactMin;       // do not compact below this many slots
     u32 compactQ8;        // compact when alive*256 < slots*compactQ8
     u32 bytesPerPairSite; // algorithmic bytes per (candidate, query entry), x1000
+    u32 maxBatch;         // stale rows per rescan phase, 1..kMaxBatch
+    u32 deathWords;       // words of the per-CTA shared-memory bitmap of joined nodes (0: none)
     unsigned long long* prof;  // nullable: CTA 0 section times (ns), see PROF_*
 };
 
 // Sections timed by CTA 0 when Common::prof is set.
 enum { PROF_BARRIER = 0, PROF_TABLE, PROF_DECIDE, PROF_BUILD, PROF_SCAN, PROF_POST, PROF_STALE_POST, PROF_COMPACT,
-       PROF_N };
+       PROF_SELECT, PROF_STALE_SCAN, PROF_SC_COPY, PROF_SC_ACC, PROF_SC_RED, PROF_N };
+
+// The section sums live in shared memory (only thread 0 of CTA 0 adds to
+// them), so the persistent loop does not hold them in registers, and model
+// code marks its own sub-sections with prof_mark().
+__shared__ unsigned long long prof_acc[PROF_N + 1];  // [PROF_N] = time of the last mark
+__shared__ int prof_on;
+
+__device__ __forceinline__ void prof_mark(int sec) {
+    if (threadIdx.x != 0 || !prof_on) return;
+    const u64 n = globaltimer_ns();
+    prof_acc[sec] += n - prof_acc[PROF_N];
+    prof_acc[PROF_N] = n;
+}
 
 struct Prof {
-    unsigned long long acc[PROF_N];
-    u64 t;
     bool on;
     __device__ __forceinline__ void init(bool enable) {
         on = enable && threadIdx.x == 0;
-        for (int i = 0; i < PROF_N; i++) acc[i] = 0;
-        t = on ? globaltimer_ns() : 0;
+        if (threadIdx.x == 0) {
+            prof_on = on;
+            for (int i = 0; i <= PROF_N; i++) prof_acc[i] = 0;
+            if (on) prof_acc[PROF_N] = globaltimer_ns();
+        }
+        __syncthreads();
     }
     __device__ __forceinline__ void mark(int sec) {
-        if (!on) return;
-        const u64 n = globaltimer_ns();
-        acc[sec] += n - t;
-        t = n;
+        if (on) prof_mark(sec);
     }
 };
 
@@ -307,16 +328,125 @@ __device__ inline void compact_slots(const Common& a, u32 buf, u32 nb, const Ran
     __syncthreads();
 }
 
+// The rows rescanned in a stale phase: every visible record (the table holds
+// each CTA's top two) whose partner has joined and whose key beats the best
+// visible fresh record, best first, at most maxB.  out[0] is the table's best
+// record.  Rescanning a stale row before the sequential loop would reach it
+// gives the same record the later rescan would (the value is the best over
+// the live rows, ties go to the smaller node and new nodes only replace a
+// record by a strictly larger value), and a join is taken only when the best
+// record is fresh, so the joins come in the sequential order.  Warp 0 selects;
+// every CTA reads the same table and so selects the same rows.
+__device__ inline u32 stale_batch(const Common& a, const Table& t, const u32* deathBits, u32 k, u32 S, u32 maxB,
+                                  BlockRec* out, u32* s_n) {
+    if (threadIdx.x < 32) {
+        const u32 lane = threadIdx.x, nrec = 2 * a.nCTA;
+        u32 staleMask = 0;  // bit j: record lane + 32 j
+        u64 fresh = 0ull;
+        // every partner's death and slot loaded before any is used
+        u32 pn[kBatchRecPerLane], dv[kBatchRecPerLane], sv[kBatchRecPerLane];
+        bool ok[kBatchRecPerLane];
+#pragma unroll
+        for (u32 j = 0; j < kBatchRecPerLane; j++) {
+            const u32 i = lane + 32 * j;
+            ok[j] = i < nrec && (i & 1u) < t.cnt[i >> 1];
+            pn[j] = ok[j] ? t.tab[i].partner : 0u;
+        }
+        if (a.deathWords) {
+            // joined nodes from this CTA's own bitmap: no L2 round trip
+#pragma unroll
+            for (u32 j = 0; j < kBatchRecPerLane; j++) {
+                dv[j] = ok[j] && ((deathBits[pn[j] >> 5] >> (pn[j] & 31)) & 1u) ? 0u : kNone;
+                sv[j] = 0u;
+            }
+        } else {
+#pragma unroll
+            for (u32 j = 0; j < kBatchRecPerLane; j++) {
+                dv[j] = ok[j] ? ld_cg_u32(a.nodeDeath + pn[j]) : 0u;
+                sv[j] = ok[j] ? ld_cg_u32(a.node2slot + pn[j]) : 0u;
+            }
+        }
+#pragma unroll
+        for (u32 j = 0; j < kBatchRecPerLane; j++) {
+            if (!ok[j]) continue;
+            const u64 key = t.tab[lane + 32 * j].key;
+            if (dv[j] < k || sv[j] >= S) staleMask |= 1u << j;
+            else fresh = key > fresh ? key : fresh;
+        }
+        fresh = warp_max_u64(fresh);
+        u32 n = 0;
+        while (n < maxB) {
+            u64 best = 0ull;
+            for (u32 m = staleMask; m; m &= m - 1) {
+                const u32 j = __ffs(m) - 1;
+                const u64 key = t.tab[lane + 32 * j].key;
+                if (key > fresh && key > best) best = key;
+            }
+            const u64 top = warp_max_u64(best);
+            if (top == 0ull) break;
+            // keys of live rows are unique: exactly one lane holds it
+            for (u32 m = staleMask; m; m &= m - 1) {
+                const u32 j = __ffs(m) - 1;
+                if (t.tab[lane + 32 * j].key == top) {
+                    out[n] = t.tab[lane + 32 * j];
+                    staleMask &= ~(1u << j);
+                    break;
+                }
+            }
+            n++;
+        }
+        if (lane == 0) *s_n = n;
+    }
+    __syncthreads();
+    const u32 n = *s_n;
+    __syncthreads();
+    return n;
+}
+
+// Rescans of nb stale rows one query at a time (models without a fused
+// multi-query scan): best[q] gets the top (score, node) key over this CTA's
+// live slots other than row q's own.
+template <class M>
+__device__ inline void stale_scan_each(const Common& a, const typename M::Args& m, typename M::Smem& ms, u32 buf,
+                                       const Range& rg, u32 nb, const BlockRec* rows, u64* best, int* nEout,
+                                       u32* ordOut, u64* red, BlockRec* s_rec, u32* wcount) {
+    const u32* sn = slotNode_of(a, buf);
+    for (u32 q = 0; q < nb; q++) {
+        const u32 c1 = rows[q].slot;
+        const int nE = M::build_stale(m, ms, key_node(rows[q].key), wcount);
+        Top2 tt;
+        tt.init();
+        const u32 cap = M::pass_cap(m, rg.hi - rg.lo);
+        for (u32 base = rg.lo; base < rg.hi; base += cap) {
+            M::score_pass(m, ms, buf, rg, base, cap, nE, ordOut);
+            for (u32 x = threadIdx.x; x < cap && base + x < rg.hi; x += kThreads) {
+                const u32 c = base + x;
+                const u32 node = ld_cg_u32(sn + c);
+                if (node == kDead || c == c1) continue;
+                tt.push(make_key(ordOut[x], node), c, 0u);
+            }
+            __syncthreads();
+        }
+        const BlockRec pr = block_best_rec(tt.k0, tt.s0, 0u, red, s_rec);
+        if (threadIdx.x == 0) {
+            best[q] = pr.key;
+            nEout[q] = nE;
+        }
+    }
+    __syncthreads();
+}
+
 // The join loop for CTA b of a.nCTA co-resident CTAs (b = 0 of 1 when one
 // CTA runs a whole join by itself).  smem: engine + model dynamic memory.
 template <class M>
 __device__ __forceinline__ void join_run(const Common& a, const typename M::Args& m, u32 b, unsigned char* smem) {
     u32* ordOut = reinterpret_cast<u32*>(smem);                        // kMaxCap
-    BlockRec* tabRec = reinterpret_cast<BlockRec*>(ordOut + kMaxCap);  // 2*nCTA
+    u32* deathBits = ordOut + kMaxCap;                                 // joined nodes (deathWords)
+    BlockRec* tabRec = reinterpret_cast<BlockRec*>(deathBits + death_words_padded(a.deathWords));  // 2*nCTA
     u32* ranks = reinterpret_cast<u32*>(tabRec + 2 * a.nCTA);          // Rmax
     unsigned char* tabCnt = reinterpret_cast<unsigned char*>(ranks + a.Rmax);
     unsigned char* tabExact = tabCnt + a.nCTA;
-    unsigned char* msm = smem + M::engine_smem_bytes(a.nCTA, a.Rmax);  // model shared memory
+    unsigned char* msm = smem + M::engine_smem_bytes(a.nCTA, a.Rmax, a.deathWords);  // model shared memory
     typename M::Smem ms;
     M::carve_smem(m, msm, ms);
     __shared__ u64 red[32];
@@ -326,6 +456,10 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
     __shared__ u32 wsum[16];
     __shared__ u32 s_val[4];
     __shared__ int s_flag;
+    __shared__ BlockRec s_batch[kMaxBatch];
+    __shared__ u64 s_pbest[kMaxBatch];
+    __shared__ int s_nE[kMaxBatch];
+    __shared__ u32 s_nb;
 
     const Table T{tabRec, tabCnt, tabExact};
     const u32 nCTA = a.nCTA;
@@ -339,6 +473,7 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
     int fail = 0;
     u32 cnt = 0;
 
+    for (u32 i = threadIdx.x; i < a.deathWords; i += kThreads) deathBits[i] = 0u;
     own_top2(a, buf, rg, red, &s_rec, s_top, &cnt, wsum);
     publish(a, p, b, s_top, cnt);
     if (flag_barrier(a.flags, nCTA, b, ++p, a.err, a.limitNs)) goto out;
@@ -374,75 +509,114 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
         const bool stale = death < k || c2 >= rg.S;
         pf.mark(PROF_DECIDE);
         if (stale) {
-            // rescore j1 against every live slot
-            const int nE = M::build_stale(m, ms, j1, wcount);
-            pf.mark(PROF_BUILD);
-            Top2 tt;
-            tt.init();
-            const u32* sn = slotNode_of(a, buf);
-            const u32 cap = M::pass_cap(m, rg.hi - rg.lo);
-            for (u32 base = rg.lo; base < rg.hi; base += cap) {
-                M::score_pass(m, ms, buf, rg, base, cap, nE, ordOut);
-                for (u32 x = threadIdx.x; x < cap && base + x < rg.hi; x += kThreads) {
-                    const u32 c = base + x;
-                    const u32 node = ld_cg_u32(sn + c);
-                    if (node == kDead || c == c1) continue;
-                    tt.push(make_key(ordOut[x], node), c, 0u);
-                }
+            // rescan a batch of stale rows (the best record first) against every live slot
+            u32 nb = 1;
+            if (a.maxBatch > 1 && 2 * nCTA <= 32 * kBatchRecPerLane) {
+                nb = stale_batch(a, T, deathBits, k, rg.S, a.maxBatch, s_batch, &s_nb);
+            } else {
+                if (threadIdx.x == 0) s_batch[0] = g;
                 __syncthreads();
             }
-            const BlockRec pr = block_best_rec(tt.k0, tt.s0, 0u, red, &s_rec);
-            pf.mark(PROF_SCAN);
-            if (threadIdx.x == 0) {
-                asm volatile("st.global.cg.u64 [%0], %1;" ::"l"(a.partial + (p & 1) * nCTA + b), "l"(pr.key)
+            if (nb == 0 || s_batch[0].slot != c1) { fail = CASPHY_EINTERNAL; break; }
+            pf.mark(PROF_SELECT);
+            if constexpr (M::kFusedStale) {
+                if (nb > 1)
+                    M::stale_multi(m, ms, buf, rg, slotNode_of(a, buf), nb, s_batch, s_pbest, s_nE, ordOut, red,
+                                   wcount);
+                else
+                    stale_scan_each<M>(a, m, ms, buf, rg, 1, s_batch, s_pbest, s_nE, ordOut, red, &s_rec, wcount);
+            } else {
+                stale_scan_each<M>(a, m, ms, buf, rg, nb, s_batch, s_pbest, s_nE, ordOut, red, &s_rec, wcount);
+            }
+            pf.mark(PROF_STALE_SCAN);
+            if (threadIdx.x < nb) {
+                asm volatile("st.global.cg.u64 [%0], %1;" ::"l"(a.partial + ((p & 1) * nCTA + b) * kMaxBatch +
+                                                                  threadIdx.x),
+                             "l"(s_pbest[threadIdx.x])
                              : "memory");
             }
-            nStale++;
-            nPairs += (a.ntip - k) - 1;
-            algMilli += (unsigned long long)a.bytesPerPairSite * (u64)nE * ((a.ntip - k) - 1);
+            for (u32 q = 0; q < nb; q++) {
+                nStale++;
+                nPairs += (a.ntip - k) - 1;
+                algMilli += (unsigned long long)a.bytesPerPairSite * (u64)s_nE[q] * ((a.ntip - k) - 1);
+            }
             if (flag_barrier(a.flags, nCTA, b, ++p, a.err, a.limitNs)) goto out;
             pf.mark(PROF_BARRIER);
-            u64 pb = make_key(a.ordNeg1, 0u);
-            if (nCTA == 1) {
-                pb = pr.key > pb ? pr.key : pb;  // the lone CTA's own best
-            } else {
-                for (u32 i = threadIdx.x; i < nCTA; i += kThreads) {
-                    const u64 v = ld_cg_u64(a.partial + ((p - 1) & 1) * nCTA + i);
-                    pb = v > pb ? v : pb;
-                }
-                pb = block_max_u64(pb, red);
-            }
-            const u32 vOrd = key_ord(pb), vIdx = key_node(pb);
-            const u32 ob = c1 / rg.R;
-            if (ob == b && threadIdx.x == 0) {
-                lmOrd_of(a, buf)[c1] = vOrd;
-                lmIdx_of(a, buf)[c1] = vIdx;
-            }
-            if (threadIdx.x == 0) {
-                BlockRec nr;
-                nr.key = make_key(vOrd, j1);
-                nr.slot = c1;
-                nr.partner = vIdx;
-                BlockRec* L = T.tab + 2 * ob;
-                unsigned char n = T.cnt[ob];
-                if (n == 2) L[0] = L[1];
-                n = n > 0 ? n - 1 : 0;
-                const bool real = vOrd != a.ordNeg1;
-                if (T.exact[ob]) {
-                    if (real) {
-                        if (n == 0) L[0] = nr;
-                        else if (nr.key > L[0].key) { L[1] = L[0]; L[0] = nr; }
-                        else L[1] = nr;
-                        n++;
+            // warp q reduces row q's partial bests over the CTAs
+            {
+                const u32 wq = threadIdx.x >> 5, lane = threadIdx.x & 31;
+                if (wq < nb) {
+                    u64 pb = make_key(a.ordNeg1, 0u);
+                    if (nCTA == 1) {
+                        pb = s_pbest[wq] > pb ? s_pbest[wq] : pb;  // the lone CTA's own best
+                    } else {
+                        // all of a lane's loads issued before any is used
+                        const u64* src = a.partial + ((p - 1) & 1) * nCTA * kMaxBatch + wq;
+                        u64 v[kBatchRecPerLane / 2];
+#pragma unroll
+                        for (u32 j = 0; j < kBatchRecPerLane / 2; j++) {
+                            const u32 i = lane + 32 * j;
+                            v[j] = i < nCTA ? ld_cg_u64(src + (size_t)i * kMaxBatch) : 0ull;
+                        }
+#pragma unroll
+                        for (u32 j = 0; j < kBatchRecPerLane / 2; j++) pb = v[j] > pb ? v[j] : pb;
+                        for (u32 i = lane + 16 * kBatchRecPerLane; i < nCTA; i += 32) {
+                            const u64 x = ld_cg_u64(src + (size_t)i * kMaxBatch);
+                            pb = x > pb ? x : pb;
+                        }
+                        pb = warp_max_u64(pb);
                     }
-                } else if (n >= 1 && real && nr.key > L[n - 1].key) {
-                    if (nr.key > L[0].key) { L[1] = L[0]; L[0] = nr; }
-                    else L[1] = nr;
-                    n = 2;
+                    __syncwarp();
+                    if (lane == 0) s_pbest[wq] = pb;
                 }
-                T.cnt[ob] = n;
             }
             __syncthreads();
+            // owners store the new maxima; every CTA patches its table copy in batch order
+            if (threadIdx.x < nb) {
+                const BlockRec row = s_batch[threadIdx.x];
+                if (row.slot / rg.R == b) {
+                    lmOrd_of(a, buf)[row.slot] = key_ord(s_pbest[threadIdx.x]);
+                    lmIdx_of(a, buf)[row.slot] = key_node(s_pbest[threadIdx.x]);
+                }
+            }
+            if (threadIdx.x == 0) {
+                for (u32 q = 0; q < nb; q++) {
+                    const BlockRec row = s_batch[q];
+                    const u32 vOrd = key_ord(s_pbest[q]), vIdx = key_node(s_pbest[q]);
+                    const u32 ob = row.slot / rg.R;
+                    BlockRec nr;
+                    nr.key = make_key(vOrd, key_node(row.key));
+                    nr.slot = row.slot;
+                    nr.partner = vIdx;
+                    BlockRec* L = T.tab + 2 * ob;
+                    unsigned char n = T.cnt[ob];
+                    // drop the row's old record (it is listed: it was selected from this table)
+                    if (n >= 1 && L[0].slot == row.slot) {
+                        L[0] = L[1];
+                        n--;
+                    } else if (n == 2 && L[1].slot == row.slot) {
+                        n--;
+                    } else {
+                        fail = CASPHY_EINTERNAL;
+                    }
+                    const bool real = vOrd != a.ordNeg1;
+                    if (T.exact[ob]) {
+                        if (real) {
+                            if (n == 0) L[0] = nr;
+                            else if (nr.key > L[0].key) { L[1] = L[0]; L[0] = nr; }
+                            else L[1] = nr;
+                            n++;
+                        }
+                    } else if (n >= 1 && real && nr.key > L[n - 1].key) {
+                        // above the last listed record, hence above every unlisted one
+                        if (nr.key > L[0].key) { L[1] = L[0]; L[0] = nr; }
+                        else L[1] = nr;
+                        n = 2;
+                    }
+                    T.cnt[ob] = n;
+                }
+            }
+            if (__syncthreads_or(fail)) break;
             pf.mark(PROF_STALE_POST);
             continue;
         }
@@ -513,6 +687,10 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
         pf.mark(PROF_POST);
         nPairs += (a.ntip - k - 1) - 1;
         algMilli += (unsigned long long)a.bytesPerPairSite * (u64)nE * ((a.ntip - k - 1) - 1);
+        if (a.deathWords && threadIdx.x == 0) {
+            deathBits[j1 >> 5] |= 1u << (j1 & 31);
+            deathBits[j2 >> 5] |= 1u << (j2 & 31);
+        }
         k++;
         if (flag_barrier(a.flags, nCTA, b, ++p, a.err, a.limitNs)) goto out;
         pf.mark(PROF_BARRIER);
@@ -578,7 +756,7 @@ out:
         a.statsOut[5] = algMilli / 1000ull;
     }
     if (pf.on)
-        for (int i = 0; i < PROF_N; i++) a.prof[i] = pf.acc[i];
+        for (int i = 0; i < PROF_N; i++) a.prof[i] = prof_acc[i];
 }
 
 template <class M>
@@ -587,9 +765,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_join(Common a, typename M::Args
     join_run<M>(a, m, blockIdx.x, smem);
 }
 
+// Host: stale rows per rescan phase (CASPHY_STALE_BATCH, 1..kMaxBatch;
+// default kMaxBatch).
+inline u32 stale_batch_setting() {
+    const char* e = getenv("CASPHY_STALE_BATCH");
+    if (!e) return kMaxBatch;
+    const long v = strtol(e, nullptr, 10);
+    return v < 1 ? 1u : (v > (long)kMaxBatch ? kMaxBatch : (u32)v);
+}
+
 // Host: bytes of engine shared memory before the model's part.
-__host__ __device__ inline size_t engine_smem(u32 nCTA, u32 Rmax) {
-    size_t s = sizeof(u32) * kMaxCap + sizeof(BlockRec) * 2 * nCTA + sizeof(u32) * Rmax + 2 * nCTA;
+__host__ __device__ inline size_t engine_smem(u32 nCTA, u32 Rmax, u32 deathWords = 0) {
+    size_t s = sizeof(u32) * kMaxCap + sizeof(u32) * death_words_padded(deathWords) + sizeof(BlockRec) * 2 * nCTA +
+               sizeof(u32) * Rmax + 2 * nCTA;
     return (s + 15) & ~size_t(15);
 }
 

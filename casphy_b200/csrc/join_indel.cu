@@ -349,6 +349,7 @@ __device__ int build_indel_query(u32 ncol, u32 ncolP, int unitW, const u16* Wsel
 
 template <bool INTP>
 struct IndelDense {
+    static constexpr bool kFusedStale = false;  // stale batches rescan one query at a time
     struct Args {
         u32 ncol, ncolP, nState, minSize;
         float minRatio;
@@ -363,7 +364,9 @@ struct IndelDense {
         u16* eW;
         u16* mrow;
     };
-    __host__ __device__ static size_t engine_smem_bytes(u32 nCTA, u32 Rmax) { return joinx::engine_smem(nCTA, Rmax); }
+    __host__ __device__ static size_t engine_smem_bytes(u32 nCTA, u32 Rmax, u32 deathWords = 0) {
+        return joinx::engine_smem(nCTA, Rmax, deathWords);
+    }
     __host__ static size_t model_smem_bytes(const Args& m) {
         return sizeof(u16) * kCap + sizeof(u32) * m.ncol + sizeof(u16) * (((m.ncol + 7u) & ~7u) + m.ncolP) + 16;
     }
@@ -456,6 +459,8 @@ template struct IndelDense<false>;
 // few logic operations.  The integer path guarantees every score <= 2048.
 
 constexpr int kPlanes = 12;
+constexpr u32 kBitsAlign = 128;      // slots: 4 bitset words, one 16-byte copy
+constexpr u32 kStageWords = 12288;   // 48 KB of staged bitset words per round
 
 // c += x * w in bit-sliced form (w <= 2048)
 __device__ __forceinline__ void vadd(u32 (&c)[kPlanes], u32 x, u32 w) {
@@ -483,6 +488,38 @@ __device__ __forceinline__ void vadd(u32 (&c)[kPlanes], u32 x, u32 w) {
             carry = t;
             if (!carry) break;
         }
+    }
+}
+
+// c += x0 + ... + x7 (unit weights) in bit-sliced form: a carry-save adder
+// tree reduces the eight words to a 4-bit per-slot sum (26 logic operations),
+// which one ripple adds into the planes; about 7.5 operations per word where
+// vadd's carry chain costs several times that.
+__device__ __forceinline__ void fa(u32 a, u32 b, u32 c, u32& s, u32& cy) {
+    const u32 u = a ^ b;
+    s = u ^ c;
+    cy = (a & b) | (u & c);
+}
+__device__ __forceinline__ void vadd8(u32 (&c)[kPlanes], const u32 (&x)[8]) {
+    u32 s0, c0, s1, c1, s2, c2, s4, c4;
+    fa(x[0], x[1], x[2], s0, c0);
+    fa(x[3], x[4], x[5], s1, c1);
+    fa(s0, s1, x[6], s2, c2);
+    const u32 b0 = s2 ^ x[7], c3 = s2 & x[7];   // weight 1, carry of weight 2
+    fa(c0, c1, c2, s4, c4);                       // weight 2 and 4
+    const u32 b1 = s4 ^ c3, c5 = s4 & c3;         // weight 2, carry of weight 4
+    const u32 b2 = c4 ^ c5, b3 = c4 & c5;         // weight 4 and 8
+    u32 cy = c[0] & b0;
+    c[0] ^= b0;
+    u32 t;
+    t = c[1] ^ b1; const u32 n1 = (c[1] & b1) | (t & cy); c[1] = t ^ cy; cy = n1;
+    t = c[2] ^ b2; const u32 n2 = (c[2] & b2) | (t & cy); c[2] = t ^ cy; cy = n2;
+    t = c[3] ^ b3; const u32 n3 = (c[3] & b3) | (t & cy); c[3] = t ^ cy; cy = n3;
+#pragma unroll
+    for (int k = 4; k < kPlanes; k++) {
+        const u32 n = c[k] & cy;
+        c[k] ^= cy;
+        cy = n;
     }
 }
 
@@ -602,6 +639,7 @@ __global__ void __launch_bounds__(kThreads) k_init_bits(InitBitsArgs a) {
 }
 
 struct IndelBits {
+    static constexpr bool kFusedStale = true;  // stale batches share one scan (stale_multi)
     struct Args {
         u32 ncol, ncolP, nState, minSize;
         float minRatio;
@@ -609,6 +647,7 @@ struct IndelBits {
         const u16* Wsel;
         u16* nodeRow;
         u32* bits[2];
+        u32 maxBatch;  // query lists kept for a stale batch
     };
     struct Smem {
         u32* eSC;
@@ -616,17 +655,34 @@ struct IndelBits {
         u16* mrow;
         u16* orow;    // j1's row (the slot's previous occupant)
         u32* planes;  // kThreads x kPlanes
+        u64* bbest;   // kMaxBatch: a stale batch's best keys over the passes
+        u32* bSC;     // maxBatch x ncol: a stale batch's query lists
+        u16* bW;      // maxBatch x ncolW
+        u32* bwc;     // kMaxBatch x 33: per-query warp counts of the fused build
+        u32* stage;   // kStageWords: bitset words copied for the current round
     };
-    __host__ __device__ static size_t engine_smem_bytes(u32 nCTA, u32 Rmax) { return joinx::engine_smem(nCTA, Rmax); }
-    __host__ static size_t model_smem_bytes(const Args& m) {
-        return sizeof(u32) * kThreads * kPlanes + sizeof(u32) * m.ncol +
-               sizeof(u16) * (((m.ncol + 7u) & ~7u) + 2 * m.ncolP) + 16;
+    __host__ __device__ static size_t engine_smem_bytes(u32 nCTA, u32 Rmax, u32 deathWords = 0) {
+        return joinx::engine_smem(nCTA, Rmax, deathWords);
     }
+    __host__ __device__ static u32 ncolW(u32 ncol) { return (ncol + 7u) & ~7u; }
+    __host__ static size_t model_smem_bytes(const Args& m) {
+        return sizeof(u32) * kThreads * kPlanes + sizeof(u32) * kStageWords + sizeof(u64) * joinx::kMaxBatch +
+               sizeof(u32) * m.ncol +
+               sizeof(u32) * (size_t)m.maxBatch * m.ncol + sizeof(u32) * joinx::kMaxBatch * 33 +
+               sizeof(u16) * (ncolW(m.ncol) * (1 + (size_t)m.maxBatch) + 2 * m.ncolP) + 16;
+    }
+    // bytes of one more query list in a stale batch
+    __host__ static size_t batch_list_bytes(u32 ncol) { return sizeof(u32) * ncol + sizeof(u16) * ncolW(ncol); }
     __device__ static void carve_smem(const Args& m, unsigned char* p, Smem& s) {
         s.planes = reinterpret_cast<u32*>(p);
-        s.eSC = s.planes + kThreads * kPlanes;
-        s.eW = reinterpret_cast<u16*>(s.eSC + m.ncol);
-        s.mrow = s.eW + ((m.ncol + 7u) & ~7u);
+        s.stage = s.planes + kThreads * kPlanes;
+        s.bbest = reinterpret_cast<u64*>(s.stage + kStageWords);
+        s.eSC = reinterpret_cast<u32*>(s.bbest + joinx::kMaxBatch);
+        s.bSC = s.eSC + m.ncol;
+        s.bwc = s.bSC + (size_t)m.maxBatch * m.ncol;
+        s.eW = reinterpret_cast<u16*>(s.bwc + joinx::kMaxBatch * 33);
+        s.bW = s.eW + ncolW(m.ncol);
+        s.mrow = s.bW + (size_t)m.maxBatch * ncolW(m.ncol);
         s.orow = s.mrow + m.ncolP;
     }
     __device__ static u32* bitsOf(const Args& m, u32 buf) { return buf ? m.bits[1] : m.bits[0]; }
@@ -661,6 +717,76 @@ struct IndelBits {
         }
     }
     __device__ static u32 pass_cap(const Args&, u32 R) { return min(4096u, (R + 31u) & ~31u); }
+
+    // Bit-sliced counts of nq queries over the bitset words [w0, w0 + Wc) of
+    // this CTA.  Query q's entries are lists eSC/eW + q * stride (nE[q] of
+    // them); the queries' entries form one sequence that is staged in shared
+    // memory round by round: every thread issues its 16-byte cp.async copies
+    // of the round's (entry, 4 words) pieces, so a round costs one trip to
+    // L2/HBM whatever the number of queries and holds no data in registers.
+    // Thread (q, g, t) of set q (setSize threads), group g < F of TG threads,
+    // then adds word t of entries g, g + F, ... of query q into c.
+    __device__ static void staged_counts(const Args& m, Smem& s, const u32* B, u32 Wd, u32 w0, u32 Wc, u32 nq,
+                                         const u32* eSC0, const u16* eW0, u32 strideSC, u32 strideW, const int* nEq,
+                                         u32 setSize, u32 TG, u32 F, u32 (&c)[kPlanes]) {
+        const u32 Wc4 = (Wc + 3u) & ~3u, cpe = Wc4 / 4;  // 16-byte pieces per entry
+        const u32 q = threadIdx.x / setSize, ts = threadIdx.x % setSize;
+        const u32 g = ts / TG, t = ts % TG;
+        __shared__ u32 off[joinx::kMaxBatch + 1];  // query q's entries start at off[q]
+        if (threadIdx.x == 0) {
+            off[0] = 0;
+            for (u32 i = 0; i < nq; i++) off[i + 1] = off[i] + (u32)nEq[i];
+        }
+        __syncthreads();
+        const u32 total = off[nq];
+        const u32 per = kStageWords / Wc4;  // entries per round
+        const u32 myOff = q < nq ? off[q] : 0u, myN = q < nq ? (u32)nEq[q] : 0u;
+        const u16* eWq = eW0 + (size_t)(q < nq ? q : 0) * strideW;
+        const bool active = q < nq && g < F && t < Wc;
+        for (u32 r0 = 0; r0 < total; r0 += per) {
+            const u32 r1 = min(total, r0 + per);
+            for (u32 i = threadIdx.x; i < (r1 - r0) * cpe; i += kThreads) {
+                const u32 ce = r0 + i / cpe, k = i % cpe;
+                u32 qq = 0;
+                while (qq + 1 < nq && ce >= off[qq + 1]) qq++;
+                const u32 sc = eSC0[(size_t)qq * strideSC + (ce - off[qq])];
+                cp_async16(s.stage + (size_t)(ce - r0) * Wc4 + 4 * k,
+                           B + ((size_t)(sc & 0xFFFFu) * m.nState + (sc >> 16) - 2) * Wd + w0 + 4 * k);
+            }
+            cp_async_wait_all();
+            __syncthreads();
+            joinx::prof_mark(joinx::PROF_SC_COPY);
+            if (active) {
+                const u32 lo = max(r0, myOff) - myOff, hi = min(r1, myOff + myN);
+                if (myOff + lo < hi) {
+                    u32 e = lo + (g + F - lo % F) % F;  // first entry >= lo of this group
+                    const u32 end = hi - myOff;
+                    if (m.unitW) {
+                        for (; e + 7 * F < end; e += 8 * F) {
+                            u32 x[8];
+#pragma unroll
+                            for (int j = 0; j < 8; j++) x[j] = s.stage[(size_t)(myOff + e + j * F - r0) * Wc4 + t];
+                            vadd8(c, x);
+                        }
+                    }
+                    for (; e + 3 * F < end; e += 4 * F) {
+                        u32 x[4], wt[4];
+#pragma unroll
+                        for (int j = 0; j < 4; j++) {
+                            x[j] = s.stage[(size_t)(myOff + e + j * F - r0) * Wc4 + t];
+                            wt[j] = eWq[e + j * F];
+                        }
+#pragma unroll
+                        for (int j = 0; j < 4; j++) vadd(c, x[j], wt[j]);
+                    }
+                    for (; e < end; e += F) vadd(c, s.stage[(size_t)(myOff + e - r0) * Wc4 + t], eWq[e]);
+                }
+            }
+            __syncthreads();  // the next round overwrites the stage
+            joinx::prof_mark(joinx::PROF_SC_ACC);
+        }
+    }
+
     __device__ static void score_pass(const Args& m, Smem& s, u32 buf, const joinx::Range& rg, u32 base, u32 cap,
                                       int nE, u32* ordOut) {
         const u32 T = cap / 32;
@@ -668,40 +794,14 @@ struct IndelBits {
         const u32 F = kThreads / TG;
         const u32 g = threadIdx.x / TG, t = threadIdx.x % TG;
         const u32 Wd = rg.Sp / 32;
-        const u32 w = base / 32 + t;
-        const u32* B = bitsOf(m, buf);
+        const u32 Wc = min(T, (rg.hi - base + 31u) / 32u);
         u32 c[kPlanes];
 #pragma unroll
         for (int i = 0; i < kPlanes; i++) c[i] = 0u;
-        if (t < T && w * 32 < rg.hi) {
-            int e = (int)g;
-            for (; e + 15 * (int)F < nE; e += 16 * (int)F) {
-                u32 x[16], wt[16];
-#pragma unroll
-                for (int i = 0; i < 16; i++) {
-                    const u32 sc = s.eSC[e + i * F];
-                    wt[i] = s.eW[e + i * F];
-                    x[i] = ld_cg_u32(B + ((size_t)(sc & 0xFFFFu) * m.nState + (sc >> 16) - 2) * Wd + w);
-                }
-#pragma unroll
-                for (int i = 0; i < 16; i++) vadd(c, x[i], wt[i]);
-            }
-            for (; e + 3 * (int)F < nE; e += 4 * (int)F) {
-                u32 x[4], wt[4];
-#pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    const u32 sc = s.eSC[e + i * F];
-                    wt[i] = s.eW[e + i * F];
-                    x[i] = ld_cg_u32(B + ((size_t)(sc & 0xFFFFu) * m.nState + (sc >> 16) - 2) * Wd + w);
-                }
-#pragma unroll
-                for (int i = 0; i < 4; i++) vadd(c, x[i], wt[i]);
-            }
-            for (; e < nE; e += (int)F) {
-                const u32 sc = s.eSC[e];
-                vadd(c, ld_cg_u32(B + ((size_t)(sc & 0xFFFFu) * m.nState + (sc >> 16) - 2) * Wd + w), s.eW[e]);
-            }
-        }
+        __shared__ int s_nE1;
+        if (threadIdx.x == 0) s_nE1 = nE;
+        __syncthreads();
+        staged_counts(m, s, bitsOf(m, buf), Wd, base / 32, Wc, 1, s.eSC, s.eW, 0, 0, &s_nE1, kThreads, TG, F, c);
         // tree-reduce the F groups' bit-sliced counters
         for (u32 h = F / 2; h >= 1; h /= 2) {
             if (g >= h && g < 2 * h) {
@@ -721,6 +821,180 @@ struct IndelBits {
             const u32 cnt = vget(s.planes + (x >> 5) * kPlanes, x & 31);
             ordOut[x] = ord_f16((u16)half_bits_of_int(cnt));
         }
+        __syncthreads();
+        joinx::prof_mark(joinx::PROF_SC_RED);
+    }
+    // Query lists of nq stale rows at once: the rows are staged in shared
+    // memory (in the planes area, unused until the scan) by one round of
+    // 16-byte loads, then each list is compacted with a block prefix sum; the
+    // nq sums share two block barriers.  List q goes to bSC/bW + q.  Needs
+    // nq * ncolP u16 <= the planes area (build_multi_fits).
+    __device__ static bool build_multi_fits(const Args& m, u32 nq) {
+        return (size_t)nq * m.ncolP * sizeof(u16) <= sizeof(u32) * kThreads * kPlanes;
+    }
+    // Issues the asynchronous copies of the nq rows into the staging area.
+    __device__ static void stage_rows_async(const Args& m, Smem& s, u32 nq, const joinx::BlockRec* rows) {
+        u16* stage = reinterpret_cast<u16*>(s.planes);
+        const u32 v16 = m.ncolP / 8;  // 16-byte words per row (ncolP is a multiple of 8)
+        for (u32 i = threadIdx.x; i < nq * v16; i += kThreads) {
+            const u32 q = i / v16, x = i % v16;
+            cp_async16(stage + (size_t)q * m.ncolP + 8 * x, m.nodeRow + (size_t)key_node(rows[q].key) * m.ncolP + 8 * x);
+        }
+    }
+    // Expects the rows staged (stage_rows_async, then wait and a barrier).
+    __device__ static void build_multi(const Args& m, Smem& s, u32 nq, int* nEout) {
+        const u32 lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        const u16* stage = reinterpret_cast<const u16*>(s.planes);
+        const u32 per = (m.ncol + kThreads - 1) / kThreads;
+        const u32 s0 = threadIdx.x * per, s1 = min(s0 + per, m.ncol);
+        for (u32 q = 0; q < nq; q++) {
+            const u16* row = stage + (size_t)q * m.ncolP;
+            u32 c = 0;
+            for (u32 x = s0; x < s1; x++) c += row[x] > 1;
+            u32 v = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const u32 n = __shfl_up_sync(0xFFFFFFFFu, v, o);
+                if (lane >= (u32)o) v += n;
+            }
+            if (lane == 31) s.bwc[q * 33 + wid] = v;
+        }
+        __syncthreads();
+        // warp q: exclusive offsets of the 16 warps' counts of query q
+        if (wid < nq) {
+            const u32 v = lane < kThreads / 32 ? s.bwc[wid * 33 + lane] : 0u;
+            u32 wi = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const u32 n = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+                if (lane >= (u32)o) wi += n;
+            }
+            __syncwarp();
+            if (lane < kThreads / 32) s.bwc[wid * 33 + 16 + lane] = wi - v;
+            if (lane == kThreads / 32 - 1) s.bwc[wid * 33 + 32] = wi;
+        }
+        __syncthreads();
+        for (u32 q = 0; q < nq; q++) {
+            const u16* row = stage + (size_t)q * m.ncolP;
+            // this thread's offset: its warp's offset plus the earlier lanes' counts
+            u32 c = 0;
+            for (u32 x = s0; x < s1; x++) c += row[x] > 1;
+            u32 v = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const u32 n = __shfl_up_sync(0xFFFFFFFFu, v, o);
+                if (lane >= (u32)o) v += n;
+            }
+            u32 pos = s.bwc[q * 33 + 16 + wid] + v - c;
+            u32* eSC = s.bSC + (size_t)q * m.ncol;
+            u16* eW = s.bW + (size_t)q * ncolW(m.ncol);
+            for (u32 x = s0; x < s1; x++) {
+                const u32 code = row[x];
+                if (code > 1) {
+                    eSC[pos] = x | (code << 16);
+                    eW[pos] = m.unitW ? (u16)1 : m.Wsel[(size_t)(code - 2) * m.ncol + x];
+                    pos++;
+                }
+            }
+        }
+        if (threadIdx.x < nq) nEout[threadIdx.x] = (int)s.bwc[threadIdx.x * 33 + 32];
+        __syncthreads();
+    }
+
+    // Rescans of nq stale rows in one pass over the allele bitsets.  The CTA
+    // splits into nq thread sets (512/2^ceil(log2 nq) threads each); in set q
+    // thread (g, t) adds query q's entries g, g+F, ... for the 32 slots of
+    // word t, so all nq queries' bitset loads are in flight together.  The F
+    // groups' bit-sliced counters are summed in shared memory and best[q]
+    // gets the top (score, node) key over the live slots other than row q's.
+    __device__ static void stale_multi(const Args& m, Smem& s, u32 buf, const joinx::Range& rg, const u32* sn, u32 nq,
+                                       const joinx::BlockRec* rows, u64* best, int* nEout, u32* snCache, u64* red,
+                                       u32* wc) {
+        const u32 nqP = nq <= 1 ? 1u : (nq <= 2 ? 2u : (nq <= 4 ? 4u : 8u));
+        const u32 setSize = kThreads / nqP;
+        const u32 capMax = min(setSize * 32u, joinx::kMaxCap);
+        // the first pass's slot nodes and the staged rows share one round trip
+        const u32 cap0 = min(capMax, (rg.hi - rg.lo + 31u) & ~31u);
+        if (rg.lo < rg.hi)
+            for (u32 i = threadIdx.x; i < cap0 / 4; i += kThreads) cp_async16(snCache + 4 * i, sn + rg.lo + 4 * i);
+        const bool fused = build_multi_fits(m, nq);
+        if (fused) stage_rows_async(m, s, nq, rows);
+        cp_async_wait_all();
+        __syncthreads();
+        if (fused) {
+            build_multi(m, s, nq, nEout);
+        } else {
+            for (u32 q = 0; q < nq; q++) {
+                const int n = build_indel_query(m.ncol, m.ncolP, m.unitW, m.Wsel,
+                                                m.nodeRow + (size_t)key_node(rows[q].key) * m.ncolP, nullptr, 0,
+                                                nullptr, nullptr, s.bSC + (size_t)q * m.ncol,
+                                                s.bW + (size_t)q * ncolW(m.ncol), wc);
+                if (threadIdx.x == 0) nEout[q] = n;
+            }
+            __syncthreads();
+        }
+        const u32 q = threadIdx.x / setSize, ts = threadIdx.x % setSize;
+        const u32 lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        const u32 Wd = rg.Sp / 32;
+        const u32* B = bitsOf(m, buf);
+        const u32 myRow = q < nq ? rows[q].slot : kNone;
+        if (threadIdx.x < joinx::kMaxBatch) s.bbest[threadIdx.x] = 0ull;
+        for (u32 base = rg.lo; base < rg.hi; base += capMax) {
+            const u32 cap = min(capMax, (rg.hi - base + 31u) & ~31u);
+            const u32 Wc = cap / 32;
+            if (base != rg.lo) {  // later passes copy their slot nodes here
+                __syncthreads();
+                for (u32 i = threadIdx.x; i < cap / 4; i += kThreads) cp_async16(snCache + 4 * i, sn + base + 4 * i);
+                cp_async_wait_all();
+                __syncthreads();
+            }
+            // TG threads per group (a power of two >= Wc) and F <= 16 groups
+            // sharing a word's entries (group 0 sums the others' counters)
+            u32 TG = 32;
+            while (TG < Wc) TG *= 2;
+            const u32 F = min(setSize / TG, 16u);
+            const u32 g = ts / TG, t = ts % TG;
+            u32 c[kPlanes];
+#pragma unroll
+            for (int i = 0; i < kPlanes; i++) c[i] = 0u;
+            staged_counts(m, s, B, Wd, base / 32, Wc, nq, s.bSC, s.bW, m.ncol, ncolW(m.ncol), nEout, setSize, TG, F,
+                          c);
+            // sum the F groups' counters of (q, t) into group 0's smem entry
+            u32* P = s.planes + (size_t)q * setSize * kPlanes;
+            if (q < nq && g < F && g > 0 && t < Wc) {
+#pragma unroll
+                for (int i = 0; i < kPlanes; i++) P[(g * TG + t) * kPlanes + i] = c[i];
+            }
+            __syncthreads();
+            if (q < nq && g == 0 && t < Wc) {
+                for (u32 gg = 1; gg < F; gg++) vsum(c, P + (gg * TG + t) * kPlanes);
+#pragma unroll
+                for (int i = 0; i < kPlanes; i++) P[t * kPlanes + i] = c[i];
+            }
+            __syncthreads();
+            // best key of query q over this pass's live slots
+            u64 bk = 0ull;
+            if (q < nq) {
+                for (u32 x = ts; x < cap; x += setSize) {
+                    const u32 slot = base + x, node = snCache[x];
+                    if (slot >= rg.hi || node == joinx::kDead || slot == myRow) continue;
+                    const u32 cnt = vget(P + (x >> 5) * kPlanes, x & 31);
+                    const u64 key = make_key(ord_f16((u16)half_bits_of_int(cnt)), node);
+                    bk = key > bk ? key : bk;
+                }
+            }
+            bk = warp_max_u64(bk);
+            if (lane == 0) red[wid] = bk;
+            __syncthreads();
+            if (threadIdx.x < nq) {
+                const u32 w0 = threadIdx.x * (setSize / 32), w1 = w0 + setSize / 32;
+                u64 b2 = s.bbest[threadIdx.x];
+                for (u32 i = w0; i < w1; i++) b2 = red[i] > b2 ? red[i] : b2;
+                s.bbest[threadIdx.x] = b2;
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x < nq) best[threadIdx.x] = s.bbest[threadIdx.x];
         __syncthreads();
     }
     // C1: clear this CTA's words of the new layout in every row
@@ -821,13 +1095,16 @@ struct IndelBuffers {
 
 // Bytes of the two allele-bitset buffers for the bitset scan.
 static size_t bits_bytes(u32 ntip, u32 ncol, u32 nState) {
-    const size_t Wd = ((size_t)ntip + 31) / 32;
+    const size_t Wd = ((size_t)ntip + kBitsAlign - 1) / kBitsAlign * (kBitsAlign / 32);
     return 2 * (size_t)ncol * nState * Wd * sizeof(u32);
 }
 
 static IndelBuffers carve_indel(Carve& c, u32 ntip, u32 ncol, u32 nState, u32 nCTA, u32 nChunks, bool useBits) {
     const u32 nnode = 2 * ntip - 1, nedge = 2 * ntip - 2;
-    const u32 ncolP = (ncol + 7u) & ~7u, Sp = (ntip + 31u) & ~31u;
+    // the bitset scan copies 16-byte pieces of bitset rows: slot ranges and
+    // row strides are multiples of 128 slots (kBitsAlign)
+    const u32 ncolP = (ncol + 7u) & ~7u, Sp = useBits ? (ntip + kBitsAlign - 1) / kBitsAlign * kBitsAlign
+                                                      : (ntip + 31u) & ~31u;
     const size_t nw = (size_t)nState * ncol;
     IndelBuffers l;
     l.Wsel = c.take<u16>(nw ? nw : 1);
@@ -848,7 +1125,7 @@ static IndelBuffers carve_indel(Carve& c, u32 ntip, u32 ncol, u32 nState, u32 nC
     l.initKey = c.take<unsigned long long>(ntip);
     l.pub = c.take<joinx::BlockRec>(4 * nCTA);
     l.pubCnt = c.take<u32>(2 * nCTA);
-    l.partial = c.take<u64>(2 * nCTA);
+    l.partial = c.take<u64>((size_t)2 * nCTA * joinx::kMaxBatch);
     l.counts = c.take<u32>(nCTA);
     l.flags = c.take<u32>(16 * nCTA);
     l.jerr = c.take<int>(1);
@@ -868,6 +1145,30 @@ static void chunk_table(u32 ntip, u32 nChunks, u64* chunkStart) {
     }
 }
 
+// Launches the persistent join of model M after fitting its shared memory
+// to the device: first fewer query lists per stale batch (when the model
+// keeps them, *batch), then no joined-node bitmap (the engine then reads
+// node deaths from global memory).
+template <class M>
+static int launch_join_fitted(joinx::Common& c, typename M::Args& m, u32* batch, u32 nCTA, cudaStream_t st) {
+    int smemMax = 0, dev = 0;
+    CASPHY_CUDA_TRY(cudaGetDevice(&dev));
+    CASPHY_CUDA_TRY(cudaDeviceGetAttribute(&smemMax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const size_t lim = (size_t)smemMax - 4096;  // the kernel's static shared memory
+    auto need = [&] { return M::engine_smem_bytes(nCTA, c.Rmax, c.deathWords) + M::model_smem_bytes(m); };
+    if (batch) {
+        while (*batch > 1 && need() > lim) (*batch)--;
+        c.maxBatch = *batch;
+    }
+    if (need() > lim) c.deathWords = 0;
+    const size_t smem = need();
+    void* fn = (void*)joinx::k_join<M>;
+    CASPHY_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    void* args[] = {&c, &m};
+    CASPHY_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(nCTA), dim3(kThreads), args, smem, st));
+    return CASPHY_OK;
+}
+
 // Launches prep, initial scan and the persistent join.  Assumes Wsel,
 // tipSize and chunkStart are already on the device; clears everything the
 // kernels expect at zero.  Returns the number of kernels launched.
@@ -877,7 +1178,7 @@ static int launch_indel(const IndelBuffers& L, u32 ntip, u32 ncol, u32 nState, c
     const u32 nnode = 2 * ntip - 1;
     // slot stride: bitset words need multiples of 32 slots, the u16 column
     // scan multiples of 8 (one 16-byte load); the engine uses the same rule
-    const u32 align = useBits ? 32u : 8u;
+    const u32 align = useBits ? kBitsAlign : 8u;
     const u32 ncolP = (ncol + 7u) & ~7u, Sp = (ntip + align - 1) / align * align;
     const u32 nCTA = nSM;
     CASPHY_CUDA_TRY(cudaMemsetAsync(L.prepErr, 0, sizeof(int), st));
@@ -931,33 +1232,25 @@ static int launch_indel(const IndelBuffers& L, u32 ntip, u32 ncol, u32 nState, c
     c.prof = getenv("CASPHY_PROFILE") ? L.stats + 8 : nullptr;
     c.Rmax = (((ntip + nCTA - 1) / nCTA) + 31u) & ~31u;
     c.ordNeg1 = ORD_F16_NEG1; c.compactMin = 4096; c.compactQ8 = 192; c.bytesPerPairSite = 2000;
+    c.maxBatch = joinx::stale_batch_setting();
+    c.deathWords = (nnode + 31) / 32;  // 50 KB at 200k cells
     if (useBits) {
         using M = IndelBits;
-        c.align = 32;
+        c.align = kBitsAlign;
+        c.Rmax = (((ntip + nCTA - 1) / nCTA) + kBitsAlign - 1) / kBitsAlign * kBitsAlign;
         c.compactQ8 = 128;
         c.bytesPerPairSite = 125;  // one bit per (candidate, query site)
-        M::Args m{ncol, ncolP, nState, minSize, minRatio, unitW ? 1 : 0, L.Wsel, L.nodeRow, {L.bits0, L.bits1}};
-        const size_t smem = M::engine_smem_bytes(nCTA, c.Rmax) + M::model_smem_bytes(m);
-        void* fn = (void*)joinx::k_join<M>;
-        CASPHY_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        void* args[] = {&c, &m};
-        CASPHY_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(nCTA), dim3(kThreads), args, smem, st));
+        M::Args m{ncol, ncolP, nState, minSize, minRatio, unitW ? 1 : 0, L.Wsel, L.nodeRow, {L.bits0, L.bits1},
+                  c.maxBatch};
+        if (int rc = launch_join_fitted<M>(c, m, &m.maxBatch, nCTA, st)) return rc;
     } else if (intPath) {
         using M = IndelDense<true>;
         M::Args m{ncol, ncolP, nState, minSize, minRatio, unitW ? 1 : 0, L.Wsel, L.nodeRow, {L.colT0, L.colT1}};
-        const size_t smem = M::engine_smem_bytes(nCTA, c.Rmax) + M::model_smem_bytes(m);
-        void* fn = (void*)joinx::k_join<M>;
-        CASPHY_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        void* args[] = {&c, &m};
-        CASPHY_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(nCTA), dim3(kThreads), args, smem, st));
+        if (int rc = launch_join_fitted<M>(c, m, nullptr, nCTA, st)) return rc;
     } else {
         using M = IndelDense<false>;
         M::Args m{ncol, ncolP, nState, minSize, minRatio, 0, L.Wsel, L.nodeRow, {L.colT0, L.colT1}};
-        const size_t smem = M::engine_smem_bytes(nCTA, c.Rmax) + M::model_smem_bytes(m);
-        void* fn = (void*)joinx::k_join<M>;
-        CASPHY_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        void* args[] = {&c, &m};
-        CASPHY_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(nCTA), dim3(kThreads), args, smem, st));
+        if (int rc = launch_join_fitted<M>(c, m, nullptr, nCTA, st)) return rc;
     }
     n++;
     *launches = n;
@@ -1050,8 +1343,9 @@ static int join_indel_impl(u32 ntip, u32 ncol, const u32* d_codes, u32 nState, c
         }
         joinx::preorder_relabel(ntip, raw.data(), edge_out, order.data());
         if (getenv("CASPHY_PROFILE")) {
-            static const char* names[joinx::PROF_N] = {"barrier", "table", "decide", "build",
-                                                       "scan", "post", "stale_post", "compact"};
+            static const char* names[joinx::PROF_N] = {"barrier", "table", "decide", "build", "scan", "post",
+                                                       "stale_post", "compact", "select", "stale_scan",
+                                                       "sc_copy", "sc_acc", "sc_red"};
             fprintf(stderr, "join-loop sections (CTA 0, ms):");
             for (int i = 0; i < joinx::PROF_N; i++) fprintf(stderr, " %s=%.1f", names[i], prof[i] / 1e6);
             fprintf(stderr, "\n");

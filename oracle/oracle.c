@@ -766,7 +766,7 @@ static int phased_join_run(const PhasedModel *m, u32 ntip, u32 maxBatch, int pai
     int st = book_init(&R.b, ntip);
     if (st || !batch || !R.localMax || !R.shared || !R.rawState) { st = ORACLE_ENOMEM; goto done; }
     JoinBook *b = &R.b;
-    u64 nStale = 0, nJoin = 0, nPhase = 0, nPaired = 0, nHidden = 0;
+    u64 nStale = 0, nJoin = 0, nPhase = 0, nPaired = 0, nHidden = 0, nRiding = 0;
 
     for (u32 i = 0; i + 1 < ntip; i++) {
 #pragma omp parallel for num_threads(R.nthreads) schedule(static)
@@ -791,10 +791,11 @@ static int phased_join_run(const PhasedModel *m, u32 ntip, u32 maxBatch, int pai
             if (better(v, node, bv, bi)) { bv = v; bi = node; }
             if (node < nnode && phased_fresh(&R, c) && better(v, node, fv, fi)) { fv = v; fi = node; }
         }
-        const u32 j1 = bi;
+        u32 j1 = bi;
         if (j1 >= nnode || b->node2cache[j1] >= ntip) { st = ORACLE_EINTERNAL; goto done; }
-        const u32 c1 = b->node2cache[j1];
-        if (!phased_fresh(&R, c1)) {
+        u32 jj = j1;
+        if (!phased_fresh(&R, b->node2cache[j1])) {
+            const u32 c1 = b->node2cache[j1];
             /* one phase: the stale rows that beat the best fresh record, best first */
             u32 n = 0;
             for (u32 c = 0; c < ntip; c++) {
@@ -817,8 +818,21 @@ static int phased_join_run(const PhasedModel *m, u32 ntip, u32 maxBatch, int pai
             for (u32 x = 0; x < n; x++) phased_rescan(&R, batch[x]);
             nStale += n;
             nPhase++;
-            continue;
+            /* the join of the best fresh record rides along when it is still
+             * the decision after the rescans (bit 1 of pairJoins) */
+            if (!(pairJoins & 2) || fv < 0) continue;
+            double b2 = -1.0;
+            u32 i2 = 0;
+            for (u32 c = 0; c < ntip; c++)
+                if (better(R.localMax[c], b->cache2node[c], b2, i2)) { b2 = R.localMax[c]; i2 = b->cache2node[c]; }
+            if (i2 != fi || !phased_fresh(&R, b->node2cache[fi])) continue;
+            jj = fi;
+            nRiding++;
+        } else {
+            nPhase++;
         }
+        const u32 c1 = b->node2cache[jj];
+        j1 = jj;
         const u32 j2 = b->localMaxIdx[c1], c2 = b->node2cache[j2];
         /* the best record among the other rows, before this join */
         double vcd = -1.0;
@@ -829,7 +843,7 @@ static int phased_join_run(const PhasedModel *m, u32 ntip, u32 maxBatch, int pai
         }
         int ok = 0;
         u32 cc = ntip, dNode = nnode;
-        if (pairJoins && vcd >= 0 && cNode < nnode && b->node2cache[cNode] < ntip) {
+        if ((pairJoins & 1) && vcd >= 0 && cNode < nnode && b->node2cache[cNode] < ntip) {
             cc = b->node2cache[cNode];
             dNode = b->localMaxIdx[cc];
             ok = phased_fresh(&R, cc) && dNode != j1 && dNode != j2;
@@ -840,7 +854,6 @@ static int phased_join_run(const PhasedModel *m, u32 ntip, u32 maxBatch, int pai
         }
         phased_join(&R, j1, j2, c1, c2, vcd, cNode, ok ? &ok : NULL);
         nJoin++;
-        nPhase++;
         if (ok && R.nodeCount < nnode) {
             phased_join(&R, cNode, dNode, cc, b->node2cache[dNode], 0.0, 0, NULL);
             nJoin++;
@@ -851,7 +864,7 @@ static int phased_join_run(const PhasedModel *m, u32 ntip, u32 maxBatch, int pai
     st = dfs_output(b, R.rawState, m->rowlen, edge_out, state_out);
     if (stats) {
         stats[0] = nStale; stats[1] = R.nPairs; stats[2] = nJoin; stats[3] = nPhase; stats[4] = nPaired;
-        stats[5] = nHidden;
+        stats[5] = nHidden; stats[6] = nRiding;
     }
 done:
     book_free(&R.b);

@@ -80,10 +80,12 @@ def join_indel(codes, nstate, w, tip_size=None, min_size=0, min_ratio=2.0, nthre
 
 
 def join_indel_phased(codes, nstate, w, tip_size=None, min_size=0, min_ratio=2.0, max_batch=8, pair_joins=True,
-                      table_ctas=0, nthreads=0):
+                      table_ctas=0, nthreads=0, ride=False):
     """The indel join in phases (oracle_join_indel_phased); stats adds
-    [3] phases, [4] phases with two joins and [5] pairs a top-2 table over
-    `table_ctas` ranges could not vouch for."""
+    [3] phases, [4] phases with two joins, [5] pairs a top-2 table over
+    `table_ctas` ranges could not vouch for and [6] joins made in a rescan
+    phase because the best fresh record was still the decision after the
+    rescans (`ride`)."""
     codes = _u32(codes)
     ntip, ncol = codes.shape
     w = np.ascontiguousarray(w, dtype=np.float64).reshape(-1)
@@ -91,9 +93,9 @@ def join_indel_phased(codes, nstate, w, tip_size=None, min_size=0, min_ratio=2.0
     nedge = 2 * ntip - 2
     edge = np.zeros(max(nedge, 1) * 2, dtype=np.uint32)
     state = np.zeros(max(ntip - 1, 1) * ncol, dtype=np.uint32)
-    stats = np.zeros(6, dtype=np.uint64)
+    stats = np.zeros(7, dtype=np.uint64)
     _chk(lib().oracle_join_indel_phased(ntip, ncol, codes, nstate, w, ts, min_size, min_ratio, max_batch,
-                                        1 if pair_joins else 0, table_ctas, edge, state, stats,
+                                        (1 if pair_joins else 0) | (2 if ride else 0), table_ctas, edge, state, stats,
                                         nthreads or os.cpu_count()),
          "join_indel_phased")
     return edge[: 2 * nedge].reshape(nedge, 2), state.reshape(-1, ncol), stats
@@ -262,10 +264,12 @@ def approx_compare(clade_rows, ntip, edge1, edge2, nnode2=None, cache_size=8192,
     return r, q
 
 
-def join_bit_phased(words, w=None, ancestral_type=1, max_batch=8, pair_joins=True, table_ctas=0, nthreads=0):
+def join_bit_phased(words, w=None, ancestral_type=1, max_batch=8, pair_joins=True, table_ctas=0, nthreads=0,
+                    ride=False):
     """The bit join in phases (oracle_join_bit_phased); stats adds [3] phases,
-    [4] phases with two joins and [5] pairs a top-2 table over `table_ctas`
-    ranges could not vouch for."""
+    [4] phases with two joins, [5] pairs a top-2 table over `table_ctas`
+    ranges could not vouch for and [6] joins made in a rescan phase
+    (`ride`)."""
     words = _u32(words)
     ntip, nbin = words.shape
     w = np.ones(nbin * 32) if w is None else w
@@ -273,7 +277,8 @@ def join_bit_phased(words, w=None, ancestral_type=1, max_batch=8, pair_joins=Tru
     nedge = 2 * ntip - 2
     edge = np.zeros(max(nedge, 1) * 2, dtype=np.uint32)
     state = np.zeros(max(ntip - 1, 1) * nbin, dtype=np.uint32)
-    stats = np.zeros(6, dtype=np.uint64)
-    _chk(lib().oracle_join_bit_phased(ntip, nbin, words, w, ancestral_type, max_batch, 1 if pair_joins else 0,
+    stats = np.zeros(7, dtype=np.uint64)
+    _chk(lib().oracle_join_bit_phased(ntip, nbin, words, w, ancestral_type, max_batch,
+                                      (1 if pair_joins else 0) | (2 if ride else 0),
                                       table_ctas, edge, state, stats, nthreads or os.cpu_count()), "join_bit_phased")
     return edge[: 2 * nedge].reshape(nedge, 2), state.reshape(-1, nbin), stats

@@ -34,3 +34,11 @@ def gpu_lib():
     import casphy_b200.lib as L
     L.lib()
     return L
+
+
+@pytest.fixture(params=["1", "8"])
+def stale_batch(request, monkeypatch):
+    """Run a join test with one stale rescan per phase (the sequential
+    schedule, whose counts equal the oracle's) and with batches of up to 8."""
+    monkeypatch.setenv("CASPHY_STALE_BATCH", request.param)
+    return int(request.param)

@@ -29,12 +29,15 @@ def test_golden_bit_joins(golden, gpu_lib):
 
 @pytest.mark.parametrize("at", [0, 1])
 @pytest.mark.parametrize("seed,ncell,nsite", [(201, 3000, 512), (202, 900, 96), (203, 6000, 64)])
-def test_random_bit_vs_oracle(gpu_lib, seed, ncell, nsite, at):
+def test_random_bit_vs_oracle(gpu_lib, stale_batch, seed, ncell, nsite, at):
     words = synth.binary_workload(ncell, nsite, 14, 0.04, 0.05, seed=seed)
     e1, s1, st1 = gpu_lib.join_bit(words, None, at)
     e0, s0, st0 = O.join_bit(words, None, at)
     assert np.array_equal(e1, e0) and np.array_equal(s1, s0)
-    assert st1["stale_recomputes"] == st0[0]
+    if stale_batch == 1:
+        assert st1["stale_recomputes"] == st0[0]
+    else:
+        assert st1["stale_recomputes"] >= st0[0]
 
 
 def test_integer_weight_planes(gpu_lib):
