@@ -341,7 +341,6 @@ __device__ inline u32 stale_batch(const Common& a, const Table& t, const u32* de
                                   BlockRec* out, u32* s_n) {
     if (threadIdx.x < 32) {
         const u32 lane = threadIdx.x, nrec = 2 * a.nCTA;
-        u32 staleMask = 0;  // bit j: record lane + 32 j
         u64 fresh = 0ull;
         // every partner's death and slot loaded before any is used
         u32 pn[kBatchRecPerLane], dv[kBatchRecPerLane], sv[kBatchRecPerLane];
@@ -366,31 +365,31 @@ __device__ inline u32 stale_batch(const Common& a, const Table& t, const u32* de
                 sv[j] = ok[j] ? ld_cg_u32(a.node2slot + pn[j]) : 0u;
             }
         }
+        // candidate keys (stale, above the best fresh record) stay in registers
+        u64 ck[kBatchRecPerLane];
 #pragma unroll
         for (u32 j = 0; j < kBatchRecPerLane; j++) {
-            if (!ok[j]) continue;
-            const u64 key = t.tab[lane + 32 * j].key;
-            if (dv[j] < k || sv[j] >= S) staleMask |= 1u << j;
-            else fresh = key > fresh ? key : fresh;
+            const u64 key = ok[j] ? t.tab[lane + 32 * j].key : 0ull;
+            const bool st = ok[j] && (dv[j] < k || sv[j] >= S);
+            ck[j] = st ? key : 0ull;
+            if (ok[j] && !st) fresh = key > fresh ? key : fresh;
         }
         fresh = warp_max_u64(fresh);
+#pragma unroll
+        for (u32 j = 0; j < kBatchRecPerLane; j++) ck[j] = ck[j] > fresh ? ck[j] : 0ull;
         u32 n = 0;
         while (n < maxB) {
             u64 best = 0ull;
-            for (u32 m = staleMask; m; m &= m - 1) {
-                const u32 j = __ffs(m) - 1;
-                const u64 key = t.tab[lane + 32 * j].key;
-                if (key > fresh && key > best) best = key;
-            }
+#pragma unroll
+            for (u32 j = 0; j < kBatchRecPerLane; j++) best = ck[j] > best ? ck[j] : best;
             const u64 top = warp_max_u64(best);
             if (top == 0ull) break;
             // keys of live rows are unique: exactly one lane holds it
-            for (u32 m = staleMask; m; m &= m - 1) {
-                const u32 j = __ffs(m) - 1;
-                if (t.tab[lane + 32 * j].key == top) {
+#pragma unroll
+            for (u32 j = 0; j < kBatchRecPerLane; j++) {
+                if (ck[j] == top) {
                     out[n] = t.tab[lane + 32 * j];
-                    staleMask &= ~(1u << j);
-                    break;
+                    ck[j] = 0ull;
                 }
             }
             n++;
@@ -520,7 +519,7 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
             if (nb == 0 || s_batch[0].slot != c1) { fail = CASPHY_EINTERNAL; break; }
             pf.mark(PROF_SELECT);
             if constexpr (M::kFusedStale) {
-                if (nb > 1)
+                if (nb >= 1)
                     M::stale_multi(m, ms, buf, rg, slotNode_of(a, buf), nb, s_batch, s_pbest, s_nE, ordOut, red,
                                    wcount);
                 else

@@ -460,7 +460,7 @@ template struct IndelDense<false>;
 
 constexpr int kPlanes = 12;
 constexpr u32 kBitsAlign = 128;      // slots: 4 bitset words, one 16-byte copy
-constexpr u32 kStageWords = 12288;   // 48 KB of staged bitset words per round
+constexpr u32 kStageWords = 14336;   // 56 KB of staged bitset words per round (325 entries of 44 words)
 
 // c += x * w in bit-sliced form (w <= 2048)
 __device__ __forceinline__ void vadd(u32 (&c)[kPlanes], u32 x, u32 w) {
@@ -563,6 +563,7 @@ __global__ void k_build_bits(const u16* __restrict__ nodeRow, u32 ntip, u32 ncol
 
 struct InitBitsArgs {
     u32 ntip, ncol, nState, Wd;
+    int unitW;
     const u32* bits;
     const u32* eSC;
     const u16* eW;
@@ -607,8 +608,12 @@ __global__ void __launch_bounds__(kThreads) k_init_bits(InitBitsArgs a) {
                     wt[i] = ew[e + i];
                     x[i] = __ldg(a.bits + ((size_t)(sc & 0xFFFFu) * a.nState + (sc >> 16) - 2) * a.Wd + w);
                 }
+                if (a.unitW) {
+                    vadd8(c, x);
+                } else {
 #pragma unroll
-                for (int i = 0; i < 8; i++) vadd(c, x[i], wt[i]);
+                    for (int i = 0; i < 8; i++) vadd(c, x[i], wt[i]);
+                }
             }
             for (; e < nE; e++) {
                 const u32 sc = es[e];
@@ -743,80 +748,106 @@ struct IndelBits {
         const u32 myOff = q < nq ? off[q] : 0u, myN = q < nq ? (u32)nEq[q] : 0u;
         const u16* eWq = eW0 + (size_t)(q < nq ? q : 0) * strideW;
         const bool active = q < nq && g < F && t < Wc;
-        for (u32 r0 = 0; r0 < total; r0 += per) {
-            const u32 r1 = min(total, r0 + per);
-            for (u32 i = threadIdx.x; i < (r1 - r0) * cpe; i += kThreads) {
-                const u32 ce = r0 + i / cpe, k = i % cpe;
-                u32 qq = 0;
+        // copy mapping: lane = (entry j of the warp's epw, piece k); no division in the loop
+        const u32 lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        const u32 epw = 32 / cpe, jl = lane / cpe, kl = lane % cpe;
+        const bool copier = jl < epw;
+        // copies of entries [a, b) of the round starting at r0
+        auto copy_range = [&](u32 r0, u32 a, u32 b) {
+            if (!copier) return;
+            u32 qq = 0;
+            for (u32 ce = a + wid * epw + jl; ce < b; ce += (kThreads / 32) * epw) {
                 while (qq + 1 < nq && ce >= off[qq + 1]) qq++;
                 const u32 sc = eSC0[(size_t)qq * strideSC + (ce - off[qq])];
-                cp_async16(s.stage + (size_t)(ce - r0) * Wc4 + 4 * k,
-                           B + ((size_t)(sc & 0xFFFFu) * m.nState + (sc >> 16) - 2) * Wd + w0 + 4 * k);
+                cp_async16(s.stage + (size_t)(ce - r0) * Wc4 + 4 * kl,
+                           B + ((size_t)(sc & 0xFFFFu) * m.nState + (sc >> 16) - 2) * Wd + w0 + 4 * kl);
             }
-            cp_async_wait_all();
-            __syncthreads();
-            joinx::prof_mark(joinx::PROF_SC_COPY);
-            if (active) {
-                const u32 lo = max(r0, myOff) - myOff, hi = min(r1, myOff + myN);
-                if (myOff + lo < hi) {
-                    u32 e = lo + (g + F - lo % F) % F;  // first entry >= lo of this group
-                    const u32 end = hi - myOff;
-                    if (m.unitW) {
-                        for (; e + 7 * F < end; e += 8 * F) {
-                            u32 x[8];
+        };
+        // this thread's additions from the staged entries [a, b)
+        auto add_range = [&](u32 r0, u32 a, u32 b) {
+            if (!active) return;
+            const u32 lo = max(a, myOff) - myOff, hi = min(b, myOff + myN);
+            if (myOff + lo >= hi) return;
+            u32 e = lo + (g + F - lo % F) % F;  // first entry >= lo of this group
+            const u32 end = hi - myOff;
+            if (m.unitW) {
+                for (; e < end; e += 8 * F) {  // the last group of 8 is padded with zero words
+                    u32 x[8];
 #pragma unroll
-                            for (int j = 0; j < 8; j++) x[j] = s.stage[(size_t)(myOff + e + j * F - r0) * Wc4 + t];
-                            vadd8(c, x);
-                        }
-                    }
-                    for (; e + 3 * F < end; e += 4 * F) {
-                        u32 x[4], wt[4];
-#pragma unroll
-                        for (int j = 0; j < 4; j++) {
-                            x[j] = s.stage[(size_t)(myOff + e + j * F - r0) * Wc4 + t];
-                            wt[j] = eWq[e + j * F];
-                        }
-#pragma unroll
-                        for (int j = 0; j < 4; j++) vadd(c, x[j], wt[j]);
-                    }
-                    for (; e < end; e += F) vadd(c, s.stage[(size_t)(myOff + e - r0) * Wc4 + t], eWq[e]);
+                    for (int j = 0; j < 8; j++)
+                        x[j] = e + j * F < end ? s.stage[(size_t)(myOff + e + j * F - r0) * Wc4 + t] : 0u;
+                    vadd8(c, x);
                 }
             }
+            for (; e + 3 * F < end; e += 4 * F) {
+                u32 x[4], wt[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    x[j] = s.stage[(size_t)(myOff + e + j * F - r0) * Wc4 + t];
+                    wt[j] = eWq[e + j * F];
+                }
+#pragma unroll
+                for (int j = 0; j < 4; j++) vadd(c, x[j], wt[j]);
+            }
+            for (; e < end; e += F) vadd(c, s.stage[(size_t)(myOff + e - r0) * Wc4 + t], eWq[e]);
+        };
+        // each round in two halves: the first half is added while the second is in flight
+        for (u32 r0 = 0; r0 < total; r0 += per) {
+            const u32 r1 = min(total, r0 + per), rm = r0 + (r1 - r0 + 1) / 2;
+            copy_range(r0, r0, rm);
+            cp_async_commit();
+            copy_range(r0, rm, r1);
+            cp_async_commit();
+            cp_async_wait_group<1>();
+            __syncthreads();
+            joinx::prof_mark(joinx::PROF_SC_COPY);
+            add_range(r0, r0, rm);
+            cp_async_wait_group<0>();
+            __syncthreads();
+            add_range(r0, rm, r1);
             __syncthreads();  // the next round overwrites the stage
             joinx::prof_mark(joinx::PROF_SC_ACC);
         }
     }
 
+    // Sums the F groups' counters of word t (groups of TG threads, planes
+    // area P) into P[t] by a tree of ceil(log2 F) rounds; F need not be a
+    // power of two.  Block-wide barriers: every set of a CTA calls it with
+    // the same F.
+    __device__ static void reduce_groups(u32 (&c)[kPlanes], u32* P, u32 g, u32 t, u32 TG, u32 F, bool live) {
+        for (u32 Fl = F; Fl > 1;) {
+            const u32 h = (Fl + 1) / 2;
+            if (live && g >= h && g < Fl) {
+#pragma unroll
+                for (int i = 0; i < kPlanes; i++) P[((g - h) * TG + t) * kPlanes + i] = c[i];
+            }
+            __syncthreads();
+            if (live && g < Fl - h) vsum(c, P + (g * TG + t) * kPlanes);
+            __syncthreads();
+            Fl = h;
+        }
+        if (live && g == 0) {
+#pragma unroll
+            for (int i = 0; i < kPlanes; i++) P[t * kPlanes + i] = c[i];
+        }
+        __syncthreads();
+    }
+
     __device__ static void score_pass(const Args& m, Smem& s, u32 buf, const joinx::Range& rg, u32 base, u32 cap,
                                       int nE, u32* ordOut) {
         const u32 T = cap / 32;
-        const u32 TG = T <= 32 ? 32 : (T <= 64 ? 64 : 128);
-        const u32 F = kThreads / TG;
-        const u32 g = threadIdx.x / TG, t = threadIdx.x % TG;
         const u32 Wd = rg.Sp / 32;
         const u32 Wc = min(T, (rg.hi - base + 31u) / 32u);
+        // groups of exactly Wc threads (one per word), as many as fit, at most 16
+        const u32 TG = Wc, F = min(kThreads / TG, 16u);
+        const u32 g = threadIdx.x / TG, t = threadIdx.x % TG;
         u32 c[kPlanes];
 #pragma unroll
         for (int i = 0; i < kPlanes; i++) c[i] = 0u;
-        __shared__ int s_nE1;
+        __shared__ int s_nE1;  // read by thread 0 before staged_counts' first barrier, by all after it
         if (threadIdx.x == 0) s_nE1 = nE;
-        __syncthreads();
         staged_counts(m, s, bitsOf(m, buf), Wd, base / 32, Wc, 1, s.eSC, s.eW, 0, 0, &s_nE1, kThreads, TG, F, c);
-        // tree-reduce the F groups' bit-sliced counters
-        for (u32 h = F / 2; h >= 1; h /= 2) {
-            if (g >= h && g < 2 * h) {
-#pragma unroll
-                for (int i = 0; i < kPlanes; i++) s.planes[((g - h) * TG + t) * kPlanes + i] = c[i];
-            }
-            __syncthreads();
-            if (g < h) vsum(c, s.planes + (g * TG + t) * kPlanes);
-            __syncthreads();
-        }
-        if (g == 0) {
-#pragma unroll
-            for (int i = 0; i < kPlanes; i++) s.planes[t * kPlanes + i] = c[i];
-        }
-        __syncthreads();
+        reduce_groups(c, s.planes, g, t, TG, F, g < F);
         for (u32 x = threadIdx.x; x < cap && base + x < rg.hi; x += kThreads) {
             const u32 cnt = vget(s.planes + (x >> 5) * kPlanes, x & 31);
             ordOut[x] = ord_f16((u16)half_bits_of_int(cnt));
@@ -948,30 +979,17 @@ struct IndelBits {
                 cp_async_wait_all();
                 __syncthreads();
             }
-            // TG threads per group (a power of two >= Wc) and F <= 16 groups
-            // sharing a word's entries (group 0 sums the others' counters)
-            u32 TG = 32;
-            while (TG < Wc) TG *= 2;
-            const u32 F = min(setSize / TG, 16u);
+            // groups of exactly Wc threads (one per word), at most 16 per set
+            const u32 TG = Wc, F = min(setSize / TG, 16u);
             const u32 g = ts / TG, t = ts % TG;
             u32 c[kPlanes];
 #pragma unroll
             for (int i = 0; i < kPlanes; i++) c[i] = 0u;
             staged_counts(m, s, B, Wd, base / 32, Wc, nq, s.bSC, s.bW, m.ncol, ncolW(m.ncol), nEout, setSize, TG, F,
                           c);
-            // sum the F groups' counters of (q, t) into group 0's smem entry
-            u32* P = s.planes + (size_t)q * setSize * kPlanes;
-            if (q < nq && g < F && g > 0 && t < Wc) {
-#pragma unroll
-                for (int i = 0; i < kPlanes; i++) P[(g * TG + t) * kPlanes + i] = c[i];
-            }
-            __syncthreads();
-            if (q < nq && g == 0 && t < Wc) {
-                for (u32 gg = 1; gg < F; gg++) vsum(c, P + (gg * TG + t) * kPlanes);
-#pragma unroll
-                for (int i = 0; i < kPlanes; i++) P[t * kPlanes + i] = c[i];
-            }
-            __syncthreads();
+            // sum the F groups' counters of (q, t) into group 0's entry
+            u32* P = s.planes + (size_t)(q < nqP ? q : 0) * setSize * kPlanes;
+            reduce_groups(c, P, g, t, TG, F, q < nq && g < F);
             // best key of query q over this pass's live slots
             u64 bk = 0ull;
             if (q < nq) {
@@ -1204,7 +1222,7 @@ static int launch_indel(const IndelBuffers& L, u32 ntip, u32 ncol, u32 nState, c
     InitArgs ia{ntip, ncol, Sp, L.colT0, L.eSC, L.eW, L.eLen, L.chunkStart, nChunks, nTiles, L.tileCounter, L.initKey};
     int perSM = 0;
     if (useBits) {
-        InitBitsArgs ib{ntip, ncol, nState, Sp / 32, L.bits0, L.eSC, L.eW, L.eLen, L.chunkStart, nChunks, nTiles,
+        InitBitsArgs ib{ntip, ncol, nState, Sp / 32, unitW ? 1 : 0, L.bits0, L.eSC, L.eW, L.eLen, L.chunkStart, nChunks, nTiles,
                         L.tileCounter, L.initKey};
         CASPHY_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_init_bits, kThreads, 0));
         k_init_bits<<<nSM * std::max(perSM, 1), kThreads, 0, st>>>(ib);
