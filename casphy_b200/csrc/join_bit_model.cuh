@@ -148,8 +148,8 @@ struct BitModel {
         u32* mseq;
         u32* mbis;
     };
-    __host__ __device__ static size_t engine_smem_bytes(u32 nCTA, u32 Rmax, u32 deathWords = 0) {
-        return joinx::engine_smem(nCTA, Rmax, deathWords);
+    __host__ __device__ static size_t engine_smem_bytes(u32 nCTA, u32 Rmax, u32 deathWords = 0, u32 pre = 0) {
+        return joinx::engine_smem(nCTA, Rmax, deathWords, pre);
     }
     __host__ static size_t model_smem_bytes(const Args& m) {
         const size_t ne = (size_t)m.nbin * (m.nplanes ? m.nplanes : 1);

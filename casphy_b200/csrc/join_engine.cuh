@@ -72,6 +72,8 @@ struct Common {
     u32 bytesPerPairSite; // algorithmic bytes per (candidate, query entry), x1000
     u32 maxBatch;         // stale rows per rescan phase, 1..kMaxBatch
     u32 deathWords;       // words of the per-CTA shared-memory bitmap of joined nodes (0: none)
+    u32 needSizes;        // the model's join reads the two node sizes (minSize > 0)
+    u32 preSlots;         // a join's scan prefetches its slots' node, maximum and partner into shared memory
     unsigned long long* prof;  // nullable: CTA 0 section times (ns), see PROF_*
 };
 
@@ -441,11 +443,14 @@ template <class M>
 __device__ __forceinline__ void join_run(const Common& a, const typename M::Args& m, u32 b, unsigned char* smem) {
     u32* ordOut = reinterpret_cast<u32*>(smem);                        // kMaxCap
     u32* deathBits = ordOut + kMaxCap;                                 // joined nodes (deathWords)
-    BlockRec* tabRec = reinterpret_cast<BlockRec*>(deathBits + death_words_padded(a.deathWords));  // 2*nCTA
+    u32* preSn = deathBits + death_words_padded(a.deathWords);         // 3 x Rmax when a.preSlots
+    u32* preLo = preSn + a.Rmax;
+    u32* preLi = preLo + a.Rmax;
+    BlockRec* tabRec = reinterpret_cast<BlockRec*>(preSn + (a.preSlots ? 3 * a.Rmax : 0u));  // 2*nCTA
     u32* ranks = reinterpret_cast<u32*>(tabRec + 2 * a.nCTA);          // Rmax
     unsigned char* tabCnt = reinterpret_cast<unsigned char*>(ranks + a.Rmax);
     unsigned char* tabExact = tabCnt + a.nCTA;
-    unsigned char* msm = smem + M::engine_smem_bytes(a.nCTA, a.Rmax, a.deathWords);  // model shared memory
+    unsigned char* msm = smem + M::engine_smem_bytes(a.nCTA, a.Rmax, a.deathWords, a.preSlots);  // model part
     typename M::Smem ms;
     M::carve_smem(m, msm, ms);
     __shared__ u64 red[32];
@@ -496,16 +501,28 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
         const BlockRec g = s_best;
         const u32 j1 = key_node(g.key), c1 = g.slot, j2 = g.partner;
         if (c1 >= rg.S || j1 >= a.nnode || j2 >= a.nnode) { fail = CASPHY_EINTERNAL; break; }
-        if (threadIdx.x == 0) {
-            s_val[0] = ld_cg_u32(a.nodeDeath + j2);
-            s_val[1] = ld_cg_u32(a.node2slot + j2);
-            s_val[2] = ld_cg_u32(a.nodeSize + j1);
-            s_val[3] = ld_cg_u32(a.nodeSize + j2);
+        // With the joined-node bitmap and no size rule, the decision needs no
+        // load: the partner's slot is loaded by thread 0 and first used after
+        // the query build, which hides its latency.
+        const bool quick = a.deathWords && !a.needSizes;
+        bool stale;
+        u32 c2 = 0, s1 = 0, s2 = 0, c2pending = 0;
+        if (quick) {
+            stale = (deathBits[j2 >> 5] >> (j2 & 31)) & 1u;
+            if (!stale && threadIdx.x == 0) c2pending = ld_cg_u32(a.node2slot + j2);
+        } else {
+            if (threadIdx.x == 0) {
+                s_val[0] = ld_cg_u32(a.nodeDeath + j2);
+                s_val[1] = ld_cg_u32(a.node2slot + j2);
+                s_val[2] = ld_cg_u32(a.nodeSize + j1);
+                s_val[3] = ld_cg_u32(a.nodeSize + j2);
+            }
+            __syncthreads();
+            const u32 death = s_val[0];
+            c2 = s_val[1]; s1 = s_val[2]; s2 = s_val[3];
+            __syncthreads();
+            stale = death < k || c2 >= rg.S;
         }
-        __syncthreads();
-        const u32 death = s_val[0], c2 = s_val[1], s1 = s_val[2], s2 = s_val[3];
-        __syncthreads();
-        const bool stale = death < k || c2 >= rg.S;
         pf.mark(PROF_DECIDE);
         if (stale) {
             // rescan a batch of stale rows (the best record first) against every live slot
@@ -622,6 +639,14 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
         // join j1 and j2 into node ntip+k
         const u32 newNode = a.ntip + k;
         const int nE = M::build_join(m, ms, j1, j2, s1, s2, wcount);
+        if (quick) {
+            if (threadIdx.x == 0) s_val[1] = c2pending;
+            __syncthreads();
+            c2 = s_val[1];
+            if (c2 >= rg.S) fail = CASPHY_EINTERNAL;  // a live node always has a slot
+            __syncthreads();
+            if (fail) break;
+        }
         pf.mark(PROF_BUILD);
         if (b == 0) {
             M::store_node(m, ms, newNode);
@@ -656,14 +681,27 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
             u32* lop = lmOrd_of(a, buf);
             u32* lip = lmIdx_of(a, buf);
             const u32 cap = M::pass_cap(m, rg.hi - rg.lo);
+            // one pass over the range: its slots' node, maximum and partner are
+            // copied into shared memory in the scan's first load round (the
+            // model waits for every copy of this thread before it returns)
+            const bool pre = a.preSlots && cap >= rg.hi - rg.lo;
+            if (pre && rg.lo < rg.hi) {
+                const u32 n4 = (rg.hi - rg.lo + 3u) / 4u;
+                for (u32 i = threadIdx.x; i < 3 * n4; i += kThreads) {
+                    const u32 arr = i / n4, j = 4 * (i % n4);
+                    const u32* src = arr == 0 ? sn : (arr == 1 ? lop : lip);
+                    cp_async16(preSn + arr * a.Rmax + j, src + rg.lo + j);
+                }
+            }
             for (u32 base = rg.lo; base < rg.hi; base += cap) {
                 M::score_pass(m, ms, buf, rg, base, cap, nE, ordOut);
                 for (u32 x = threadIdx.x; x < cap && base + x < rg.hi; x += kThreads) {
                     const u32 c = base + x;
-                    const u32 node = ld_cg_u32(sn + c);
-                    u32 lo = ld_cg_u32(lop + c);
-                    u32 li = ld_cg_u32(lip + c);
-                    if (node == kDead || c == c1) continue;
+                    const u32 node = pre ? preSn[x] : ld_cg_u32(sn + c);
+                    u32 lo = pre ? preLo[x] : ld_cg_u32(lop + c);
+                    u32 li = pre ? preLi[x] : ld_cg_u32(lip + c);
+                    // c1 and c2 changed this phase (the copies may predate the changes)
+                    if (node == kDead || c == c1 || c == c2) continue;
                     const u32 o = ordOut[x];
                     if (o > lo) {  // strict improvement
                         lo = o;
@@ -774,9 +812,10 @@ inline u32 stale_batch_setting() {
 }
 
 // Host: bytes of engine shared memory before the model's part.
-__host__ __device__ inline size_t engine_smem(u32 nCTA, u32 Rmax, u32 deathWords = 0) {
-    size_t s = sizeof(u32) * kMaxCap + sizeof(u32) * death_words_padded(deathWords) + sizeof(BlockRec) * 2 * nCTA +
-               sizeof(u32) * Rmax + 2 * nCTA;
+__host__ __device__ inline size_t engine_smem(u32 nCTA, u32 Rmax, u32 deathWords = 0, u32 preSlots = 0) {
+    size_t s = sizeof(u32) * kMaxCap + sizeof(u32) * death_words_padded(deathWords) +
+               (preSlots ? sizeof(u32) * 3 * (size_t)Rmax : 0) + sizeof(BlockRec) * 2 * nCTA + sizeof(u32) * Rmax +
+               2 * nCTA;
     return (s + 15) & ~size_t(15);
 }
 

@@ -364,8 +364,8 @@ struct IndelDense {
         u16* eW;
         u16* mrow;
     };
-    __host__ __device__ static size_t engine_smem_bytes(u32 nCTA, u32 Rmax, u32 deathWords = 0) {
-        return joinx::engine_smem(nCTA, Rmax, deathWords);
+    __host__ __device__ static size_t engine_smem_bytes(u32 nCTA, u32 Rmax, u32 deathWords = 0, u32 pre = 0) {
+        return joinx::engine_smem(nCTA, Rmax, deathWords, pre);
     }
     __host__ static size_t model_smem_bytes(const Args& m) {
         return sizeof(u16) * kCap + sizeof(u32) * m.ncol + sizeof(u16) * (((m.ncol + 7u) & ~7u) + m.ncolP) + 16;
@@ -401,7 +401,7 @@ struct IndelDense {
     // INT: the query entries are split over F thread groups that share the
     // candidates (F as large as the CTA's slot range allows); HALF: one group,
     // because binary16 sums must be formed in ascending site order.
-    __device__ static u32 pass_cap(const Args&, u32 R) {
+    __host__ __device__ static u32 pass_cap(const Args&, u32 R) {
         u32 F = 1;
         if (INTP) {
             while (F < 16 && (u32)(kCap / (F * 2)) >= R) F *= 2;
@@ -666,8 +666,8 @@ struct IndelBits {
         u32* bwc;     // kMaxBatch x 33: per-query warp counts of the fused build
         u32* stage;   // kStageWords: bitset words copied for the current round
     };
-    __host__ __device__ static size_t engine_smem_bytes(u32 nCTA, u32 Rmax, u32 deathWords = 0) {
-        return joinx::engine_smem(nCTA, Rmax, deathWords);
+    __host__ __device__ static size_t engine_smem_bytes(u32 nCTA, u32 Rmax, u32 deathWords = 0, u32 pre = 0) {
+        return joinx::engine_smem(nCTA, Rmax, deathWords, pre);
     }
     __host__ __device__ static u32 ncolW(u32 ncol) { return (ncol + 7u) & ~7u; }
     __host__ static size_t model_smem_bytes(const Args& m) {
@@ -721,7 +721,10 @@ struct IndelBits {
             if (n > 1) atomicOr(B + ((size_t)i * m.nState + n - 2) * Wd + word, bit);
         }
     }
-    __device__ static u32 pass_cap(const Args&, u32 R) { return min(4096u, (R + 31u) & ~31u); }
+    __host__ __device__ static u32 pass_cap(const Args&, u32 R) {
+        const u32 r = (R + 31u) & ~31u;
+        return r < 4096u ? r : 4096u;
+    }
 
     // Bit-sliced counts of nq queries over the bitset words [w0, w0 + Wc) of
     // this CTA.  Query q's entries are lists eSC/eW + q * stride (nE[q] of
@@ -808,6 +811,10 @@ struct IndelBits {
             __syncthreads();  // the next round overwrites the stage
             joinx::prof_mark(joinx::PROF_SC_ACC);
         }
+        // copies the caller issued before (slot prefetch) are complete even
+        // when there was no entry to stage; the caller's next barrier
+        // publishes them
+        cp_async_wait_all();
     }
 
     // Sums the F groups' counters of word t (groups of TG threads, planes
@@ -1173,10 +1180,24 @@ static int launch_join_fitted(joinx::Common& c, typename M::Args& m, u32* batch,
     CASPHY_CUDA_TRY(cudaGetDevice(&dev));
     CASPHY_CUDA_TRY(cudaDeviceGetAttribute(&smemMax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     const size_t lim = (size_t)smemMax - 4096;  // the kernel's static shared memory
-    auto need = [&] { return M::engine_smem_bytes(nCTA, c.Rmax, c.deathWords) + M::model_smem_bytes(m); };
+    auto need = [&] {
+        return M::engine_smem_bytes(nCTA, c.Rmax, c.deathWords, c.preSlots) + M::model_smem_bytes(m);
+    };
+    // shared memory goes first to the joined-node bitmap, then to slot
+    // prefetch (models that stage their scan, one pass per range), then to
+    // stale batches beyond 4 rows, then to the rest of the batches
+    c.preSlots = M::kFusedStale && c.Rmax <= M::pass_cap(m, c.Rmax) ? 1u : 0u;
+    const u32 want = batch ? *batch : 1u;
     if (batch) {
+        while (*batch > 4 && need() > lim) (*batch)--;
+        if (need() > lim) {
+            c.preSlots = 0;
+            *batch = want;
+        }
         while (*batch > 1 && need() > lim) (*batch)--;
         c.maxBatch = *batch;
+    } else if (need() > lim) {
+        c.preSlots = 0;
     }
     if (need() > lim) c.deathWords = 0;
     const size_t smem = need();
@@ -1252,6 +1273,7 @@ static int launch_indel(const IndelBuffers& L, u32 ntip, u32 ncol, u32 nState, c
     c.ordNeg1 = ORD_F16_NEG1; c.compactMin = 4096; c.compactQ8 = 192; c.bytesPerPairSite = 2000;
     c.maxBatch = joinx::stale_batch_setting();
     c.deathWords = (nnode + 31) / 32;  // 50 KB at 200k cells
+    c.needSizes = minSize > 0;         // the minSize / minRatio rule reads node sizes
     if (useBits) {
         using M = IndelBits;
         c.align = kBitsAlign;
