@@ -41,6 +41,8 @@ WORKLOAD = dict(ncell=200_000, nsite=1024, depth=20, p_edit=0.02, nallele=256, z
                 p_missing=0.15, seed=5)
 CPU_SAMPLE_CELLS = 5000      # oracle port (multi-threaded restatement of cu/joinEdgeIndel.cu)
 TWIN_SAMPLE_CELLS = 1024     # the reference's own CPU join (greedyJoinEdge2), a few seconds a tree
+RADIUS_SPARSE = 150          # C2 radius with sparse lists (3.3 neighbours per row); shared >= 4 lists every pair
+DTYPE = "fp16-exact integer counts"  # integer sums that equal the reference's binary16 sums (unit weights)
 
 
 def workload_name():
@@ -230,7 +232,7 @@ def run_reference(args, world, rank):
               f"({pairs:.0f} pair-scores, {tot / args.steps:.2f} s a tree; {what}; {cores} thread(s))")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot / args.steps * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": DTYPE, "data": "synthetic",
             "config": {"workload": workload_name(), "cells_per_step": ncell},
             "impl": "reference",
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
@@ -289,7 +291,10 @@ def blopt_suite(L):
     edge = np.stack([par, ch], 1).astype(np.uint32)
     t0 = np.full(len(t_true), 0.01)
     L.felsenstein_optimize(edge, t0, codes, kappa=4.0, pi=pi, rel_tol=1e-9, max_iter=3)  # warm-up
-    _, full = L.felsenstein_optimize(edge, t0, codes, kappa=4.0, pi=pi, rel_tol=1e-9, max_iter=1000)
+    t_end, full = L.felsenstein_optimize(edge, t0, codes, kappa=4.0, pi=pi, rel_tol=1e-9, max_iter=1000)
+    # the GPU's log L at its final branch lengths against FP64 pruning of the same tree
+    import oracle as O
+    ll64 = O.loglik_hky85(edge, t_end, codes, 4.0, pi)
     s_states, (sp, sc, st) = synth.hky85_alignment(128, 2000, 4.0, pi, 0.01, 0.02, seed=14)
     s_codes = synth.dna_nibbles(s_states)
     s_edge = np.stack([sp, sc], 1).astype(np.uint32)
@@ -314,6 +319,8 @@ def blopt_suite(L):
             "eval_graph_s": full["eval_seconds"],
             "ms_per_evaluation": full["seconds"] * 1e3 / max(full["evaluations"], 1),
             "loglik_start": full["loglik_start"], "loglik_end": full["loglik_end"],
+            "loglik_fp64_at_end": ll64, "loglik_rel_err_vs_fp64": abs(full["loglik_end"] - ll64) / abs(ll64),
+            "fp64_oracle": "oracle_loglik_hky85 (Felsenstein pruning in double precision) at the final lengths",
             "fd_evaluations_per_gradient": 2 * len(t0),
             "roofline": {"kernels": "k_inside_hky + k_outside_hky (evaluation graph)", "bound": "hbm",
                          "alg_bytes_per_evaluation": alg, "achieved": achieved, "peak": hbm, "unit": "GB/s",
@@ -384,6 +391,16 @@ def rows_suite(L, nthreads):
     bmat = np.ascontiguousarray(words.T)
     wr = np.ones(512)
     (cnt, idx), t_rad = _timed(lambda: L.radius_bit(bmat, wr, 4))
+    (cnt_s, idx_s), t_rad_s = _timed(lambda: L.radius_bit(bmat, wr, RADIUS_SPARSE), reps=3)
+    t0 = time.perf_counter()
+    oc_full, oi_full = O.radius_bit(bmat, wr, 4, nthreads)
+    t_cr_full = time.perf_counter() - t0
+    rad_full_same = bool(np.array_equal(cnt, oc_full) and np.array_equal(idx, oi_full))
+    del oc_full, oi_full
+    t0 = time.perf_counter()
+    oc_s, oi_s = O.radius_bit(bmat, wr, RADIUS_SPARSE, nthreads)
+    t_cr_s = time.perf_counter() - t0
+    rad_sparse_same = bool(np.array_equal(cnt_s, oc_s) and np.array_equal(idx_s, oi_s))
     truth = synth.lineage_clades(10_000, 16, seed=23)
     est = B.clade_bits(bedge, 10_000, (10_000 + 31) // 32)
     (ymin, ysize, xmin, xsize), t_td = _timed(lambda: L.transfer_dis(truth, est, 10_000))
@@ -402,8 +419,13 @@ def rows_suite(L, nthreads):
         "joinEdgeBitReverse": {"gpu_s": t_join, "device_ms": bst["total_ms"], "pairs": bst["pair_scores"],
                                "cpu_sample": f"first {sub} cells", "cpu_s_sample": t_cj},
         "radiusNeighbor_r4": {"gpu_s": t_rad, "pairs": 10_000 * 10_000, "neighbours": int(cnt.sum()),
+                              "note": "shared >= 4 lists every pair: a 400 MB list expansion and copy",
                               "cpu_sample": f"first {sub} cells", "cpu_s_sample": t_cr,
-                              "sample_identical": None},
+                              "sample_identical": None, "identical": rad_full_same,
+                              "cpu_full_s": t_cr_full},
+        f"radiusNeighbor_r{RADIUS_SPARSE}": {"gpu_s": t_rad_s, "pairs": 10_000 * 10_000,
+                                             "neighbours": int(cnt_s.sum()), "cpu_full_s": t_cr_s,
+                                             "identical": rad_sparse_same},
         "TransferDisStream_vs_true_tree": {"gpu_s": t_td, "rows_y": int(truth.shape[0]), "rows_x": int(est.shape[0]),
                                            "words": int(truth.shape[1]),
                                            "mean_normalised_distance": float(np.mean(ymin / np.maximum(ysize, 1))),
@@ -469,12 +491,17 @@ def rows_suite(L, nthreads):
     oc, oi = O.radius_dna(raw[:sub], lvalid - 20, nthreads)
     t_cd = time.perf_counter() - t0
     gc, gi = L.radius_dna(raw[:sub], lvalid - 20)
+    t0 = time.perf_counter()
+    ocf, oif = O.radius_dna(raw, lvalid - 20, nthreads)
+    t_cdf = time.perf_counter() - t0
+    dna_full_same = bool(np.array_equal(dc, ocf) and np.array_equal(di, oif))
     res["C3_radiusNeighborDNA"] = {
         "workload": f"HKY85 20000 x 2000 (kappa 4, pi .3/.2/.2/.3, Exp(0.01) Yule), 2% gaps, fasta2bin coding, "
                     f"{lvalid} variable columns; shared >= L_valid - 20",
         "gpu_s": t_dna, "pairs": 20_000 * 20_000, "neighbours": int(dc.sum()),
         "cpu_sample": f"first {sub} sequences", "cpu_s_sample": t_cd, "cpu_cores": nthreads,
-        "sample_identical": bool(np.array_equal(gc, oc) and np.array_equal(gi, oi))}
+        "sample_identical": bool(np.array_equal(gc, oc) and np.array_equal(gi, oi)),
+        "identical": dna_full_same, "cpu_full_s": t_cdf}
     if twin:
         t0 = time.perf_counter()
         tc, _ = T.radius_weighted_dna_rows(raw[:sub], lvalid - 20, 0, sub, nthreads)
@@ -521,6 +548,131 @@ def rows_suite(L, nthreads):
     return res
 
 
+def reference_gpu_rows(budget_s=240.0):
+    """The reference's own GPU tools (built from cu/*.cu for sm_100a into
+    oracle/_ref/ by oracle/Makefile) against the drop-in executables on the
+    same input files: process wall clock of each, one run each after one
+    untimed run of both (CUDA start-up is inside both), output files compared
+    byte for byte.  A reference run that exceeds its time limit is reported as
+    such; the rows stop when the whole budget is spent."""
+    import tempfile
+    from casphy_b200 import bootstrap as B
+    from casphy_b200 import formats, synth
+    ref_bin = os.path.join(ROOT, "oracle", "_ref")
+    our_bin = os.path.join(ROOT, "casphy_b200", "bin")
+    if not os.path.isdir(ref_bin):
+        return {"unavailable": "oracle/_ref was not built (needs the CasPhy source tree at build time)"}
+    t_start = time.perf_counter()
+    rows = {}
+
+    def run(exe, args, cwd, timeout):
+        t0 = time.perf_counter()
+        try:
+            r = subprocess.run([exe] + args, cwd=cwd, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
+                               timeout=timeout)
+            return time.perf_counter() - t0, r.returncode
+        except subprocess.TimeoutExpired:
+            return None, "timeout"
+
+    def row(name, ref_exe, our_exe, args, outputs, setup, timeout=120.0, reps=1):
+        left = budget_s - (time.perf_counter() - t_start)
+        if left < 10:
+            rows[name] = {"skipped": "bench budget for these rows spent"}
+            return
+        with tempfile.TemporaryDirectory() as d:
+            desc = setup(d)
+            res = {"workload": desc}
+            got = {}
+            for who, exe in (("reference", os.path.join(ref_bin, ref_exe)), ("casphy", os.path.join(our_bin, our_exe))):
+                if not os.path.exists(exe):
+                    res[who + "_s"] = None
+                    continue
+                run(exe, args, d, min(timeout, left))  # untimed first run
+                times = []
+                for _ in range(reps):
+                    dt, rc = run(exe, args, d, min(timeout, left))
+                    if dt is None or rc != 0:
+                        times = None
+                        res[who + "_error"] = rc
+                        break
+                    times.append(dt)
+                res[who + "_s"] = min(times) if times else None
+                got[who] = {o: open(os.path.join(d, o), "rb").read() for o in outputs
+                            if os.path.exists(os.path.join(d, o))}
+                for o in outputs:
+                    if os.path.exists(os.path.join(d, o)):
+                        os.remove(os.path.join(d, o))
+            if res.get("reference_s") and res.get("casphy_s"):
+                res["speedup"] = res["reference_s"] / res["casphy_s"]
+            if "reference" in got and "casphy" in got:
+                res["identical_files"] = bool(got["reference"] == got["casphy"] and
+                                              len(got["casphy"]) == len(outputs))
+            rows[name] = res
+
+    # C1: joinEdgeIndel, 1,024 cells x 256 sites (the reference binary with MAXCOL 1000)
+    def c1(d):
+        raw = synth.lineage_states(1024, 256, 12, 0.04, 64, 1.5, 0.10, seed=21)
+        codes, ns = synth.regularize(raw)
+        formats.write_mat(os.path.join(d, "c1.tbmat"), codes)
+        formats.write_mat(os.path.join(d, "c1.tipSize"), np.ones((1024, 1), np.uint32))
+        formats.write_f64(os.path.join(d, "c1.w"), np.ones((ns, 256)))
+        c1.ns = ns
+        return "joinEdgeIndel, indel 1024 cells x 256 sites (C1), unit weights"
+    raw1 = synth.lineage_states(1024, 256, 12, 0.04, 64, 1.5, 0.10, seed=21)
+    ns1 = synth.regularize(raw1)[1]
+    row("C1_joinEdgeIndel", "joinEdgeIndel", "joinEdgeIndel", ["c1", "c1.w", str(ns1), "0", "2"],
+        ["c1.edge2", "c1.nodeState2"], c1)
+
+    # C5 prefix: joinEdgeIndel at 1,024 sites (the reference built with MAXCOL 1024)
+    codes5, ns5, _ = gen_workload(5000)
+
+    def c5(d):
+        formats.write_mat(os.path.join(d, "c5.tbmat"), codes5)
+        formats.write_mat(os.path.join(d, "c5.tipSize"), np.ones((codes5.shape[0], 1), np.uint32))
+        formats.write_f64(os.path.join(d, "c5.w"), np.ones((ns5, codes5.shape[1])))
+        return "joinEdgeIndel, first 5000 cells of the 200000 x 1024 indel workload (C5 prefix), unit weights"
+    row("C5_prefix5k_joinEdgeIndel", "joinEdgeIndel_MAXCOL1024", "joinEdgeIndel",
+        ["c5", "c5.w", str(ns5), "0", "2"], ["c5.edge2", "c5.nodeState2"], c5, timeout=180.0)
+
+    # C2: joinEdgeBitReverse, radiusNeighbor (shared >= 4 and a sparse radius), TransferDisStream
+    words = synth.binary_workload(10_000, 512, 16, 0.03, 0.05, seed=23)
+
+    def c2(d):
+        formats.write_mat(os.path.join(d, "c2.tbmat"), words)
+        formats.write_f64(os.path.join(d, "c2.w"), np.ones(512))
+        formats.write_mat(os.path.join(d, "c2.bmat"), words.T)
+        return "base-editor 10000 cells x 512 sites (C2)"
+    row("C2_joinEdgeBitReverse_type1", "joinEdgeBitReverse", "joinEdgeBitReverse", ["c2", "c2.w", "1"],
+        ["c2.edge2", "c2.nodeState2"], c2, timeout=180.0)
+    for r in (4, RADIUS_SPARSE):
+        row(f"C2_radiusNeighbor_r{r}", "radiusNeighbor", "radiusNeighbor", ["c2", str(r)],
+            ["c2.idx", "c2.nNeighbor"], c2, timeout=180.0)
+    edge, _, _ = __import__("casphy_b200.lib", fromlist=["x"]).join_bit(words, None, 1)
+    truth = synth.lineage_clades(10_000, 16, seed=23)
+    est = B.clade_bits(edge, 10_000, (10_000 + 31) // 32)
+
+    def td(d):
+        formats.write_mat(os.path.join(d, "td_y"), truth)
+        formats.write_mat(os.path.join(d, "td_x"), est)
+        return "TransferDisStream, true tree's 9998 clades against the C2 join tree's (313 words), 1 GPU"
+    row("C2_TransferDisStream", "TransferDisStream", "TransferDisStream", ["td_y", "td_x", "td", "10000"],
+        ["td_ymin.bin", "td_xmin.bin"], td, timeout=180.0)
+
+    # C3: radiusNeighborDNA at Hamming 20 on the fasta2bin matrix
+    states, _ = synth.hky85_alignment(20_000, 2000, 4.0, [0.3, 0.2, 0.2, 0.3], 0.01, 0.02, seed=13)
+    raw3, var = synth.dna_to_fasta2bin(states)
+    lv = int(var.sum())
+
+    def c3(d):
+        formats.write_mat(os.path.join(d, "c3.tbmat"), raw3)
+        return f"radiusNeighborDNA, HKY85 20000 x 2000 via fasta2bin coding, shared >= {lv} - 20 (C3)"
+    row("C3_radiusNeighborDNA", "radiusNeighborDNA", "radiusNeighborDNA", ["c3", str(lv - 20)],
+        ["c3.idx", "c3.nNeighbor"], c3, timeout=180.0)
+    rows["timing"] = ("process wall clock (CUDA start-up, file reads and writes included for both), best of one "
+                      "run after one untimed run of each")
+    return rows
+
+
 def blopt_c5(L, codes, nstate, edge):
     """Irreversible edit-model branch lengths on the 200,000-cell join tree, and
     the reference's parsimony change counts (charAncestralEC) on the same tree."""
@@ -534,18 +686,24 @@ def blopt_c5(L, codes, nstate, edge):
     par = {"gpu_s": t_par, "cpu_s": t_cpar, "edges": int(len(plen)), "total_changes": int(plen.sum()),
            "identical": bool(np.array_equal(plen, olen))}
     t0 = np.full(len(e), 0.05)
-    _, st = L.felsenstein_optimize(e, t0, codes, model="irreversible", rate=1.0, nallele=int(nstate),
-                                   rel_tol=1e-9, max_iter=1000)
+    t_end, st = L.felsenstein_optimize(e, t0, codes, model="irreversible", rate=1.0, nallele=int(nstate),
+                                       rel_tol=1e-9, max_iter=1000)
+    # FP64 pruning of the same tree at the final lengths (compact form of the
+    # edit model), allele frequencies as the library takes them by default
+    q = O.tip_allele_freqs(codes, int(nstate))
+    ll64 = O.loglik_irreversible(e, t_end, codes, int(nstate), q, 1.0)
     # the same optimisation started from the parsimony counts
     from casphy_b200.branch_lengths import parsimony_start
     tw = parsimony_start(e, pstate, plen, raw.shape[0], rate=1.0)
     del pstate
-    _, sw = L.felsenstein_optimize(e, tw, codes, model="irreversible", rate=1.0, nallele=int(nstate),
-                                   rel_tol=1e-9, max_iter=1000)
+    tw_end, sw = L.felsenstein_optimize(e, tw, codes, model="irreversible", rate=1.0, nallele=int(nstate),
+                                        rel_tol=1e-9, max_iter=1000)
+    llw64 = O.loglik_irreversible(e, tw_end, codes, int(nstate), q, 1.0)
     par["warm_start"] = {
         "start": "t = -log(1 - k/n0) per edge from the change counts k and the parent's unedited sites n0",
         "adjoint_s": sw["seconds"], "iterations": sw["iterations"], "evaluations": sw["evaluations"],
         "loglik_start": sw["loglik_start"], "loglik_end": sw["loglik_end"],
+        "loglik_fp64_at_end": llw64, "loglik_rel_err_vs_fp64": abs(sw["loglik_end"] - llw64) / abs(llw64),
         "loglik_end_rel_diff_to_flat_start": (sw["loglik_end"] - st["loglik_end"]) / abs(st["loglik_end"])}
     return {"workload": "irreversible edit model (rate 1, allele frequencies from the tips) on the 200000-cell "
                         "join tree of the headline workload, 1024 sites; start at t = 0.05",
@@ -553,6 +711,9 @@ def blopt_c5(L, codes, nstate, edge):
             "eval_graph_s": st["eval_seconds"],
             "ms_per_evaluation": st["seconds"] * 1e3 / max(st["evaluations"], 1),
             "loglik_start": st["loglik_start"], "loglik_end": st["loglik_end"],
+            "loglik_fp64_at_end": ll64, "loglik_rel_err_vs_fp64": abs(st["loglik_end"] - ll64) / abs(ll64),
+            "fp64_oracle": "oracle_loglik_irreversible (compact FP64 pruning) at the final lengths, allele "
+                           "frequencies from the tips' counts",
             "levels_inside": st["levels_inside"], "levels_outside": st["levels_outside"],
             "charAncestralEC": par}
 
@@ -629,8 +790,26 @@ def main():
         barrier(world)
     elapsed = ev0.elapsed_time(ev1) / 1e3
     elapsed = max_over_ranks(elapsed, world)
-    pairs = float(stats["pair_scores"])
+    # pair-scores of a tree counted as (N-1)^2, the count of the reference's
+    # CPU join (greedyJoinEdge2) that the reference arm reports, so that the
+    # two arms' values compare as tree times; the lazy loop's own count (the
+    # reference GPU loop's schedule, from the oracle) is reported beside it
+    pairs = float(ntip - 1) ** 2
     value = pairs * args.steps * world / elapsed
+    # the tree against the oracle's digest of the same workload
+    identical, digest_case = None, {None: "c5_200k", 50_000: "c5_50k", 20_000: "c5_20k"}.get(args.cells)
+    hashes = {}
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "scale_hashes.json")) as f:
+            hashes = json.load(f)
+    except OSError:
+        pass
+    if digest_case in hashes:
+        import hashlib
+        ref = hashes[digest_case]
+        sha = lambda a: hashlib.sha256(np.ascontiguousarray(a, dtype="<u4").tobytes()).hexdigest()  # noqa: E731
+        identical = bool(sha(edge[: 2 * (2 * ntip - 2)]) == ref["edge_sha256"] and
+                         sha(d_state.cpu().numpy().view(np.uint32)) == ref["state_sha256"])
 
     # end to end through the host-buffer entry point
     h_codes = torch.from_numpy(codes.view(np.int32)).pin_memory()
@@ -679,25 +858,42 @@ def main():
             "unit": "GB/s", "frac": achieved / hbm, "peak_source": f"{how} hbm_gbs",
             "traffic": traffic_from_profile("k_join"),
             "alg_bytes_per_launch": stats["alg_bytes_join"], "launch_ms": jl,
+            "alg_bytes_rule": "1/8 byte per (candidate, query site): one bitset bit",
+            "two_byte_rule": {"note": "2 bytes per (candidate, query site), the u16-code rule of the scope table",
+                              "achieved": achieved * 16, "frac": achieved * 16 / hbm},
             "init_scan": {"alg_bytes": stats["alg_bytes_init"], "ms": stats["init_scan_ms"],
                           "achieved_gbs": stats["alg_bytes_init"] / (stats["init_scan_ms"] / 1e3) / 1e9
                           if stats["init_scan_ms"] else None}}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": DTYPE, "data": "synthetic",
             "config": {"workload": workload_name() if args.cells is None else
                        f"first {ntip} cells of: " + workload_name(), "cells": ntip, "sites": ncol, "nState": int(nstate),
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs (800 MB codes) larger than the 126 MB L2; no flush between steps"},
             "tree_s": elapsed / args.steps,
-            "tree_stats": {k: stats[k] for k in ("joins", "stale_recomputes", "pair_scores", "compactions",
-                                                  "phases", "int_path")},
+            "pair_scores_counted": "(N-1)^2 per tree, as the reference's CPU join computes",
+            "identical": identical,
+            "identical_to": (f"sha256 of the oracle's edge list and node states for this workload "
+                             f"(tests/golden/scale_hashes.json {digest_case})" if identical is not None else None),
+            "tree_stats": dict({k: stats[k] for k in ("joins", "stale_recomputes", "pair_scores", "compactions",
+                                                      "phases", "refreshes", "int_path")},
+                               reference_loop_pair_scores=hashes.get(digest_case, {}).get("pair_scores"),
+                               reference_loop_stale_rescans=hashes.get(digest_case, {}).get("stale_recomputes")),
             "e2e": {"value": e2e_val, "unit": UNIT,
                     "h2d_bytes_per_step": int(codes.nbytes + wflat.nbytes + tip.nbytes),
                     "d2h_bytes_per_step": int(edge.nbytes + hstate_np.nbytes), "tree_s": e2e_s / e2e_steps},
             "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary()}
+    if cpu is not None and cpu.get("kind") == "reference":
+        # the headline as tree times: the reference CPU join's rate extrapolated
+        # to (N-1)^2 pair-scores (its N x N float cache needs 160 GB at 200k)
+        cpu_tree_s = pairs / cpu["value"]
+        line["vs_reference_tree_time"] = {"reference_cpu_tree_s_extrapolated": cpu_tree_s,
+                                          "casphy_e2e_tree_s": e2e_s / e2e_steps,
+                                          "ratio": cpu_tree_s / (e2e_s / e2e_steps)}
     if rank == 0 and world == 1 and args.cells is None and not args.no_extras:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        line["reference_gpu"] = reference_gpu_rows()
         line["blopt_c5"] = blopt_c5(L, codes, nstate, edge)
         line["bootstrap"] = bootstrap_suite(L)
         line["blopt"] = blopt_suite(L)

@@ -1752,3 +1752,268 @@ done:
     free(d1); free(m1); free(d2); free(m2);
     return st;
 }
+
+/* ------------------------------------------------------------------ */
+/* FP64 log-likelihoods for branch-length checks at full size.          */
+/* CasPhy has no likelihood code; these restate Felsenstein (1981)      */
+/* pruning in double precision, like oracle/felsenstein.py (which the   */
+/* CPU tests compare them with), but site-blocked in C so that trees    */
+/* of 10^5 tips take seconds.  Tree: edge nedge x 2 (parent, child),    */
+/* tips 0..ntip-1, every internal node with two children, the root the  */
+/* node that is no child.                                               */
+/* ------------------------------------------------------------------ */
+
+typedef struct {
+    u32 nn, root;
+    u32 *kid;   /* nn x 2 */
+    u32 *eoc;   /* edge of child, per node */
+    u32 *post;  /* internal nodes, children before parents */
+    u32 npost;
+} FelTree;
+
+static int fel_tree(u32 ntip, u32 nedge, const u32 *edge, FelTree *T) {
+    const u32 nn = nedge + 1;
+    T->nn = nn;
+    T->kid = (u32 *)malloc(sizeof(u32) * 2 * nn);
+    T->eoc = (u32 *)malloc(sizeof(u32) * nn);
+    T->post = (u32 *)malloc(sizeof(u32) * nn);
+    u32 *nk = (u32 *)calloc(nn, sizeof(u32));
+    u32 *stack = (u32 *)malloc(sizeof(u32) * nn);
+    unsigned char *isChild = (unsigned char *)calloc(nn, 1);
+    if (!T->kid || !T->eoc || !T->post || !nk || !stack || !isChild) { free(nk); free(stack); free(isChild); return ORACLE_ENOMEM; }
+    int st = ORACLE_OK;
+    for (u32 e = 0; e < nedge; e++) {
+        const u32 p = edge[2 * e], c = edge[2 * e + 1];
+        if (p >= nn || c >= nn || p < ntip || nk[p] >= 2 || isChild[c]) { st = ORACLE_EINVAL; goto out; }
+        T->kid[2 * p + nk[p]++] = c;
+        T->eoc[c] = e;
+        isChild[c] = 1;
+    }
+    T->root = nn;
+    for (u32 v = 0; v < nn; v++)
+        if (!isChild[v]) { if (T->root != nn) { st = ORACLE_EINVAL; goto out; } T->root = v; }
+    for (u32 v = ntip; v < nn; v++) if (nk[v] != 2) { st = ORACLE_EINVAL; goto out; }
+    /* reverse of a pre-order walk: children before parents */
+    u32 sp = 0, n = 0;
+    stack[sp++] = T->root;
+    while (sp) {
+        const u32 v = stack[--sp];
+        if (v < ntip) continue;
+        T->post[n++] = v;
+        stack[sp++] = T->kid[2 * v];
+        stack[sp++] = T->kid[2 * v + 1];
+    }
+    for (u32 i = 0; i < n / 2; i++) { const u32 x = T->post[i]; T->post[i] = T->post[n - 1 - i]; T->post[n - 1 - i] = x; }
+    T->npost = n;
+out:
+    free(nk); free(stack); free(isChild);
+    return st;
+}
+
+static void fel_tree_free(FelTree *T) { free(T->kid); free(T->eoc); free(T->post); }
+
+#define FEL_SB 16u /* sites per block */
+
+/* HKY85 (Hasegawa, Kishino & Yano 1985) on fasta2bin nibbles (bit 0 A,
+ * 1 T, 2 C, 3 G; several bits ambiguous, none missing).  P(t) = expm(Q t)
+ * with Q normalised to one substitution per unit time, from the eigen
+ * decomposition of the symmetrised Q (Q is reversible). */
+static void hky_Q(double kappa, const double *pi, double Q[4][4]) {
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) Q[i][j] = i == j ? 0.0 : pi[j];
+    Q[0][3] *= kappa; Q[3][0] *= kappa; Q[1][2] *= kappa; Q[2][1] *= kappa;
+    double mu = 0;
+    for (int i = 0; i < 4; i++) {
+        double s = 0;
+        for (int j = 0; j < 4; j++) s += Q[i][j];
+        Q[i][i] = -s;
+        mu += pi[i] * s;
+    }
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) Q[i][j] /= mu;
+}
+
+/* Jacobi eigen decomposition of a symmetric 4x4 matrix: A = V diag(w) V^T. */
+static void jacobi4(double A[4][4], double w[4], double V[4][4]) {
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) V[i][j] = i == j;
+    for (int sweep = 0; sweep < 100; sweep++) {
+        double off = 0;
+        for (int i = 0; i < 4; i++)
+            for (int j = i + 1; j < 4; j++) off += A[i][j] * A[i][j];
+        if (off < 1e-300) break;
+        for (int p = 0; p < 4; p++)
+            for (int q = p + 1; q < 4; q++) {
+                if (fabs(A[p][q]) < 1e-300) continue;
+                const double th = (A[q][q] - A[p][p]) / (2 * A[p][q]);
+                const double tt = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1));
+                const double c = 1 / sqrt(tt * tt + 1), s = tt * c;
+                for (int k = 0; k < 4; k++) {
+                    const double akp = A[k][p], akq = A[k][q];
+                    A[k][p] = c * akp - s * akq;
+                    A[k][q] = s * akp + c * akq;
+                }
+                for (int k = 0; k < 4; k++) {
+                    const double apk = A[p][k], aqk = A[q][k];
+                    A[p][k] = c * apk - s * aqk;
+                    A[q][k] = s * apk + c * aqk;
+                }
+                for (int k = 0; k < 4; k++) {
+                    const double vkp = V[k][p], vkq = V[k][q];
+                    V[k][p] = c * vkp - s * vkq;
+                    V[k][q] = s * vkp + c * vkq;
+                }
+            }
+    }
+    for (int i = 0; i < 4; i++) w[i] = A[i][i];
+}
+
+int oracle_loglik_hky85(uint32_t ntip, uint32_t nedge, const uint32_t *edge, const double *t, uint32_t nsite,
+                        const uint32_t *codes, const double *weights, double kappa, const double *pi, double *ll,
+                        int nthreads) {
+    FelTree T;
+    memset(&T, 0, sizeof(T));
+    int st = fel_tree(ntip, nedge, edge, &T);
+    if (st) { fel_tree_free(&T); return st; }
+    double Q[4][4], S[4][4], w[4], V[4][4], sq[4];
+    hky_Q(kappa, pi, Q);
+    for (int i = 0; i < 4; i++) sq[i] = sqrt(pi[i]);
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) S[i][j] = sq[i] * Q[i][j] / sq[j];
+    jacobi4(S, w, V);
+    /* P(t) for every edge: P = D^-1/2 V exp(w t) V^T D^1/2 */
+    double *P = (double *)malloc(sizeof(double) * 16 * (nedge ? nedge : 1));
+    if (!P) { fel_tree_free(&T); return ORACLE_ENOMEM; }
+    for (u32 e = 0; e < nedge; e++)
+        for (int i = 0; i < 4; i++)
+            for (int j = 0; j < 4; j++) {
+                double s = 0;
+                for (int k = 0; k < 4; k++) s += V[i][k] * exp(w[k] * t[e]) * V[j][k];
+                P[16 * e + 4 * i + j] = s * sq[j] / sq[i];
+            }
+    const u32 nn = T.nn, nblk = (nsite + FEL_SB - 1) / FEL_SB;
+    double total = 0;
+    nthreads = nthreads_or_default(nthreads);
+#pragma omp parallel num_threads(nthreads) reduction(+ : total)
+    {
+        double *L = (double *)malloc(sizeof(double) * (size_t)nn * FEL_SB * 4);
+        double *lsc = (double *)malloc(sizeof(double) * (size_t)nn * FEL_SB);
+#pragma omp for schedule(dynamic, 1)
+        for (long blk = 0; blk < (long)nblk; blk++) {
+            const u32 s0 = (u32)blk * FEL_SB, ns = nsite - s0 < FEL_SB ? nsite - s0 : FEL_SB;
+            for (u32 v = 0; v < ntip; v++)
+                for (u32 k = 0; k < ns; k++) {
+                    const u32 nib = codes[(size_t)v * nsite + s0 + k] & 0xFu;
+                    for (int i = 0; i < 4; i++) L[((size_t)v * FEL_SB + k) * 4 + i] = nib ? (double)((nib >> i) & 1u) : 1.0;
+                    lsc[(size_t)v * FEL_SB + k] = 0;
+                }
+            for (u32 x = 0; x < T.npost; x++) {
+                const u32 v = T.post[x];
+                for (u32 k = 0; k < ns; k++) {
+                    double acc[4] = {1, 1, 1, 1}, sc = 0;
+                    for (int h = 0; h < 2; h++) {
+                        const u32 c = T.kid[2 * v + h];
+                        const double *Pc = P + 16 * T.eoc[c], *Lc = L + ((size_t)c * FEL_SB + k) * 4;
+                        for (int i = 0; i < 4; i++)
+                            acc[i] *= Pc[4 * i] * Lc[0] + Pc[4 * i + 1] * Lc[1] + Pc[4 * i + 2] * Lc[2] + Pc[4 * i + 3] * Lc[3];
+                        sc += lsc[(size_t)c * FEL_SB + k];
+                    }
+                    double m = acc[0];
+                    for (int i = 1; i < 4; i++) m = acc[i] > m ? acc[i] : m;
+                    if (m <= 0) m = 1;
+                    for (int i = 0; i < 4; i++) L[((size_t)v * FEL_SB + k) * 4 + i] = acc[i] / m;
+                    lsc[(size_t)v * FEL_SB + k] = sc + log(m);
+                }
+            }
+            for (u32 k = 0; k < ns; k++) {
+                const double *Lr = L + ((size_t)T.root * FEL_SB + k) * 4;
+                const double site = log(pi[0] * Lr[0] + pi[1] * Lr[1] + pi[2] * Lr[2] + pi[3] * Lr[3]) +
+                                    lsc[(size_t)T.root * FEL_SB + k];
+                total += (weights ? weights[s0 + k] : 1.0) * site;
+            }
+        }
+        free(L); free(lsc);
+    }
+    *ll = total;
+    free(P);
+    fel_tree_free(&T);
+    return ORACLE_OK;
+}
+
+/* Irreversible edit model: per site state 0 = unedited, 1..K alleles;
+ * P(0->0) = exp(-r t), P(0->a) = q_a (1 - exp(-r t)), P(a->b) = [a == b];
+ * the root is unedited.  Tip codes (.tbmat): 0 missing, 1 unedited, c >= 2
+ * allele c-1.  Because alleles never change, a node's partial is non-zero
+ * on state 0 and on at most one allele: the one its subtree's non-missing
+ * tips share (none when they disagree or one is unedited; every allele,
+ * with one common value, when all its tips are missing).  The partial is
+ * kept as (L0, La, allele) with allele -1 none, 0 every allele, a >= 1. */
+int oracle_loglik_irreversible(uint32_t ntip, uint32_t nedge, const uint32_t *edge, const double *t, uint32_t nsite,
+                               const uint32_t *codes, const double *weights, uint32_t K, const double *q,
+                               double rate, double *ll, int nthreads) {
+    FelTree T;
+    memset(&T, 0, sizeof(T));
+    int st = fel_tree(ntip, nedge, edge, &T);
+    if (st) { fel_tree_free(&T); return st; }
+    const u32 nn = T.nn, nblk = (nsite + FEL_SB - 1) / FEL_SB;
+    double total = 0;
+    nthreads = nthreads_or_default(nthreads);
+#pragma omp parallel num_threads(nthreads) reduction(+ : total)
+    {
+        double *L0 = (double *)malloc(sizeof(double) * (size_t)nn * FEL_SB);
+        double *La = (double *)malloc(sizeof(double) * (size_t)nn * FEL_SB);
+        double *lsc = (double *)malloc(sizeof(double) * (size_t)nn * FEL_SB);
+        int *A = (int *)malloc(sizeof(int) * (size_t)nn * FEL_SB);
+#pragma omp for schedule(dynamic, 1)
+        for (long blk = 0; blk < (long)nblk; blk++) {
+            const u32 s0 = (u32)blk * FEL_SB, ns = nsite - s0 < FEL_SB ? nsite - s0 : FEL_SB;
+            for (u32 v = 0; v < ntip; v++)
+                for (u32 k = 0; k < ns; k++) {
+                    const u32 c = codes[(size_t)v * nsite + s0 + k];
+                    const size_t i = (size_t)v * FEL_SB + k;
+                    lsc[i] = 0;
+                    if (c == 0) { L0[i] = 1; La[i] = 1; A[i] = 0; }
+                    else if (c == 1) { L0[i] = 1; La[i] = 0; A[i] = -1; }
+                    else { L0[i] = 0; La[i] = 1; A[i] = (int)c - 1; }
+                }
+            for (u32 x = 0; x < T.npost; x++) {
+                const u32 v = T.post[x];
+                for (u32 k = 0; k < ns; k++) {
+                    const size_t iv = (size_t)v * FEL_SB + k;
+                    double l0 = 1, la = 1, sc = 0;
+                    int a = 0;
+                    for (int h = 0; h < 2; h++) {
+                        const u32 c = T.kid[2 * v + h];
+                        const size_t ic = (size_t)c * FEL_SB + k;
+                        const double p = exp(-rate * t[T.eoc[c]]);
+                        /* sum over the child's alleles of P(0->b) L_c(b) */
+                        double edited = 0;
+                        if (A[ic] == 0) edited = (1 - p) * La[ic];
+                        else if (A[ic] > 0) edited = (1 - p) * q[(size_t)(s0 + k) * (K + 1) + (u32)A[ic]] * La[ic];
+                        l0 *= p * L0[ic] + edited;
+                        /* alleles pass unchanged: the sets intersect */
+                        if (A[ic] < 0 || a < 0) { a = -1; la = 0; }
+                        else if (A[ic] == 0) la *= La[ic];
+                        else if (a == 0 || a == A[ic]) { a = A[ic]; la *= La[ic]; }
+                        else { a = -1; la = 0; }
+                        sc += lsc[ic];
+                    }
+                    double m = l0 > la ? l0 : la;
+                    if (m <= 0) m = 1;
+                    L0[iv] = l0 / m;
+                    La[iv] = la / m;
+                    A[iv] = a;
+                    lsc[iv] = sc + log(m);
+                }
+            }
+            for (u32 k = 0; k < ns; k++) {
+                const size_t ir = (size_t)T.root * FEL_SB + k;
+                total += (weights ? weights[s0 + k] : 1.0) * (log(L0[ir]) + lsc[ir]);
+            }
+        }
+        free(L0); free(La); free(lsc); free(A);
+    }
+    *ll = total;
+    fel_tree_free(&T);
+    return ORACLE_OK;
+}

@@ -150,6 +150,18 @@ int oracle_approx_compare(uint32_t ntip, uint32_t nnode1, uint32_t nbin, const u
                           const uint32_t *edge1, uint32_t nedge2, const uint32_t *edge2, uint32_t nnode2,
                           uint32_t cacheSize, float threshold, int32_t *ref2qry, int32_t *qry2ref);
 
+/* FP64 log-likelihoods (Felsenstein pruning) for branch-length checks at
+ * full size.  edge: nedge x 2 (parent, child), tips 0..ntip-1, binary, one
+ * root.  weights (nullable) per site.  HKY85 on fasta2bin nibbles;
+ * irreversible edits on .tbmat codes with q: nsite x (K+1) allele
+ * frequencies (column 0 unused). */
+int oracle_loglik_hky85(uint32_t ntip, uint32_t nedge, const uint32_t *edge, const double *t, uint32_t nsite,
+                        const uint32_t *codes, const double *weights, double kappa, const double *pi, double *ll,
+                        int nthreads);
+int oracle_loglik_irreversible(uint32_t ntip, uint32_t nedge, const uint32_t *edge, const double *t, uint32_t nsite,
+                               const uint32_t *codes, const double *weights, uint32_t K, const double *q,
+                               double rate, double *ll, int nthreads);
+
 #ifdef __cplusplus
 }
 #endif

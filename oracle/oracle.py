@@ -282,3 +282,61 @@ def join_bit_phased(words, w=None, ancestral_type=1, max_batch=8, pair_joins=Tru
                                       (1 if pair_joins else 0) | (2 if ride else 0),
                                       table_ctas, edge, state, stats, nthreads or os.cpu_count()), "join_bit_phased")
     return edge[: 2 * nedge].reshape(nedge, 2), state.reshape(-1, nbin), stats
+
+
+def _fel_edge(edge):
+    e = _u32(edge).reshape(-1, 2)
+    return e, e.shape[0]
+
+
+def loglik_hky85(edge, t, codes, kappa, pi, weights=None, nthreads=0):
+    """FP64 HKY85 log-likelihood (oracle_loglik_hky85); codes: (ntip, nsite)
+    fasta2bin nibbles, edge (nedge, 2) parent/child."""
+    e, ne = _fel_edge(edge)
+    codes = _u32(codes)
+    ntip, nsite = codes.shape
+    ll = C.c_double(0)
+    t = np.ascontiguousarray(t, dtype=np.float64)
+    pi = np.ascontiguousarray(pi, dtype=np.float64)
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+    L = lib()
+    L.oracle_loglik_hky85.argtypes = [C.c_uint32, C.c_uint32, _u32p, _f64p, C.c_uint32, _u32p, C.c_void_p,
+                                      C.c_double, _f64p, C.POINTER(C.c_double), C.c_int]
+    _chk(L.oracle_loglik_hky85(ntip, ne, e.reshape(-1), t, nsite, codes, None if w is None else w.ctypes.data,
+                               kappa, pi, C.byref(ll), nthreads or os.cpu_count()), "loglik_hky85")
+    return ll.value
+
+
+def tip_allele_freqs(codes, nallele):
+    """Per-site allele frequencies from the tips' allele counts, uniform over
+    the nallele alleles where a site has none (the library's default):
+    (nsite, nallele + 1), column 0 unused."""
+    codes = np.asarray(codes)
+    nsite = codes.shape[1]
+    q = np.zeros((nsite, nallele + 1))
+    for s in range(nsite):
+        col = codes[:, s].astype(np.int64)
+        cnt = np.bincount(col[col >= 2] - 1, minlength=nallele + 1)[: nallele + 1].astype(np.float64)
+        tot = cnt[1:].sum()
+        q[s, 1:] = cnt[1:] / tot if tot > 0 else 1.0 / nallele
+    return q
+
+
+def loglik_irreversible(edge, t, codes, nallele, q, rate, weights=None, nthreads=0):
+    """FP64 irreversible-edit log-likelihood in the compact form
+    (oracle_loglik_irreversible); codes: (ntip, nsite) .tbmat codes."""
+    e, ne = _fel_edge(edge)
+    codes = _u32(codes)
+    ntip, nsite = codes.shape
+    ll = C.c_double(0)
+    t = np.ascontiguousarray(t, dtype=np.float64)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    assert q.shape == (nsite, nallele + 1)
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+    L = lib()
+    L.oracle_loglik_irreversible.argtypes = [C.c_uint32, C.c_uint32, _u32p, _f64p, C.c_uint32, _u32p, C.c_void_p,
+                                             C.c_uint32, _f64p, C.c_double, C.POINTER(C.c_double), C.c_int]
+    _chk(L.oracle_loglik_irreversible(ntip, ne, e.reshape(-1), t, nsite, codes,
+                                      None if w is None else w.ctypes.data, nallele, q, rate, C.byref(ll),
+                                      nthreads or os.cpu_count()), "loglik_irreversible")
+    return ll.value

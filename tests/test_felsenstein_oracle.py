@@ -101,3 +101,26 @@ def test_gradients_match_central_differences():
     fd = F.central_differences(lambda tt: F.loglik_irreversible(12, par, ch, tt, ecodes, None, 1.0, q), t)
     assert np.isfinite(ll)
     assert np.allclose(g, fd, rtol=1e-5, atol=1e-5 * np.abs(g).max())
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_c_loglik_matches_dense_numpy(seed):
+    """The site-blocked C log-likelihoods used at full size (HKY85, and the
+    compact irreversible-edit form) equal the dense numpy oracle."""
+    import oracle as O
+    rng = np.random.default_rng(seed)
+    pi = [0.3, 0.2, 0.2, 0.3]
+    states, (par, ch, t) = synth.hky85_alignment(40, 37, 4.0, pi, 0.05, 0.05, seed=seed)
+    nib = synth.dna_nibbles(states)
+    w = rng.uniform(0.5, 2.0, 37)
+    e = np.stack([par, ch], 1)
+    want = F.loglik_hky85(40, par, ch, t, nib, w, 4.0, pi)
+    assert abs(O.loglik_hky85(e, t, nib, 4.0, pi, w) - want) <= 1e-11 * abs(want)
+    # irreversible edits on a lineage matrix with missing entries, on a random tree
+    raw = synth.lineage_states(30, 41, 8, 0.08, 6, 1.3, 0.2, seed=seed)
+    codes, ns = synth.regularize(raw)
+    _, (p2, c2, t2) = synth.hky85_alignment(30, 2, 4.0, pi, 0.3, 0.0, seed=seed + 10)
+    q = O.tip_allele_freqs(codes, ns)
+    want = F.loglik_irreversible(30, p2, c2, t2, codes, None, 0.8, q)
+    got = O.loglik_irreversible(np.stack([p2, c2], 1), t2, codes, ns, q, 0.8)
+    assert abs(got - want) <= 1e-11 * abs(want)
