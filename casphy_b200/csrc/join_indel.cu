@@ -1468,8 +1468,14 @@ extern "C" int casphy_join_indel_dev(uint32_t ntip, uint32_t ncol, const uint32_
 // buffers the caller passes in plus one fixed scratch region compiled into
 // this library.
 //
-// The scratch region is the file-scope array below.  Every GPU that loads
-// libcasphy.so holds it (kScratchBytes) until the process exits.  All calls on
+// The scratch region is the file-scope array below.  The CUDA runtime
+// reserves it on a device when it loads this file's device code there: at
+// context creation when modules load eagerly (CUDA_MODULE_LOADING=EAGER),
+// otherwise at the first use of any kernel or symbol of this file on that
+// device (the first indel join, with or without allocation).  From then on
+// the GPU holds it (kScratchBytes) until the process exits.  A caller that
+// hands the rest of the GPU's memory to its own pool should make its first
+// call (or set CUDA_MODULE_LOADING=EAGER) before it does.  All calls on
 // a device share it and each call overwrites it, so calls whose GPU work
 // overlaps (two host threads, or two streams) race; calls are serialised per
 // device by a host lock and return only after their work on the stream is
@@ -1617,6 +1623,14 @@ extern "C" int casphy_join_indel_noalloc(uint32_t ntip, uint32_t ncol, const uin
     if (rc) return rc;
     std::lock_guard<std::mutex> devLock(g_dev_mu[dev & 63]);
     cudaStream_t st = (cudaStream_t)stream;
+    // On every return from here on, wait for this call's work on the stream
+    // before the device lock is released (destroyed before devLock), so an
+    // early error return never leaves kernels using the shared scratch while
+    // the next call starts to overwrite it.
+    struct DrainOnReturn {
+        cudaStream_t s;
+        ~DrainOnReturn() { (void)cudaStreamSynchronize(s); }
+    } drain{st};
     Carve c;
     c.base = static_cast<char*>(base);
     const IndelBuffers L = carve_indel(c, ntip, ncol, nState, (u32)nSM, nChunks, false);

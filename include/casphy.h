@@ -383,12 +383,20 @@ int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t *words, co
  *   d_state_out  device, (ntip-1) x ncol u32 (the .nodeState2 body)
  * Needs ntip >= 2.  Sizes whose working set exceeds the 64 MiB scratch
  * (roughly ntip*ncol*14 bytes plus per-site tables) are rejected with
- * CASPHY_ERANGE and a message in casphy_last_error().  The first call on a
- * device looks up the scratch address for that device, so make that first
- * call before any stream capture.  All calls on a device share the scratch
- * and overwrite it: calls whose GPU work overlaps race, so the library
- * serialises them per device and each call returns only when its work on
- * `stream` has finished.
+ * CASPHY_ERANGE and a message in casphy_last_error().  The CUDA runtime
+ * reserves the scratch array on a device when it loads the library's device
+ * code there: at context creation with CUDA_MODULE_LOADING=EAGER, otherwise
+ * at the first indel join on that device (this call or casphy_join_indel*).
+ * A caller that gives the rest of the GPU to its own pool should make one
+ * call, or set CUDA_MODULE_LOADING=EAGER, before doing so; later calls change
+ * no device allocation.  The first call on a device also looks up the
+ * scratch address for that device, so make that first call before any stream
+ * capture.  All calls on a device share the scratch and overwrite it: calls
+ * whose GPU work overlaps race, so the library serialises them per device
+ * and each call, on success and on error, returns only when its work on
+ * `stream` has finished.  This variant uses the column-major u16 code scan
+ * (not the allele-bitset scan) and relabels the tree in one device thread,
+ * which suits its small sizes.
  */
 int casphy_join_indel_noalloc(uint32_t ntip, uint32_t ncol, const uint32_t *d_codes,
                               uint32_t nState, const double *weight, const uint32_t *tipSize,
