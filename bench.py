@@ -673,6 +673,73 @@ def reference_gpu_rows(budget_s=240.0):
     return rows
 
 
+def sharded_suite(L, world, rank, local):
+    """The parts of the path that shard, over all ranks (one GPU each, NCCL
+    on the ranks' GPUs): radius search by query-row blocks, TransferDisStream
+    by y-row blocks, bootstrap replicates k::world.  Each part is timed on the
+    device around the whole sharded call (compute and exchange), max over
+    ranks; rank 0 also checks the gathered result against one-GPU calls."""
+    import torch
+    from casphy_b200 import bootstrap as B
+    from casphy_b200 import shard, synth
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    res = {"ranks": world, "exchange": "NCCL all-gather / all-reduce of int32 views of u32 data on the GPUs"}
+
+    def timed(fn):
+        barrier(world)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        out = fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return out, max_over_ranks(a.elapsed_time(b) / 1e3, world)
+
+    words = synth.binary_workload(10_000, 512, 16, 0.03, 0.05, seed=23)
+    bmat = np.ascontiguousarray(words.T)
+    wr = np.ones(512)
+    rows = lambda lo, hi: L.radius_bit_rows(bmat, wr, RADIUS_SPARSE, lo, hi)  # noqa: E731
+    timed(lambda: shard.radius_sharded(rows, 10_000, device=dev))  # warm-up
+    (c, i), t = timed(lambda: shard.radius_sharded(rows, 10_000, device=dev))
+    res[f"C2_radiusNeighbor_r{RADIUS_SPARSE}"] = {"s": t}
+    if rank == 0:
+        c1, i1 = L.radius_bit(bmat, wr, RADIUS_SPARSE)
+        res[f"C2_radiusNeighbor_r{RADIUS_SPARSE}"]["identical_to_one_gpu"] = bool(
+            np.array_equal(c, c1) and np.array_equal(i, i1))
+    states, _ = synth.hky85_alignment(20_000, 2000, 4.0, [0.3, 0.2, 0.2, 0.3], 0.01, 0.02, seed=13)
+    raw, var = synth.dna_to_fasta2bin(states)
+    lv = int(var.sum())
+    drows = lambda lo, hi: L.radius_dna_rows(raw, lv - 20, lo, hi)  # noqa: E731
+    timed(lambda: shard.radius_sharded(drows, 20_000, device=dev))
+    (dc, di), t = timed(lambda: shard.radius_sharded(drows, 20_000, device=dev))
+    res["C3_radiusNeighborDNA"] = {"s": t}
+    if rank == 0:
+        c1, i1 = L.radius_dna(raw, lv - 20)
+        res["C3_radiusNeighborDNA"]["identical_to_one_gpu"] = bool(np.array_equal(dc, c1) and np.array_equal(di, i1))
+    edge, _, _ = L.join_bit(words, None, 1)
+    truth = synth.lineage_clades(10_000, 16, seed=23)
+    est = B.clade_bits(edge, 10_000, (10_000 + 31) // 32)
+    timed(lambda: shard.transfer_dis_sharded(L.transfer_dis, truth, est, 10_000, device=dev))
+    td, t = timed(lambda: shard.transfer_dis_sharded(L.transfer_dis, truth, est, 10_000, device=dev))
+    res["C2_TransferDisStream"] = {"s": t}
+    if rank == 0:
+        one = L.transfer_dis(truth, est, 10_000)
+        res["C2_TransferDisStream"]["identical_to_one_gpu"] = bool(all(np.array_equal(a, b) for a, b in zip(td, one)))
+    bwords = synth.binary_workload(10_000, 512, 16, 0.03, 0.05, seed=11)
+    full_edge, _, _ = L.join_bit(bwords, None, 1)
+    off, cells, w = B.make_replicates(10_000, 512, 200, 2000, 10_000, seed=12)
+    bs = lambda: shard.bootstrap_sharded(L.bootstrap_bit, bwords, full_edge, off, cells, w, device=dev)  # noqa: E731
+    bs()
+    (sup, ymin, ysize), t = timed(bs)
+    res["C4_bootstrap_200"] = {"s": t}
+    if rank == 0:
+        one = L.bootstrap_bit(bwords, full_edge, off, cells, w, threshold=0.05)
+        res["C4_bootstrap_200"]["identical_to_one_gpu"] = bool(
+            np.array_equal(sup, one["support"]) and np.array_equal(ymin, one["ymin"]))
+    return res
+
+
 def blopt_c5(L, codes, nstate, edge):
     """Irreversible edit-model branch lengths on the 200,000-cell join tree, and
     the reference's parsimony change counts (charAncestralEC) on the same tree."""
@@ -891,6 +958,8 @@ def main():
         line["vs_reference_tree_time"] = {"reference_cpu_tree_s_extrapolated": cpu_tree_s,
                                           "casphy_e2e_tree_s": e2e_s / e2e_steps,
                                           "ratio": cpu_tree_s / (e2e_s / e2e_steps)}
+    if world > 1 and args.cells is None and not args.no_extras:
+        line["sharded"] = sharded_suite(L, world, rank, local)  # every rank: collectives inside
     if rank == 0 and world == 1 and args.cells is None and not args.no_extras:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         line["reference_gpu"] = reference_gpu_rows()

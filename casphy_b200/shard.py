@@ -13,6 +13,10 @@ per GPU, torch.distributed for the exchange).
 * The greedy joins do not shard (every join depends on the previous argmax):
   several GPUs run independent trees (replicas).
 
+Every exchanged array is u32 data viewed as int32 (bit for bit; the values
+that are reduced, counts and distances, are below 2^31), placed on `device`
+when one is given (the rank's GPU, for NCCL) and on the host otherwise (gloo).
+
 `compute` is the single-device function (casphy_b200.lib on a GPU); tests
 pass the CPU oracle instead to check the partitioning on gloo ranks.
 """
@@ -30,15 +34,21 @@ def block(n: int, world: int, rank: int, align: int = 1):
     return lo, hi
 
 
-def _torch_u32(a):
+def _dev(a, device):
+    """u32 array -> int32 tensor (same bits) on device (host when None)."""
     import torch
-    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.uint32).view(np.int32).astype(np.int64))
+    t = torch.from_numpy(np.ascontiguousarray(a, dtype=np.uint32).view(np.int32))
+    return t.to(device) if device is not None else t
+
+
+def _host(t):
+    """int32 tensor -> u32 array (same bits)."""
+    return t.cpu().numpy().view(np.uint32)
 
 
 def transfer_dis_sharded(compute, y, x, ntip, group=None, device=None):
     """TransferDisStream over world ranks; every rank returns the full
     (ymin, ysize, xmin, xsize)."""
-    import torch
     import torch.distributed as dist
     world, rank = dist.get_world_size(group), dist.get_rank(group)
     y = np.ascontiguousarray(y, dtype=np.uint32)
@@ -49,28 +59,24 @@ def transfer_dis_sharded(compute, y, x, ntip, group=None, device=None):
         np.zeros(0, np.uint32), np.zeros(0, np.uint32), np.full(len(x), 32 * ncol, np.uint32), None)
     if xsize is None:
         _, _, _, xsize = compute(y[:0], x, ntip)
-    xm = _torch_u32(xmin_l)
-    if device is not None:
-        xm = xm.to(device)
+    xm = _dev(xmin_l, device)
     dist.all_reduce(xm, op=dist.ReduceOp.MIN, group=group)
     # gather the y slices (fixed-size buffers: the largest share)
     share = block(ny, world, 0, align=8)[1]
-    buf = np.zeros((2, share), dtype=np.int64)
+    buf = np.zeros((2, share), dtype=np.uint32)
     buf[0, :hi - lo] = ymin_l
     buf[1, :hi - lo] = ysize_l
-    t = torch.from_numpy(buf)
-    if device is not None:
-        t = t.to(device)
-    parts = [torch.zeros_like(t) for _ in range(world)]
+    t = _dev(buf, device)
+    parts = [t.new_zeros(t.shape) for _ in range(world)]
     dist.all_gather(parts, t, group=group)
     ymin = np.zeros(ny, np.uint32)
     ysize = np.zeros(ny, np.uint32)
     for k, p in enumerate(parts):
         a, b = block(ny, world, k, align=8)
-        p = p.cpu().numpy()
+        p = _host(p)
         ymin[a:b] = p[0, :b - a]
         ysize[a:b] = p[1, :b - a]
-    return ymin, ysize, xm.cpu().numpy().astype(np.uint32), xsize
+    return ymin, ysize, _host(xm).copy(), xsize
 
 
 def bootstrap_sharded(compute, words, full_edge, offsets, cells, weights, threshold=0.05, group=None,
@@ -78,44 +84,35 @@ def bootstrap_sharded(compute, words, full_edge, offsets, cells, weights, thresh
     """Replicates k::world on rank k; returns (support over all replicates,
     ymin, ysize in replicate order) on every rank.  `compute` has the
     signature of casphy_b200.lib.bootstrap_bit."""
-    import torch
     import torch.distributed as dist
     world, rank = dist.get_world_size(group), dist.get_rank(group)
     offsets = np.asarray(offsets, dtype=np.int64)
     nrep = len(offsets) - 1
     mine = list(range(rank, nrep, world))
     nX = np.asarray(words).shape[0] - 2
-    ymin_l = np.zeros((len(mine), nX), np.int64)
-    ysize_l = np.zeros((len(mine), nX), np.int64)
-    sup = np.zeros(nX, np.int64)
+    per = (nrep + world - 1) // world
+    buf = np.zeros((2, per, nX), np.uint32)
+    sup = np.zeros(nX, np.uint32)
     if mine:
         sub_cells = np.concatenate([cells[offsets[r]:offsets[r + 1]] for r in mine])
         sub_off = np.concatenate([[0], np.cumsum([offsets[r + 1] - offsets[r] for r in mine])]).astype(np.uint32)
         got = compute(words, full_edge, sub_off, sub_cells, np.asarray(weights)[mine], threshold=threshold)
         sup[:] = got["support"]
-        ymin_l[:] = got["ymin"]
-        ysize_l[:] = got["ysize"]
-    s = torch.from_numpy(sup)
-    if device is not None:
-        s = s.to(device)
+        buf[0, :len(mine)] = got["ymin"]
+        buf[1, :len(mine)] = got["ysize"]
+    s = _dev(sup, device)
     dist.all_reduce(s, op=dist.ReduceOp.SUM, group=group)
-    per = (nrep + world - 1) // world
-    buf = np.zeros((2, per, nX), np.int64)
-    buf[0, :len(mine)] = ymin_l
-    buf[1, :len(mine)] = ysize_l
-    t = torch.from_numpy(buf)
-    if device is not None:
-        t = t.to(device)
-    parts = [torch.zeros_like(t) for _ in range(world)]
+    t = _dev(buf, device)
+    parts = [t.new_zeros(t.shape) for _ in range(world)]
     dist.all_gather(parts, t, group=group)
     ymin = np.zeros((nrep, nX), np.uint32)
     ysize = np.zeros((nrep, nX), np.uint32)
     for k, p in enumerate(parts):
-        p = p.cpu().numpy()
+        p = _host(p)
         for i, r in enumerate(range(k, nrep, world)):
             ymin[r] = p[0, i]
             ysize[r] = p[1, i]
-    return s.cpu().numpy().astype(np.uint32), ymin, ysize
+    return _host(s).copy(), ymin, ysize
 
 
 def radius_sharded(compute_rows, nrows, group=None, device=None):
@@ -123,32 +120,27 @@ def radius_sharded(compute_rows, nrows, group=None, device=None):
     idx) of query rows [lo, hi) (casphy_b200.lib.radius_bit_rows or
     radius_dna_rows with the matrix bound); every rank returns the full
     (counts, idx)."""
-    import torch
     import torch.distributed as dist
     world, rank = dist.get_world_size(group), dist.get_rank(group)
     lo, hi = block(nrows, world, rank)
     counts, idx = compute_rows(lo, hi) if hi > lo else (np.zeros(0, np.uint32), np.zeros(0, np.uint32))
-    n = torch.tensor([len(idx)], dtype=torch.int64)
-    if device is not None:
-        n = n.to(device)
-    sizes = [torch.zeros_like(n) for _ in range(world)]
+    n = _dev(np.array([len(idx)], np.uint32), device)
+    sizes = [n.new_zeros(n.shape) for _ in range(world)]
     dist.all_gather(sizes, n, group=group)
-    sizes = [int(x.item()) for x in sizes]
+    sizes = [int(_host(x)[0]) for x in sizes]
     share = block(nrows, world, 0)[1]
-    c = np.zeros(share, np.int64)
+    c = np.zeros(share, np.uint32)
     c[:hi - lo] = counts
-    i = np.zeros(max(sizes) if sizes else 0, np.int64)
+    i = np.zeros(max(max(sizes), 1), np.uint32)
     i[:len(idx)] = idx
-    tc, ti = torch.from_numpy(c), torch.from_numpy(i)
-    if device is not None:
-        tc, ti = tc.to(device), ti.to(device)
-    pc = [torch.zeros_like(tc) for _ in range(world)]
-    pi = [torch.zeros_like(ti) for _ in range(world)]
+    tc, ti = _dev(c, device), _dev(i, device)
+    pc = [tc.new_zeros(tc.shape) for _ in range(world)]
+    pi = [ti.new_zeros(ti.shape) for _ in range(world)]
     dist.all_gather(pc, tc, group=group)
     dist.all_gather(pi, ti, group=group)
     out_c, out_i = [], []
     for k in range(world):
         a, b = block(nrows, world, k)
-        out_c.append(pc[k].cpu().numpy()[:b - a])
-        out_i.append(pi[k].cpu().numpy()[:sizes[k]])
+        out_c.append(_host(pc[k])[:b - a])
+        out_i.append(_host(pi[k])[:sizes[k]])
     return np.concatenate(out_c).astype(np.uint32), np.concatenate(out_i).astype(np.uint32)

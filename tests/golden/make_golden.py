@@ -7,7 +7,8 @@ Three steps (the second needs a GPU, the others do not):
       data sets mat1k / mat_binary read from their .rda files, and the
       run1_1024 example alignment run through the reference fasta2bin) and
       stores them in tests/golden/cases.npz.  Reads the CasPhy source tree
-      (REF env var, default /root/reference) for the .rda/.fasta fixtures.
+      (REF env var, else a checkout named reference beside this repository)
+      for the .rda/.fasta fixtures.
 
   python tests/golden/make_golden.py run-ref OUTDIR
       Writes each case as the reference file set, runs the reference tools
@@ -344,7 +345,10 @@ def collect(outdir: str):
 if __name__ == "__main__":
     cmd = sys.argv[1] if len(sys.argv) > 1 else ""
     if cmd == "prepare":
-        prepare(os.environ.get("REF", "/root/reference"))
+        ref = os.environ.get("REF", os.path.join(ROOT, os.pardir, "reference"))
+        if not os.path.isdir(os.path.join(ref, "cu")):
+            raise SystemExit(f"no CasPhy source tree at {ref}: set REF to the reference checkout")
+        prepare(ref)
     elif cmd == "run-ref":
         run_ref(sys.argv[2])
     elif cmd == "collect":
