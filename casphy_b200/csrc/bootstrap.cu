@@ -674,6 +674,7 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
         c.Rmax = ((n + Gs[r] - 1) / Gs[r] + 7u) & ~7u; c.ordNeg1 = ORD_F32_NEG1; c.compactMin = 4096; c.compactQ8 = 192; c.bytesPerPairSite = 4000;
         c.prof = nullptr;
         c.maxBatch = joinx::stale_batch_setting();
+        c.deathWords = (2 * n - 1 + 31) / 32;  // joined-node bitmap: 2.5 KB at 10,000 cells
         R.m = BitModel<PATH_PLANES>::Args{nbin, nbinP, nplanes, ancestralType ? 1 : 0, b.planeMask, nullptr,
                                           b.nodeSeq, b.nodeBis, {b.colT0, b.colT1}};
         R.init = InitArgs{n, nbin, Sp, eStride, b.colT0, b.eW, b.eQ, b.eLen, nullptr, b.chunkStart, nChunks,
@@ -716,12 +717,21 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
     const u32 nItem = (u32)itemRep.size();
     // shared memory of a join CTA: engine + model, or the post-order offsets
     using M = BitModel<PATH_PLANES>;
-    size_t smemJoin = 0;
-    for (u32 r = 0; r < nrep; r++)
-        smemJoin = std::max(smemJoin, M::engine_smem_bytes(Gs[r], reps[r].c.Rmax) + M::model_smem_bytes(reps[r].m));
-    const size_t smem = std::max(smemJoin, (size_t)4 * nmax);
     int maxSmem = 0;
     CASPHY_CUDA_TRY(cudaDeviceGetAttribute(&maxSmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ds.dev));
+    auto joinSmem = [&] {
+        size_t m = 0;
+        for (u32 r = 0; r < nrep; r++)
+            m = std::max(m, M::engine_smem_bytes(Gs[r], reps[r].c.Rmax, reps[r].c.deathWords) +
+                                M::model_smem_bytes(reps[r].m));
+        return m;
+    };
+    size_t smemJoin = joinSmem();
+    if (smemJoin + 1024 > (size_t)maxSmem) {  // without the joined-node bitmaps (node deaths from global memory)
+        for (u32 r = 0; r < nrep; r++) reps[r].c.deathWords = 0;
+        smemJoin = joinSmem();
+    }
+    const size_t smem = std::max(smemJoin, (size_t)4 * nmax);
     if (smem + 1024 > (size_t)maxSmem) {
         casphy_set_last_error_msg("bootstrap: replicate too large for one CTA's shared memory");
         return CASPHY_ERANGE;

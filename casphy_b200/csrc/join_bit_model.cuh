@@ -200,17 +200,23 @@ struct BitModel {
         QueryArgs q{m.nbin, PATH == PATH_PLANES ? m.nplanes : 0u, m.planeMask};
         return build_bit_entries(q, s.mseq, s.eW, s.eQ, wc);
     }
-    __device__ static void store_node(const Args& m, Smem& s, u32 newNode) {
+    // CTA `part` of `nparts` writes its slice of the new node's rows
+    __device__ static void store_node(const Args& m, Smem& s, u32 newNode, u32 part, u32 nparts) {
         u32* ds = m.nodeSeq + (size_t)newNode * m.nbinP;
         u32* db = m.nodeBis + (size_t)newNode * m.nbinP;
-        for (u32 w = threadIdx.x; w < m.nbinP; w += kThreads) {
+        const u32 per = (m.nbinP + nparts - 1) / nparts, w1 = min(m.nbinP, (part + 1) * per);
+        for (u32 w = part * per + threadIdx.x; w < w1; w += kThreads) {
             ds[w] = s.mseq[w];
             db[w] = s.mbis[w];
         }
     }
-    __device__ static void store_slot(const Args& m, Smem& s, u32 buf, const joinx::Range& rg, u32 c1, u32) {
+    // ... and its slice of slot c1's column (c1 is skipped by this phase's
+    // scan, so the owner may read the column while others write it)
+    __device__ static void store_slot(const Args& m, Smem& s, u32 buf, const joinx::Range& rg, u32 c1, u32 part,
+                                      u32 nparts) {
         u32* c = col(m, buf);
-        for (u32 w = threadIdx.x; w < m.nbin; w += kThreads) c[(size_t)w * rg.Sp + c1] = s.mseq[w];
+        const u32 per = (m.nbin + nparts - 1) / nparts, w1 = min(m.nbin, (part + 1) * per);
+        for (u32 w = part * per + threadIdx.x; w < w1; w += kThreads) c[(size_t)w * rg.Sp + c1] = s.mseq[w];
     }
     __device__ static u32 pass_cap(const Args&, u32 R) {
         u32 F = 1;

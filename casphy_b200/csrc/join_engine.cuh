@@ -502,14 +502,19 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
         const u32 j1 = key_node(g.key), c1 = g.slot, j2 = g.partner;
         if (c1 >= rg.S || j1 >= a.nnode || j2 >= a.nnode) { fail = CASPHY_EINTERNAL; break; }
         // With the joined-node bitmap and no size rule, the decision needs no
-        // load: the partner's slot is loaded by thread 0 and first used after
-        // the query build, which hides its latency.
+        // load: the partner's slot and the two node sizes (the new node's size
+        // is kept for callers that read it) are loaded by thread 0 and first
+        // used after the query build, which hides their latency.
         const bool quick = a.deathWords && !a.needSizes;
         bool stale;
-        u32 c2 = 0, s1 = 0, s2 = 0, c2pending = 0;
+        u32 c2 = 0, s1 = 0, s2 = 0, c2pending = 0, s1pending = 0, s2pending = 0;
         if (quick) {
             stale = (deathBits[j2 >> 5] >> (j2 & 31)) & 1u;
-            if (!stale && threadIdx.x == 0) c2pending = ld_cg_u32(a.node2slot + j2);
+            if (!stale && threadIdx.x == 0) {
+                c2pending = ld_cg_u32(a.node2slot + j2);
+                s1pending = ld_cg_u32(a.nodeSize + j1);
+                s2pending = ld_cg_u32(a.nodeSize + j2);
+            }
         } else {
             if (threadIdx.x == 0) {
                 s_val[0] = ld_cg_u32(a.nodeDeath + j2);
@@ -640,16 +645,25 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
         const u32 newNode = a.ntip + k;
         const int nE = M::build_join(m, ms, j1, j2, s1, s2, wcount);
         if (quick) {
-            if (threadIdx.x == 0) s_val[1] = c2pending;
+            if (threadIdx.x == 0) {
+                s_val[1] = c2pending;
+                s_val[2] = s1pending;
+                s_val[3] = s2pending;
+            }
             __syncthreads();
             c2 = s_val[1];
+            s1 = s_val[2];
+            s2 = s_val[3];
             if (c2 >= rg.S) fail = CASPHY_EINTERNAL;  // a live node always has a slot
             __syncthreads();
             if (fail) break;
         }
         pf.mark(PROF_BUILD);
+        // every CTA writes a slice of the new node's row and of slot c1's
+        // column, so no CTA reaches the barrier late with all of them
+        M::store_node(m, ms, newNode, b, nCTA);
+        M::store_slot(m, ms, buf, rg, c1, b, nCTA);
         if (b == 0) {
-            M::store_node(m, ms, newNode);
             if (threadIdx.x == 0) {
                 a.nodeSize[newNode] = s1 + s2;
                 a.rawEdge[4 * k + 0] = newNode;
@@ -662,7 +676,6 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
             }
         }
         if (c1 >= rg.lo && c1 < rg.hi) {
-            M::store_slot(m, ms, buf, rg, c1, j1);
             if (threadIdx.x == 0) {
                 slotNode_of(a, buf)[c1] = newNode;
                 lmOrd_of(a, buf)[c1] = a.ordNeg1;

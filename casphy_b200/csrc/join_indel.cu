@@ -390,13 +390,19 @@ struct IndelDense {
         return build_indel_query(m.ncol, m.ncolP, m.unitW, m.Wsel, m.nodeRow + (size_t)j1 * m.ncolP,
                                  m.nodeRow + (size_t)j2 * m.ncolP, mode, s.mrow, nullptr, s.eSC, s.eW, wc);
     }
-    __device__ static void store_node(const Args& m, Smem& s, u32 newNode) {
+    // CTA `part` of `nparts` writes its slice of the new node's row
+    __device__ static void store_node(const Args& m, Smem& s, u32 newNode, u32 part, u32 nparts) {
         u16* dst = m.nodeRow + (size_t)newNode * m.ncolP;
-        for (u32 i = threadIdx.x; i < m.ncolP; i += kThreads) dst[i] = s.mrow[i];
+        const u32 per = (m.ncolP + nparts - 1) / nparts, i1 = min(m.ncolP, (part + 1) * per);
+        for (u32 i = part * per + threadIdx.x; i < i1; i += kThreads) dst[i] = s.mrow[i];
     }
-    __device__ static void store_slot(const Args& m, Smem& s, u32 buf, const joinx::Range& rg, u32 c1, u32) {
+    // ... and its slice of slot c1's column entries (c1 is skipped by this
+    // phase's scan, so the owner may read the column while others write it)
+    __device__ static void store_slot(const Args& m, Smem& s, u32 buf, const joinx::Range& rg, u32 c1, u32 part,
+                                      u32 nparts) {
         u16* c = col(m, buf);
-        for (u32 i = threadIdx.x; i < m.ncol; i += kThreads) c[(size_t)i * rg.Sp + c1] = s.mrow[i];
+        const u32 per = (m.ncol + nparts - 1) / nparts, i1 = min(m.ncol, (part + 1) * per);
+        for (u32 i = part * per + threadIdx.x; i < i1; i += kThreads) c[(size_t)i * rg.Sp + c1] = s.mrow[i];
     }
     // INT: the query entries are split over F thread groups that share the
     // candidates (F as large as the CTA's slot range allows); HALF: one group,
@@ -704,17 +710,22 @@ struct IndelBits {
         return build_indel_query(m.ncol, m.ncolP, m.unitW, m.Wsel, m.nodeRow + (size_t)j1 * m.ncolP,
                                  m.nodeRow + (size_t)j2 * m.ncolP, mode, s.mrow, s.orow, s.eSC, s.eW, wc);
     }
-    __device__ static void store_node(const Args& m, Smem& s, u32 newNode) {
+    // CTA `part` of `nparts` writes its slice of the new node's row
+    __device__ static void store_node(const Args& m, Smem& s, u32 newNode, u32 part, u32 nparts) {
         u16* dst = m.nodeRow + (size_t)newNode * m.ncolP;
-        for (u32 i = threadIdx.x; i < m.ncolP; i += kThreads) dst[i] = s.mrow[i];
+        const u32 per = (m.ncolP + nparts - 1) / nparts, i1 = min(m.ncolP, (part + 1) * per);
+        for (u32 i = part * per + threadIdx.x; i < i1; i += kThreads) dst[i] = s.mrow[i];
     }
-    // the new node replaces j1 in slot c1: flip c1's bit in the rows of the
-    // sites where the two states differ (fire-and-forget reductions; the word
-    // belongs to this CTA and nobody reads it before the next phase)
-    __device__ static void store_slot(const Args& m, Smem& s, u32 buf, const joinx::Range& rg, u32 c1, u32) {
+    // the new node replaces j1 in slot c1: each CTA flips c1's bit in the rows
+    // of its slice of the sites where the two states differ (fire-and-forget
+    // reductions on single bits; c1 is skipped by this phase's scans, and the
+    // next phase reads the words after the grid barrier)
+    __device__ static void store_slot(const Args& m, Smem& s, u32 buf, const joinx::Range& rg, u32 c1, u32 part,
+                                      u32 nparts) {
         u32* B = bitsOf(m, buf);
         const u32 Wd = rg.Sp / 32, word = c1 >> 5, bit = 1u << (c1 & 31);
-        for (u32 i = threadIdx.x; i < m.ncol; i += kThreads) {
+        const u32 per = (m.ncol + nparts - 1) / nparts, i1 = min(m.ncol, (part + 1) * per);
+        for (u32 i = part * per + threadIdx.x; i < i1; i += kThreads) {
             const u32 o = s.orow[i], n = s.mrow[i];
             if (o == n) continue;
             if (o > 1) atomicAnd(B + ((size_t)i * m.nState + o - 2) * Wd + word, ~bit);
