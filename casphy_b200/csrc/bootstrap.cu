@@ -675,6 +675,7 @@ extern "C" int casphy_bootstrap_bit(uint32_t ntip, uint32_t nbin, const uint32_t
         c.prof = nullptr;
         c.maxBatch = joinx::stale_batch_setting();
         c.deathWords = (2 * n - 1 + 31) / 32;  // joined-node bitmap: 2.5 KB at 10,000 cells
+        c.keepSizes = 1;                         // build_ops lays out clades by node size
         R.m = BitModel<PATH_PLANES>::Args{nbin, nbinP, nplanes, ancestralType ? 1 : 0, b.planeMask, nullptr,
                                           b.nodeSeq, b.nodeBis, {b.colT0, b.colT1}};
         R.init = InitArgs{n, nbin, Sp, eStride, b.colT0, b.eW, b.eQ, b.eLen, nullptr, b.chunkStart, nChunks,

@@ -200,7 +200,7 @@ struct BitModel {
         QueryArgs q{m.nbin, PATH == PATH_PLANES ? m.nplanes : 0u, m.planeMask};
         return build_bit_entries(q, s.mseq, s.eW, s.eQ, wc);
     }
-    // CTA `part` of `nparts` writes its slice of the new node's rows
+    // slice `part` of `nparts` of the new node's rows (the engine writes them whole)
     __device__ static void store_node(const Args& m, Smem& s, u32 newNode, u32 part, u32 nparts) {
         u32* ds = m.nodeSeq + (size_t)newNode * m.nbinP;
         u32* db = m.nodeBis + (size_t)newNode * m.nbinP;
@@ -210,8 +210,8 @@ struct BitModel {
             db[w] = s.mbis[w];
         }
     }
-    // ... and its slice of slot c1's column (c1 is skipped by this phase's
-    // scan, so the owner may read the column while others write it)
+    // slice `part` of `nparts` of slot c1's column (the engine gives the whole
+    // column to c1's owner)
     __device__ static void store_slot(const Args& m, Smem& s, u32 buf, const joinx::Range& rg, u32 c1, u32 part,
                                       u32 nparts) {
         u32* c = col(m, buf);

@@ -73,6 +73,7 @@ struct Common {
     u32 maxBatch;         // stale rows per rescan phase, 1..kMaxBatch
     u32 deathWords;       // words of the per-CTA shared-memory bitmap of joined nodes (0: none)
     u32 needSizes;        // the model's join reads the two node sizes (minSize > 0)
+    u32 keepSizes;        // the caller reads nodeSize of new nodes after the loop (bootstrap clade layout)
     u32 preSlots;         // a join's scan prefetches its slots' node, maximum and partner into shared memory
     unsigned long long* prof;  // nullable: CTA 0 section times (ns), see PROF_*
 };
@@ -502,9 +503,9 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
         const u32 j1 = key_node(g.key), c1 = g.slot, j2 = g.partner;
         if (c1 >= rg.S || j1 >= a.nnode || j2 >= a.nnode) { fail = CASPHY_EINTERNAL; break; }
         // With the joined-node bitmap and no size rule, the decision needs no
-        // load: the partner's slot and the two node sizes (the new node's size
-        // is kept for callers that read it) are loaded by thread 0 and first
-        // used after the query build, which hides their latency.
+        // load: the partner's slot (and, for callers that read the new node's
+        // size, the two node sizes) is loaded by thread 0 and first used after
+        // the query build, which hides its latency.
         const bool quick = a.deathWords && !a.needSizes;
         bool stale;
         u32 c2 = 0, s1 = 0, s2 = 0, c2pending = 0, s1pending = 0, s2pending = 0;
@@ -512,8 +513,10 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
             stale = (deathBits[j2 >> 5] >> (j2 & 31)) & 1u;
             if (!stale && threadIdx.x == 0) {
                 c2pending = ld_cg_u32(a.node2slot + j2);
-                s1pending = ld_cg_u32(a.nodeSize + j1);
-                s2pending = ld_cg_u32(a.nodeSize + j2);
+                if (a.keepSizes) {
+                    s1pending = ld_cg_u32(a.nodeSize + j1);
+                    s2pending = ld_cg_u32(a.nodeSize + j2);
+                }
             }
         } else {
             if (threadIdx.x == 0) {
@@ -540,21 +543,6 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
             }
             if (nb == 0 || s_batch[0].slot != c1) { fail = CASPHY_EINTERNAL; break; }
             pf.mark(PROF_SELECT);
-            // this CTA's slots (node, maximum, partner) for the fresh table
-            // below: copied into shared memory under the rescan (the model
-            // waits for every copy of this thread before its first barrier)
-            const bool preS = M::kFusedStale && a.preSlots && rg.lo < rg.hi;
-            if (preS) {
-                const u32 n4 = (rg.hi - rg.lo + 3u) / 4u;
-                const u32* sn0 = slotNode_of(a, buf);
-                const u32* lo0 = lmOrd_of(a, buf);
-                const u32* li0 = lmIdx_of(a, buf);
-                for (u32 i = threadIdx.x; i < 3 * n4; i += kThreads) {
-                    const u32 arr = i / n4, j = 4 * (i % n4);
-                    const u32* src = arr == 0 ? sn0 : (arr == 1 ? lo0 : li0);
-                    cp_async16(preSn + arr * a.Rmax + j, src + rg.lo + j);
-                }
-            }
             if constexpr (M::kFusedStale) {
                 if (nb >= 1)
                     M::stale_multi(m, ms, buf, rg, slotNode_of(a, buf), nb, s_batch, s_pbest, s_nE, ordOut, red,
@@ -565,32 +553,6 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
                 stale_scan_each<M>(a, m, ms, buf, rg, nb, s_batch, s_pbest, s_nE, ordOut, red, &s_rec, wcount);
             }
             pf.mark(PROF_STALE_SCAN);
-            // A fresh table instead of patches: this CTA's top two and count
-            // over its live rows outside the batch (whose maxima are final
-            // for this phase); every CTA adds the batch rows' new records
-            // after the barrier, so no list runs dry.
-            {
-                Top2 tt;
-                tt.init();
-                u32 n = 0;
-                const u32* sn0 = slotNode_of(a, buf);
-                const u32* lo0 = lmOrd_of(a, buf);
-                const u32* li0 = lmIdx_of(a, buf);
-                for (u32 c = rg.lo + threadIdx.x; c < rg.hi; c += kThreads) {
-                    const u32 x = c - rg.lo;
-                    const u32 node = preS ? preSn[x] : ld_cg_u32(sn0 + c);
-                    const u32 o = preS ? preLo[x] : ld_cg_u32(lo0 + c);
-                    if (node == kDead || o == a.ordNeg1) continue;
-                    bool inBatch = false;
-                    for (u32 q = 0; q < nb; q++) inBatch |= s_batch[q].slot == c;
-                    if (inBatch) continue;
-                    n++;
-                    tt.push(make_key(o, node), c, preS ? preLi[x] : ld_cg_u32(li0 + c));
-                }
-                cnt = block_sum_u32(n, wsum);
-                block_top2(tt, red, &s_rec, s_top);
-            }
-            publish(a, p, b, s_top, cnt);
             if (threadIdx.x < nb) {
                 asm volatile("st.global.cg.u64 [%0], %1;" ::"l"(a.partial + ((p & 1) * nCTA + b) * kMaxBatch +
                                                                   threadIdx.x),
@@ -641,33 +603,41 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
                     lmIdx_of(a, buf)[row.slot] = key_node(s_pbest[threadIdx.x]);
                 }
             }
-            load_table_any(a, p - 1, T, s_top, cnt);
             if (threadIdx.x == 0) {
-                // the batch rows' new records, in batch order, into the lists
-                // their owners published without them
                 for (u32 q = 0; q < nb; q++) {
                     const BlockRec row = s_batch[q];
                     const u32 vOrd = key_ord(s_pbest[q]), vIdx = key_node(s_pbest[q]);
-                    if (vOrd == a.ordNeg1) continue;  // no live partner: no record
                     const u32 ob = row.slot / rg.R;
                     BlockRec nr;
                     nr.key = make_key(vOrd, key_node(row.key));
                     nr.slot = row.slot;
                     nr.partner = vIdx;
                     BlockRec* L = T.tab + 2 * ob;
-                    const unsigned char n = T.cnt[ob];
+                    unsigned char n = T.cnt[ob];
+                    // drop the row's old record (it is listed: it was selected from this table)
+                    if (n >= 1 && L[0].slot == row.slot) {
+                        L[0] = L[1];
+                        n--;
+                    } else if (n == 2 && L[1].slot == row.slot) {
+                        n--;
+                    } else {
+                        fail = CASPHY_EINTERNAL;
+                    }
+                    const bool real = vOrd != a.ordNeg1;
                     if (T.exact[ob]) {
-                        // every record of the range is listed: insert in order
-                        if (n == 0) L[0] = nr;
-                        else if (nr.key > L[0].key) { L[1] = L[0]; L[0] = nr; }
-                        else if (n == 1 || nr.key > L[1].key) L[1] = nr;
-                        if (n == 2) T.exact[ob] = 0;  // three records, two listed
-                        T.cnt[ob] = n < 2 ? n + 1 : 2;
-                    } else if (nr.key > L[1].key) {
+                        if (real) {
+                            if (n == 0) L[0] = nr;
+                            else if (nr.key > L[0].key) { L[1] = L[0]; L[0] = nr; }
+                            else L[1] = nr;
+                            n++;
+                        }
+                    } else if (n >= 1 && real && nr.key > L[n - 1].key) {
                         // above the last listed record, hence above every unlisted one
                         if (nr.key > L[0].key) { L[1] = L[0]; L[0] = nr; }
                         else L[1] = nr;
+                        n = 2;
                     }
+                    T.cnt[ob] = n;
                 }
             }
             if (__syncthreads_or(fail)) break;
@@ -692,11 +662,10 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
             if (fail) break;
         }
         pf.mark(PROF_BUILD);
-        // every CTA writes a slice of the new node's row and of slot c1's
-        // column, so no CTA reaches the barrier late with all of them
-        M::store_node(m, ms, newNode, b, nCTA);
-        M::store_slot(m, ms, buf, rg, c1, b, nCTA);
+        // CTA 0 writes the new node's row and the owner of c1 its slot data
+        // (slicing them over every CTA was measured slower)
         if (b == 0) {
+            M::store_node(m, ms, newNode, 0, 1);
             if (threadIdx.x == 0) {
                 a.nodeSize[newNode] = s1 + s2;
                 a.rawEdge[4 * k + 0] = newNode;
@@ -709,6 +678,7 @@ __device__ __forceinline__ void join_run(const Common& a, const typename M::Args
             }
         }
         if (c1 >= rg.lo && c1 < rg.hi) {
+            M::store_slot(m, ms, buf, rg, c1, 0, 1);
             if (threadIdx.x == 0) {
                 slotNode_of(a, buf)[c1] = newNode;
                 lmOrd_of(a, buf)[c1] = a.ordNeg1;

@@ -390,14 +390,14 @@ struct IndelDense {
         return build_indel_query(m.ncol, m.ncolP, m.unitW, m.Wsel, m.nodeRow + (size_t)j1 * m.ncolP,
                                  m.nodeRow + (size_t)j2 * m.ncolP, mode, s.mrow, nullptr, s.eSC, s.eW, wc);
     }
-    // CTA `part` of `nparts` writes its slice of the new node's row
+    // slice `part` of `nparts` of the new node's row (the engine writes it whole)
     __device__ static void store_node(const Args& m, Smem& s, u32 newNode, u32 part, u32 nparts) {
         u16* dst = m.nodeRow + (size_t)newNode * m.ncolP;
         const u32 per = (m.ncolP + nparts - 1) / nparts, i1 = min(m.ncolP, (part + 1) * per);
         for (u32 i = part * per + threadIdx.x; i < i1; i += kThreads) dst[i] = s.mrow[i];
     }
-    // ... and its slice of slot c1's column entries (c1 is skipped by this
-    // phase's scan, so the owner may read the column while others write it)
+    // slice `part` of `nparts` of slot c1's column entries (the engine gives
+    // the whole column to c1's owner)
     __device__ static void store_slot(const Args& m, Smem& s, u32 buf, const joinx::Range& rg, u32 c1, u32 part,
                                       u32 nparts) {
         u16* c = col(m, buf);
@@ -710,16 +710,17 @@ struct IndelBits {
         return build_indel_query(m.ncol, m.ncolP, m.unitW, m.Wsel, m.nodeRow + (size_t)j1 * m.ncolP,
                                  m.nodeRow + (size_t)j2 * m.ncolP, mode, s.mrow, s.orow, s.eSC, s.eW, wc);
     }
-    // CTA `part` of `nparts` writes its slice of the new node's row
+    // slice `part` of `nparts` of the new node's row (the engine writes it whole)
     __device__ static void store_node(const Args& m, Smem& s, u32 newNode, u32 part, u32 nparts) {
         u16* dst = m.nodeRow + (size_t)newNode * m.ncolP;
         const u32 per = (m.ncolP + nparts - 1) / nparts, i1 = min(m.ncolP, (part + 1) * per);
         for (u32 i = part * per + threadIdx.x; i < i1; i += kThreads) dst[i] = s.mrow[i];
     }
-    // the new node replaces j1 in slot c1: each CTA flips c1's bit in the rows
-    // of its slice of the sites where the two states differ (fire-and-forget
-    // reductions on single bits; c1 is skipped by this phase's scans, and the
-    // next phase reads the words after the grid barrier)
+    // the new node replaces j1 in slot c1: flip c1's bit in the rows of slice
+    // `part` of `nparts` of the sites where the two states differ (the engine
+    // gives all of them to c1's owner; fire-and-forget reductions on single
+    // bits; c1 is skipped by this phase's scans, and the next phase reads the
+    // words after the grid barrier)
     __device__ static void store_slot(const Args& m, Smem& s, u32 buf, const joinx::Range& rg, u32 c1, u32 part,
                                       u32 nparts) {
         u32* B = bitsOf(m, buf);
