@@ -55,6 +55,7 @@ namespace fel {
 constexpr u32 kSites = 256;  // sites per block (one thread per site)
 constexpr int kWild = 0x7FFF, kNoneA = 0x7FFE;
 constexpr u32 kLbThreads = 512;
+constexpr u32 kMaxLbCTA = 256;  // CTAs of the cooperative L-BFGS kernels
 constexpr u32 kMaxHist = 16;
 
 struct Tree {
@@ -533,6 +534,7 @@ struct Lb {
 __device__ bool grid_reduce(const Lb& a, double v[4], u32& epoch) {
     __shared__ double red[kLbThreads / 32][4];
     __shared__ double out[4];
+    __shared__ double stage[kMaxLbCTA * 4];
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         double x = v[k];
@@ -551,10 +553,15 @@ __device__ bool grid_reduce(const Lb& a, double v[4], u32& epoch) {
         a.part[((size_t)par * a.nCTA + blockIdx.x) * 4 + threadIdx.x] = x;
     }
     if (flag_barrier(a.flags, a.nCTA, blockIdx.x, ++epoch, a.err, a.limitNs)) return false;
+    // all CTAs' partials in one round of loads, then summed in CTA order from
+    // shared memory (a chain of dependent L2 loads cost ~14 us a reduction)
+    const double* pp = a.part + (size_t)par * a.nCTA * 4;
+    for (u32 i = threadIdx.x; i < a.nCTA * 4; i += kLbThreads) stage[i] = __ldcg(pp + i);
+    __syncthreads();
     if (threadIdx.x < 4) {
         double x = 0.0;
         for (u32 i = 0; i < a.nCTA; i++) {
-            const double y = __ldcg(a.part + ((size_t)par * a.nCTA + i) * 4 + threadIdx.x);
+            const double y = stage[i * 4 + threadIdx.x];
             x = threadIdx.x == 3 ? fmax(x, y) : x + y;
         }
         out[threadIdx.x] = x;
@@ -1003,7 +1010,7 @@ static int setup_problem(FelProblem& F, DeviceScope& ds, u32 ntip, u32 nedge, co
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     }
-    const u32 nCTA = (u32)std::max(1, nsm), Mr = hist + 1;
+    const u32 nCTA = (u32)std::max(1, std::min(nsm, (int)kMaxLbCTA)), Mr = hist + 1;
     if (hist >= kMaxHist) return CASPHY_EINVAL;
     struct Bufs {
         u32 *kidA, *kidB, *edgeA, *edgeB, *inO, *outO, *codes, *flags, *inEB, *outEB;
