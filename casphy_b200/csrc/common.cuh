@@ -30,6 +30,19 @@ void casphy_set_last_cuda_error(cudaError_t e, const char* what, const char* fil
 void casphy_set_last_error_msg(const char* msg);
 
 // ---------------------------------------------------------------------------
+// Programmatic dependent launch, for chains of kernels in one stream or graph
+// that are launched with cudaLaunchAttributeProgrammaticStreamSerialization.
+// pdl_wait() returns once the preceding kernel has completed and its writes
+// are visible (at once for a kernel launched without the attribute);
+// pdl_trigger() lets the next kernel begin launching once every CTA of this
+// one has issued it or exited.  A kernel that calls pdl_wait() before it
+// touches global memory keeps plain stream order for every buffer, and the
+// next kernel's launch overlaps this one's tail.
+
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// ---------------------------------------------------------------------------
 // loads/stores that bypass L1 (data written by other CTAs of a live grid)
 
 __device__ __forceinline__ u32 ld_cg_u32(const u32* p) {

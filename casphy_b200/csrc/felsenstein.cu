@@ -128,6 +128,8 @@ struct Hky {
 
 __global__ void k_pmat_hky(const double* __restrict__ t, u32 nedge, Hky m, float* __restrict__ P,
                            float* __restrict__ dP) {
+    pdl_wait();
+    pdl_trigger();
     const u32 e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= nedge) return;
     double ex[4], dx[4];
@@ -218,6 +220,8 @@ __device__ __forceinline__ float4 child_hky(const Tree& T, const HkyBuf& B, cons
 }
 
 __global__ void __launch_bounds__(kSites) k_inside_hky(Tree T, HkyBuf B, Chunk C, u32 off) {
+    pdl_wait();
+    pdl_trigger();
     const u32 s = blockIdx.x * kSites + threadIdx.x;
     if (s >= C.w) return;
     const uint4 nf = T.inInfo[off + blockIdx.y];
@@ -235,6 +239,8 @@ __global__ void __launch_bounds__(kSites) k_inside_hky(Tree T, HkyBuf B, Chunk C
 
 __global__ void __launch_bounds__(kSites) k_loglik_hky(u32 root, Tree T, HkyBuf B, Chunk C, Hky m,
                                                        const double* __restrict__ w, double* part) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ double red[kSites / 32];
     const u32 s = blockIdx.x * kSites + threadIdx.x;
     double v = 0.0;
@@ -251,6 +257,8 @@ __global__ void __launch_bounds__(kSites) k_loglik_hky(u32 root, Tree T, HkyBuf 
 
 __global__ void __launch_bounds__(kSites / 2, 10) k_outside_hky(u32 root, Tree T, HkyBuf B, Chunk C, u32 off, Hky m,
                                                         const double* __restrict__ w, double* gpart) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ float sm[64];
     const uint4 nf = T.outInfo[off + blockIdx.y];
     const u32 v = nf.x, vi = v - T.ntip;
@@ -360,11 +368,15 @@ __device__ __forceinline__ float qsum(const IrrBuf& B, u32 gs, float4 l) {
 }
 
 __global__ void k_pmat_irr(const double* __restrict__ t, u32 nedge, double rate, float2* __restrict__ p) {
+    pdl_wait();
+    pdl_trigger();
     const u32 e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e < nedge) p[e] = make_float2((float)exp(-rate * t[e]), (float)(-expm1(-rate * t[e])));
 }
 
 __global__ void __launch_bounds__(kSites) k_inside_irr(Tree T, IrrBuf B, Chunk C, u32 off) {
+    pdl_wait();
+    pdl_trigger();
     const u32 s = blockIdx.x * kSites + threadIdx.x;
     if (s >= C.w) return;
     const u32 gs = C.s0 + s;
@@ -403,6 +415,8 @@ __global__ void __launch_bounds__(kSites) k_inside_irr(Tree T, IrrBuf B, Chunk C
 
 __global__ void __launch_bounds__(kSites) k_loglik_irr(u32 root, Tree T, IrrBuf B, Chunk C,
                                                        const double* __restrict__ w, double* part) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ double red[kSites / 32];
     const u32 s = blockIdx.x * kSites + threadIdx.x;
     double v = 0.0;
@@ -416,6 +430,8 @@ __global__ void __launch_bounds__(kSites) k_loglik_irr(u32 root, Tree T, IrrBuf 
 
 __global__ void __launch_bounds__(kSites) k_outside_irr(u32 root, Tree T, IrrBuf B, Chunk C, u32 off,
                                                         const double* __restrict__ w, double* gpart) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ float2 red[kSites / 32];
     const u32 s = blockIdx.x * kSites + threadIdx.x;
     const uint4 nf = T.outInfo[off + blockIdx.y];
@@ -498,6 +514,8 @@ __global__ void __launch_bounds__(kSites) k_outside_irr(u32 root, Tree T, IrrBuf
 // ------------------------------------------------ fixed-order reductions ---
 
 __global__ void k_sum_ll(const double* __restrict__ part, u32 n, double* out) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ double red[32];
     double v = 0;
     // each thread sums a contiguous run, then runs are added in thread order
@@ -509,6 +527,8 @@ __global__ void k_sum_ll(const double* __restrict__ part, u32 n, double* out) {
 }
 
 __global__ void k_sum_grad(const double* __restrict__ gpart, u32 nedge, u32 nblk, double* __restrict__ grad) {
+    pdl_wait();
+    pdl_trigger();
     const u32 e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= nedge) return;
     double v = 0;
@@ -870,11 +890,31 @@ struct FelProblem {
         if (st) cudaStreamDestroy(st);
     }
 
+    // Every kernel of an evaluation is launched with programmatic stream
+    // serialisation: each begins with pdl_wait(), so stream order holds for
+    // every buffer, and the next level's launch overlaps this one's tail.
+    cudaError_t launchErr = cudaSuccess;
+    template <class... KArgs, class... Args>
+    void lp(void (*k)(KArgs...), dim3 grid, u32 block, Args... args) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = grid;
+        cfg.blockDim = dim3(block);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        const cudaError_t e = cudaLaunchKernelEx(&cfg, k, args...);
+        if (e != cudaSuccess && launchErr == cudaSuccess) launchErr = e;
+    }
+
     void enqueue(bool withGrad, u64* launches) {
         u64 n = 0;
         const u32 ne = th.nedge;
-        if (model == CASPHY_MODEL_HKY85) k_pmat_hky<<<(ne + 127) / 128, 128, 0, st>>>(t, ne, hky, P, dP);
-        else k_pmat_irr<<<(ne + 127) / 128, 128, 0, st>>>(t, ne, rate, p);
+        if (model == CASPHY_MODEL_HKY85) lp(k_pmat_hky, dim3((ne + 127) / 128), 128, (const double*)t, ne, hky, P, dP);
+        else lp(k_pmat_irr, dim3((ne + 127) / 128), 128, (const double*)t, ne, rate, p);
         n++;
         for (u32 c = 0; c < nchunk; c++) {
             Chunk C;
@@ -887,26 +927,26 @@ struct FelProblem {
             const u32 nb = (C.w + kSites - 1) / kSites;
             for (size_t lv = 0; lv + 1 < th.inOff.size(); lv++) {
                 const dim3 grid(nb, th.inOff[lv + 1] - th.inOff[lv]);
-                if (model == CASPHY_MODEL_HKY85) k_inside_hky<<<grid, kSites, 0, st>>>(T, hb, C, th.inOff[lv]);
-                else k_inside_irr<<<grid, kSites, 0, st>>>(T, ib, C, th.inOff[lv]);
+                if (model == CASPHY_MODEL_HKY85) lp(k_inside_hky, grid, kSites, T, hb, C, th.inOff[lv]);
+                else lp(k_inside_irr, grid, kSites, T, ib, C, th.inOff[lv]);
                 n++;
             }
-            if (model == CASPHY_MODEL_HKY85) k_loglik_hky<<<nb, kSites, 0, st>>>(th.root, T, hb, C, hky, w, part);
-            else k_loglik_irr<<<nb, kSites, 0, st>>>(th.root, T, ib, C, w, part);
+            if (model == CASPHY_MODEL_HKY85) lp(k_loglik_hky, dim3(nb), kSites, th.root, T, hb, C, hky, (const double*)w, part);
+            else lp(k_loglik_irr, dim3(nb), kSites, th.root, T, ib, C, (const double*)w, part);
             n++;
             if (!withGrad) continue;
             for (size_t lv = 0; lv + 1 < th.outOff.size(); lv++) {
                 const dim3 grid(nb, th.outOff[lv + 1] - th.outOff[lv]);
                 if (model == CASPHY_MODEL_HKY85)
-                    k_outside_hky<<<grid, kSites / 2, 0, st>>>(th.root, T, hb, C, th.outOff[lv], hky, w, gpart);
-                else k_outside_irr<<<grid, kSites, 0, st>>>(th.root, T, ib, C, th.outOff[lv], w, gpart);
+                    lp(k_outside_hky, grid, kSites / 2, th.root, T, hb, C, th.outOff[lv], hky, (const double*)w, gpart);
+                else lp(k_outside_irr, grid, kSites, th.root, T, ib, C, th.outOff[lv], (const double*)w, gpart);
                 n++;
             }
         }
-        k_sum_ll<<<1, 256, 0, st>>>(part, nblkTot, ll);
+        lp(k_sum_ll, dim3(1), 256, (const double*)part, nblkTot, ll);
         n++;
         if (withGrad) {
-            k_sum_grad<<<(ne + 255) / 256, 256, 0, st>>>(gpart, ne, nblkTot, grad);
+            lp(k_sum_grad, dim3((ne + 255) / 256), 256, (const double*)gpart, ne, nblkTot, grad);
             n++;
         }
         if (launches) *launches = n;
@@ -918,6 +958,10 @@ struct FelProblem {
             CASPHY_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
             enqueue(k == 0, k == 0 ? &launchesFull : &launchesLL);
             CASPHY_CUDA_TRY(cudaStreamEndCapture(st, &g));
+            if (launchErr != cudaSuccess) {
+                cudaGraphDestroy(g);
+                CASPHY_CUDA_TRY(launchErr);
+            }
             cudaGraphExec_t ex;
             const cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
             cudaGraphDestroy(g);
