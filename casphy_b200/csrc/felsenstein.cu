@@ -971,15 +971,24 @@ struct FelProblem {
         return CASPHY_OK;
     }
 
-    // log L (and d log L / d t in `grad`) at the branch lengths in `t`
-    int eval(bool withGrad, double* llOut) {
+    // log L (and d log L / d t in `grad`) at the branch lengths in `t`:
+    // eval_launch() queues the graph and the read of log L into *llOut,
+    // eval_done() (after the stream is synchronised) adds its graph time
+    int eval_launch(bool withGrad, double* llOut) {
         CASPHY_CUDA_TRY(cudaEventRecord(g0, st));
         CASPHY_CUDA_TRY(cudaGraphLaunch(withGrad ? gFull : gLL, st));
         CASPHY_CUDA_TRY(cudaEventRecord(g1, st));
         CASPHY_CUDA_TRY(cudaMemcpyAsync(llOut, ll, sizeof(double), cudaMemcpyDeviceToHost, st));
-        CASPHY_CUDA_TRY(cudaStreamSynchronize(st));
+        return CASPHY_OK;
+    }
+    void eval_done() {
         float ms = 0;
         if (cudaEventElapsedTime(&ms, g0, g1) == cudaSuccess) graphMs += ms;
+    }
+    int eval(bool withGrad, double* llOut) {
+        if (int rc = eval_launch(withGrad, llOut)) return rc;
+        CASPHY_CUDA_TRY(cudaStreamSynchronize(st));
+        eval_done();
         return CASPHY_OK;
     }
     cudaEvent_t g0 = nullptr, g1 = nullptr;
@@ -1292,27 +1301,45 @@ extern "C" int casphy_felsenstein_optimize(uint32_t ntip, uint32_t nedge, const 
     double f = -ll;
     u32 first = 0, count = 0, quiet = 0;
     const u32 kQuiet = 5;
+    // After an accepted point that does not end the run, the accept, the next
+    // direction (with the history the accept gives when s.y > 1e-12), its
+    // unit-step trial and that trial's evaluation are queued together and
+    // read with one synchronisation.  These are the launches the step-by-step
+    // sequence makes when s.y > 1e-12 and the direction descends; otherwise
+    // the direction and the trial are discarded and made again by that
+    // sequence.  The kernels are deterministic, so the iterates are the same
+    // either way; a discarded evaluation still counts in `evaluations`.
+    bool spec = false;
+    double specGd = 0, specDmax = 0, specLl = 0;
     for (u32 it = 0; it < max_iter; it++) {
-        u32 cnt = count;
-        double sc[2] = {0, 0};
-        for (int attempt = 0; attempt < 2; attempt++) {
-            void* args[] = {&a, &first, &cnt};
-            if ((rc = lb_coop(F, (const void*)k_lb_dir, args))) return rc;
-            if ((rc = lb_read(F, a.sc + SC_GD, sc, 2))) return rc;
-            if (sc[0] < 0 || cnt == 0) break;
-            cnt = 0;  // not a descent direction: restart from steepest descent
+        double gd = specGd, dmax = specDmax;
+        if (!spec) {
+            u32 cnt = count;
+            double sc[2] = {0, 0};
+            for (int attempt = 0; attempt < 2; attempt++) {
+                void* args[] = {&a, &first, &cnt};
+                if ((rc = lb_coop(F, (const void*)k_lb_dir, args))) return rc;
+                if ((rc = lb_read(F, a.sc + SC_GD, sc, 2))) return rc;
+                if (sc[0] < 0 || cnt == 0) break;
+                cnt = 0;  // not a descent direction: restart from steepest descent
+            }
+            if (cnt == 0 && count != 0) first = (first + count) % a.Mr;
+            count = cnt;
+            gd = sc[0];
+            dmax = sc[1];
+            if (!(gd < 0)) break;  // stationary
         }
-        if (cnt == 0 && count != 0) first = (first + count) % a.Mr;
-        count = cnt;
-        const double gd = sc[0], dmax = sc[1];
-        if (!(gd < 0)) break;  // stationary
         double step = count == 0 ? std::min(1.0, 1.0 / std::max(dmax, 1e-12)) : 1.0;
         double fn = 0;
         bool accepted = false;
         for (int ls = 0; ls < 40; ls++) {
-            k_lb_trial<<<nb, 256, 0, F.st>>>(a, step);
-            if ((rc = F.eval(adj, &ll))) return rc;
-            st.evaluations++;
+            if (ls == 0 && spec) {
+                ll = specLl;  // the speculated unit step (count > 0, so step is 1)
+            } else {
+                k_lb_trial<<<nb, 256, 0, F.st>>>(a, step);
+                if ((rc = F.eval(adj, &ll))) return rc;
+                st.evaluations++;
+            }
             fn = -ll;
             if (fn <= f + 1e-4 * step * gd) {
                 accepted = true;
@@ -1320,30 +1347,48 @@ extern "C" int casphy_felsenstein_optimize(uint32_t ntip, uint32_t nedge, const 
             }
             step *= 0.5;
         }
+        spec = false;
         if (!accepted) {
             // leave t at the accepted point x
             k_lb_trial<<<nb, 256, 0, F.st>>>(a, 0.0);
             break;
         }
         if (!adj && (rc = fd_gradient(F, st))) return rc;
+        // converged when log L has changed by at most rel_tol (relative) in
+        // each of the last kQuiet steps: one short step alone does not stop
+        const double rel = std::fabs(f - fn) / std::max(std::fabs(f), 1e-300);
+        const u32 quietNext = rel <= rel_tol ? quiet + 1 : 0;
         u32 slot = (first + count) % a.Mr;
         void* args[] = {&a, &slot};
         if ((rc = lb_coop(F, (const void*)k_lb_accept, args))) return rc;
         double sy = 0;
-        if ((rc = lb_read(F, a.sc + SC_SY, &sy, 1))) return rc;
+        if (adj && quietNext < kQuiet && it + 1 < max_iter) {
+            u32 cntN = count < M ? count + 1 : count, firstN = count < M ? first : (first + 1) % a.Mr;
+            void* dargs[] = {&a, &firstN, &cntN};
+            if ((rc = lb_coop(F, (const void*)k_lb_dir, dargs))) return rc;
+            k_lb_trial<<<nb, 256, 0, F.st>>>(a, 1.0);
+            if ((rc = F.eval_launch(adj, &specLl))) return rc;
+            double sc3[3] = {0, 0, 0};  // g.d, max|d| of the direction; s.y of the accept
+            if ((rc = lb_read(F, a.sc + SC_GD, sc3, 3))) return rc;
+            F.eval_done();
+            st.evaluations++;
+            sy = sc3[SC_SY - SC_GD];
+            specGd = sc3[SC_GD - SC_GD];
+            specDmax = sc3[SC_DMAX - SC_GD];
+            spec = sy > 1e-12 && specGd < 0;
+        } else {
+            if ((rc = lb_read(F, a.sc + SC_SY, &sy, 1))) return rc;
+        }
         st.iterations++;
         if (sy > 1e-12) {
             if (count < M) count++;
             else first = (first + 1) % a.Mr;
         }
-        const double rel = std::fabs(f - fn) / std::max(std::fabs(f), 1e-300);
         if (trace)
-            std::fprintf(stderr, "blopt it %u f %.10f df %.3e gd %.3e step %.3e hist %u sy %.3e\n", it, fn, fn - f, gd,
-                         step, count, sy);
+            std::fprintf(stderr, "blopt it %u f %.10f df %.3e gd %.3e step %.3e hist %u sy %.3e%s\n", it, fn, fn - f,
+                         gd, step, count, sy, spec || !(adj && quietNext < kQuiet && it + 1 < max_iter) ? "" : " (speculated step discarded)");
         f = fn;
-        // converged when log L has changed by at most rel_tol (relative) in
-        // each of the last kQuiet steps: one short step alone does not stop
-        quiet = rel <= rel_tol ? quiet + 1 : 0;
+        quiet = quietNext;
         if (quiet >= kQuiet) break;
     }
     CASPHY_CUDA_TRY(cudaEventRecord(F.e1, F.st));
