@@ -219,22 +219,37 @@ __device__ __forceinline__ float4 child_hky(const Tree& T, const HkyBuf& B, cons
     return B.L[i];
 }
 
-__global__ void __launch_bounds__(kSites) k_inside_hky(Tree T, HkyBuf B, Chunk C, u32 off) {
-    pdl_wait();
-    pdl_trigger();
-    const u32 s = blockIdx.x * kSites + threadIdx.x;
-    if (s >= C.w) return;
-    const uint4 nf = T.inInfo[off + blockIdx.y];
-    const u32 vi = nf.x - T.ntip, eB = T.inEdgeB[off + blockIdx.y];
-    int ea, eb;
-    const float4 la = child_hky(T, B, C, nf.y, s, &ea);
-    const float4 lb = child_hky(T, B, C, nf.z, s, &eb);
-    const float4 ma = pmatvec(B.P + 16 * nf.w, la);
+// One (node, site) of the inside pass once its children's partials are in.
+__device__ __forceinline__ void inside_hky_site(const HkyBuf& B, const Chunk& C, u32 vi, u32 eA, u32 eB, u32 s,
+                                                float4 la, int ea, float4 lb, int eb) {
+    const float4 ma = pmatvec(B.P + 16 * eA, la);
     const float4 mb = pmatvec(B.P + 16 * eB, lb);
     float4 l = make_float4(ma.x * mb.x, ma.y * mb.y, ma.z * mb.z, ma.w * mb.w);
     const int e = renorm4(l);
     B.L[(size_t)vi * C.W + s] = l;
     B.E[(size_t)vi * C.W + s] = ea + eb + e;
+}
+
+// 128 threads per 256-site block, two sites per thread (128 apart), every
+// child load issued before any arithmetic
+__global__ void __launch_bounds__(kSites / 2) k_inside_hky(Tree T, HkyBuf B, Chunk C, u32 off) {
+    pdl_wait();
+    pdl_trigger();
+    const uint4 nf = T.inInfo[off + blockIdx.y];
+    const u32 vi = nf.x - T.ntip, eB = T.inEdgeB[off + blockIdx.y];
+    u32 sj[2];
+    float4 la[2], lb[2];
+    int ea[2], eb[2];
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        sj[j] = blockIdx.x * kSites + threadIdx.x + j * (kSites / 2);
+        const u32 ss = sj[j] < C.w ? sj[j] : 0u;
+        la[j] = child_hky(T, B, C, nf.y, ss, &ea[j]);
+        lb[j] = child_hky(T, B, C, nf.z, ss, &eb[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+        if (sj[j] < C.w) inside_hky_site(B, C, vi, nf.w, eB, sj[j], la[j], ea[j], lb[j], eb[j]);
 }
 
 __global__ void __launch_bounds__(kSites) k_loglik_hky(u32 root, Tree T, HkyBuf B, Chunk C, Hky m,
@@ -374,17 +389,10 @@ __global__ void k_pmat_irr(const double* __restrict__ t, u32 nedge, double rate,
     if (e < nedge) p[e] = make_float2((float)exp(-rate * t[e]), (float)(-expm1(-rate * t[e])));
 }
 
-__global__ void __launch_bounds__(kSites) k_inside_irr(Tree T, IrrBuf B, Chunk C, u32 off) {
-    pdl_wait();
-    pdl_trigger();
-    const u32 s = blockIdx.x * kSites + threadIdx.x;
-    if (s >= C.w) return;
+// One (node, site) of the inside pass once its children's partials are in.
+__device__ __forceinline__ void inside_irr_site(const IrrBuf& B, const Chunk& C, u32 vi, float2 pa, float2 pb, u32 s,
+                                                float4 la, float4 lb) {
     const u32 gs = C.s0 + s;
-    const uint4 nf = T.inInfo[off + blockIdx.y];
-    const u32 vi = nf.x - T.ntip;
-    const float4 la = child_irr(T, B, C, nf.y, s);
-    const float4 lb = child_irr(T, B, C, nf.z, s);
-    const float2 pa = B.p[nf.w], pb = B.p[T.inEdgeB[off + blockIdx.y]];
     const float m0a = la.x + pa.y * (qsum(B, gs, la) - la.x);
     const float m0b = lb.x + pb.y * (qsum(B, gs, lb) - lb.x);
     const int aa = __float_as_int(la.z), ab = __float_as_int(lb.z);
@@ -411,6 +419,28 @@ __global__ void __launch_bounds__(kSites) k_inside_irr(Tree T, IrrBuf B, Chunk C
     }
     e += __float_as_int(la.w) + __float_as_int(lb.w);
     B.L[(size_t)vi * C.W + s] = make_float4(l0, lA, __int_as_float(a), __int_as_float(e));
+}
+
+// 128 threads per 256-site block, two sites per thread (128 apart), every
+// child load issued before any arithmetic
+__global__ void __launch_bounds__(kSites / 2) k_inside_irr(Tree T, IrrBuf B, Chunk C, u32 off) {
+    pdl_wait();
+    pdl_trigger();
+    const uint4 nf = T.inInfo[off + blockIdx.y];
+    const u32 vi = nf.x - T.ntip;
+    const float2 pa = B.p[nf.w], pb = B.p[T.inEdgeB[off + blockIdx.y]];
+    u32 sj[2];
+    float4 la[2], lb[2];
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        sj[j] = blockIdx.x * kSites + threadIdx.x + j * (kSites / 2);
+        const u32 ss = sj[j] < C.w ? sj[j] : 0u;
+        la[j] = child_irr(T, B, C, nf.y, ss);
+        lb[j] = child_irr(T, B, C, nf.z, ss);
+    }
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+        if (sj[j] < C.w) inside_irr_site(B, C, vi, pa, pb, sj[j], la[j], lb[j]);
 }
 
 __global__ void __launch_bounds__(kSites) k_loglik_irr(u32 root, Tree T, IrrBuf B, Chunk C,
@@ -927,8 +957,8 @@ struct FelProblem {
             const u32 nb = (C.w + kSites - 1) / kSites;
             for (size_t lv = 0; lv + 1 < th.inOff.size(); lv++) {
                 const dim3 grid(nb, th.inOff[lv + 1] - th.inOff[lv]);
-                if (model == CASPHY_MODEL_HKY85) lp(k_inside_hky, grid, kSites, T, hb, C, th.inOff[lv]);
-                else lp(k_inside_irr, grid, kSites, T, ib, C, th.inOff[lv]);
+                if (model == CASPHY_MODEL_HKY85) lp(k_inside_hky, grid, kSites / 2, T, hb, C, th.inOff[lv]);
+                else lp(k_inside_irr, grid, kSites / 2, T, ib, C, th.inOff[lv]);
                 n++;
             }
             if (model == CASPHY_MODEL_HKY85) lp(k_loglik_hky, dim3(nb), kSites, th.root, T, hb, C, hky, (const double*)w, part);
