@@ -211,7 +211,9 @@ typedef struct {
 
 typedef struct {
     uint32_t iterations;        /* accepted L-BFGS steps */
-    uint32_t evaluations;       /* likelihood evaluations (graph launches) */
+    uint32_t evaluations;       /* likelihood evaluations (graph launches),
+                                   including a speculated unit step that the
+                                   accept then discards */
     uint32_t site_chunks;
     uint32_t levels_inside;     /* tree height (inside launches per chunk) */
     uint32_t levels_outside;    /* depth levels (outside launches per chunk) */
