@@ -1,5 +1,6 @@
-"""Sharded TransferDisStream and bootstrap on two gloo ranks (CPU, oracle as
-the per-rank compute) equal the one-process results."""
+"""Sharded TransferDisStream, radius lists and bootstrap on two and three gloo
+ranks (CPU, oracle as the per-rank compute) equal the one-process results;
+three ranks split 61 rows, 37 columns and 5 replicates unevenly."""
 import os
 import socket
 
@@ -62,17 +63,18 @@ def _worker(rank, world, port, q):
         dist.destroy_process_group()
 
 
-def test_two_rank_sharding_matches_one_process():
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharding_matches_one_process(world):
     import oracle as O
     from casphy_b200 import bootstrap as B
     from casphy_b200 import synth
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q)) for r in range(world)]
     for p in procs:
         p.start()
-    res = [q.get(timeout=300) for _ in range(2)]
+    res = [q.get(timeout=300) for _ in range(world)]
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
